@@ -1,0 +1,297 @@
+"""Throughput of the MD hot path on B200: MATS (million atom-timesteps per
+second) and TPS for the Kob-Andersen NVT system with cell lists.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--n PARTICLES] [--impl reference]
+
+Workload (one rank): Kob-Andersen 80:20 LJ mixture, shifted force at 2.5
+sigma_ab, density 1.2, Nose-Hoover NVT T = 0.45 (tau 0.2), dt 0.005, float32,
+cell-list neighbour list with skin 0.3, N = 1,048,576 by default (the largest
+N of the reference's KA sweep), seeded synthetic input.  A step is one MD time
+step (forces, integration, runtime actions, neighbour-list check/rebuild);
+TPS counts steps over the timeblock's device time as gamdpy does
+(benchmarks/benchmark_LJ.py:90).  The working set per step (neighbour list,
+~0.45 GB) is larger than the 126 MB L2, so no flush is needed between steps.
+
+--gpus N (one process per GPU under torchrun): N independent replicas with
+different seeds ("replicas only": one MD system does not shard); value = total
+atom-steps / max over ranks of the device time.
+
+--impl reference: the reference's algorithm on the host cores (the CPU
+oracle, all threads), same workload, a bounded sample of steps.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MATS (million atom-timesteps/s), KA-LJ NVT cell lists, 1 B200"
+UNIT = "Matom-steps/s"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=2000)
+    p.add_argument("--warmup", type=int, default=200)
+    p.add_argument("--n", type=int, default=1_048_576)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--block", type=int, default=500, help="steps per timeblock")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "b200" else "gloo"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=300))
+        pg = dist
+    return rank, world, local, pg
+
+
+def allreduce_max(pg, x, local):
+    if pg is None:
+        return x
+    import torch
+    dev = torch.device("cuda", local) if pg.get_backend() == "nccl" else torch.device("cpu")
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_atom_step():
+    """DRAM bytes per atom-step of the step kernel from the committed ncu
+    summary (profiles/step_kernel_ka.txt, line 'traffic_bytes_per_atom_step')."""
+    path = os.path.join(ROOT, "profiles", "step_kernel_ka.txt")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_atom_step"):
+                    return float(line.split("=")[1].split()[0])
+    except (OSError, ValueError, IndexError):
+        pass
+    return None
+
+
+def cpu_reference(args, n, steps, seed=0):
+    """The oracle on the host cores: ka workload, `steps` steps after one
+    build.  Returns (MATS, threads, seconds)."""
+    from gamdpy_b200 import workloads
+    from oracle import oracle as O
+    conf = workloads.ka_configuration(n, seed=seed)
+    tab = O.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    run = O.Run(conf["r"], conf["v"], conf["m"], conf.ptype, conf.simbox.lengths, tab, nblist="linked lists",
+                skin=0.3, max_nbs=300, integrator="NVT", dt=0.005, temperature=0.45, tau=0.2)
+    run.run_timeblock(1)  # first list build outside the timing, as the GPU warm-up
+    t0 = time.perf_counter()
+    run.run_timeblock(steps)
+    dt = time.perf_counter() - t0
+    return n * steps / dt / 1e6, O.num_threads(), dt
+
+
+def run_reference_arm(args):
+    rank, world, local, pg = dist_setup(args)
+    if rank != 0:
+        barrier(pg)
+        return
+    # bounded sample: a few steps of the full-size system (~tens of seconds)
+    steps = max(1, min(args.steps, 5))
+    vals = []
+    for _ in range(max(1, min(args.warmup, 1))):
+        cpu_reference(args, args.n, 1)
+    mats, threads, secs = cpu_reference(args, args.n, steps)
+    vals.append(mats)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": mats, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": 1, "ms_per_step": secs / steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattice)",
+        "config": {"workload": f"KA-LJ NVT rho=1.2 T=0.45 cells skin=0.3 N={args.n}", "n": args.n,
+                   "parallelism": "host threads"},
+        "cpu_baseline": {"value": mats, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": f"{steps} steps of N={args.n} after one list build"},
+        "e2e": {"value": mats, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    barrier(pg)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference_arm(args)
+        return
+    rank, world, local, pg = dist_setup(args)
+    import gamdpy_b200 as gp
+    from gamdpy_b200 import _lib, workloads
+
+    n = args.n
+    conf = workloads.ka_configuration(n, seed=1234 + rank)
+    pp = workloads.ka_pair_potential(max_num_nbs=300)
+    integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
+    block = min(args.block, max(1, args.steps))
+    plan = {"pb": 64, "tp": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False, "nblist": "linked lists"}
+    sim = gp.Simulation(conf, pp, integ, [gp.ScalarSaver(max(1, block // 8))], num_timeblocks=8,
+                        steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
+    dev = sim._sim
+    # warm-up (device resident), includes graph capture
+    dev.run(0.0, max(3, args.warmup))
+    dev.clear_status()
+
+    # ---- timed: K steps, device-resident inputs ---------------------------
+    nblocks = max(1, args.steps // block)
+    steps = nblocks * block
+    clocks = ClockSampler(local)
+    barrier(pg)
+    clocks.start()
+    ms_total = 0.0
+    for b in range(nblocks):
+        ms_total += dev.run(float(b * block * 0.005), block)
+    clock_info = clocks.stop()
+    barrier(pg)
+    t_max = allreduce_max(pg, ms_total / 1e3, local)
+    mats = n * steps * world / t_max / 1e6
+    tps = steps / t_max
+
+    # ---- end to end through the public API (host buffers) ------------------
+    # gamdpy's pattern (Simulation.run_timeblocks): upload once, then every
+    # timeblock run on the device and copy r, v, f, images and scalars back
+    e2e_blocks = max(1, min(nblocks, 4))
+    barrier(pg)
+    t0 = time.perf_counter()
+    conf.copy_to_device()
+    for b in range(e2e_blocks):
+        dev.run(float(b * block * 0.005), block)
+        conf.copy_to_host()
+    e2e_s = allreduce_max(pg, time.perf_counter() - t0, local)
+    e2e_steps = e2e_blocks * block
+    h2d = n * (12 + 12 + 4 + 4 + 12)  # r, v, m, type, images
+    d2h = n * (12 + 12 + 12 + 12 + 4 * 5)  # r, v, f, images, 5 scalar planes
+    e2e = {"value": n * e2e_steps * world / e2e_s / 1e6, "unit": UNIT,
+           "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
+           "timeblock_steps": block, "note": "upload once + per-timeblock device->host copy of the state"}
+
+    # ---- roofline of the fused step kernel --------------------------------
+    mean_nbs, max_nbs = dev.nblist_stats()
+    reps = 50
+    ms_launch = dev.time_step_kernel(reps)
+    bytes_per_atom = 4.0 * mean_nbs + 64.0
+    achieved = bytes_per_atom * n / (ms_launch * 1e-3) / 1e9
+    peak, peak_kind = measured_peak_hbm()
+    traffic = ncu_traffic_per_atom_step()
+
+    # launches inside the timed region: per step the fused kernel + the
+    # 9-kernel rebuild chain (gated), per block the final evaluation with its
+    # chain, the block-begin kernel
+    launches_per_block = block * 10 + 10 + 1
+    line = {
+        "metric": METRIC, "value": mats, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattice)",
+        "config": {"workload": f"KA-LJ NVT rho=1.2 T=0.45 dt=0.005 cells skin=0.3 N={n}", "n": n,
+                   "tps": tps, "timeblock_steps": block, "parallelism": f"replicas x{world}",
+                   "l2": "per-step working set (neighbour list) > 126 MB L2, no flush",
+                   "mean_neighbours": mean_nbs, "max_neighbours": max_nbs},
+        "e2e": e2e,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_source": peak_kind,
+                     "traffic": (traffic * n if traffic else None),
+                     "algorithmic_bytes_per_atom_step": bytes_per_atom, "kernel": "k_step (fused force+NVT)",
+                     "ms_per_launch": ms_launch},
+        "clocks": clock_info,
+        "gpu_launches": launches_per_block * nblocks,
+    }
+    if rank == 0 and world == 1:
+        cps = max(1, min(3, args.steps))
+        cmats, threads, secs = cpu_reference(args, n, cps)
+        line["cpu_baseline"] = {"value": cmats, "unit": UNIT, "cores": threads, "kind": "port",
+                                "sample": f"{cps} steps of the same N={n} system ({secs:.1f} s)"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,515 @@
+// analysis.cu -- radial distribution function and structure factor on B200.
+//
+// RDF (calculators/calculator_radial_distribution.py:76-107): every ordered
+// pair i != j with dist_sq < r_max^2 is counted in bin int(d / width) of its
+// (type_i, type_j) histogram, with the reference's mixed precision: dist_sq
+// in float32 (orthorhombic.py:59-73), the range test and d / width in
+// float64, d = sqrt(dist_sq) in float32.  Counts are exact integers (uint64).
+//   * r_max >= min(L)/3: all pairs, j tiles staged in shared memory.
+//   * smaller r_max: particles binned into cells of edge >= r_max (counting
+//     sort), 27-cell stencil.  Same pair set, so the same counts.
+// Per-block histograms live in shared memory (uint32) and are flushed with
+// 64-bit atomics.
+//
+// S(q) (calculators/calculator_structure_factor.py:131-156, :185-203):
+// rho_q = N_f^-1/2 sum_i f_i exp(i q.r_i) with q = 2 pi n / L.  Because q is
+// on the reciprocal lattice, exp(i q.r) = e_x(nx) e_y(ny) e_z(nz) with
+// e_d(k) = exp(2 pi i k r_d / L_d); each block tabulates e_d(k) for a tile of
+// particles in shared memory (sincospi, float32) and every thread accumulates
+// its q-vectors with complex multiplies, float32 within a tile and float64
+// across tiles.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "../../include/gamdb200.h"
+#include "gdb_internal.cuh"
+
+using namespace gdb;
+
+extern "C" {
+const float4 *gdb_internal_pos(gdb_sim *h);
+const int *gdb_internal_orig(gdb_sim *h);
+cudaStream_t gdb_internal_stream(gdb_sim *h);
+const float *gdb_internal_box(gdb_sim *h);
+int gdb_internal_n(gdb_sim *h);
+int gdb_internal_ntypes(gdb_sim *h);
+int gdb_internal_dev(gdb_sim *h);
+int gdb_internal_uploaded(gdb_sim *h);
+char *gdb_internal_err(gdb_sim *h);
+}
+
+static int aset(gdb_sim *h, int code, const char *msg, cudaError_t e = cudaSuccess) {
+    snprintf(gdb_internal_err(h), 512, "%s%s%s", msg, e != cudaSuccess ? ": " : "",
+             e != cudaSuccess ? cudaGetErrorString(e) : "");
+    return code;
+}
+
+#define ACK(call)                                                     \
+    do {                                                              \
+        cudaError_t e_ = (call);                                      \
+        if (e_ != cudaSuccess) return aset(h, GDB_ERR_CUDA, #call, e_); \
+    } while (0)
+
+namespace {
+
+constexpr int RDF_TILE = 256;
+constexpr int RDF_SMEM_MAX_BINS = 12288;  // uint32 entries kept in shared memory
+
+struct RdfArgs {
+    const float4 *pos;
+    int n, nt, bins;
+    float Lx, Ly, Lz;
+    double r_max, width, r_max_sq;
+    unsigned long long *out;
+    int fma;  // distance accumulation form (see dist_sq_exact)
+};
+
+__device__ __forceinline__ void rdf_pair(const RdfArgs &a, float4 pj, float4 pi, int ti, unsigned *hist,
+                                         bool shared_hist) {
+    const float d2 = a.fma ? dist_sq_exact<true>(pj, pi, a.Lx, a.Ly, a.Lz) : dist_sq_exact<false>(pj, pi, a.Lx, a.Ly, a.Lz);
+    if ((double)d2 < a.r_max_sq) {
+        const float d = __fsqrt_rn(d2);
+        if ((double)d < a.r_max) {
+            int b = (int)__ddiv_rn((double)d, a.width);
+            // d < r_max, yet d / width can round up to `bins`; the reference
+            // would index past its array there, this keeps the count in range
+            if (b >= a.bins) b = a.bins - 1;
+            const int tj = ptype_of(pj);
+            const int idx = (ti * a.nt + tj) * a.bins + b;
+            if (shared_hist)
+                atomicAdd(&hist[idx], 1u);
+            else
+                atomicAdd(&a.out[idx], 1ull);
+        }
+    }
+}
+
+__device__ __forceinline__ void flush_hist(const RdfArgs &a, unsigned *hist, int total) {
+    __syncthreads();
+    for (int k = threadIdx.x; k < total; k += blockDim.x)
+        if (hist[k]) atomicAdd(&a.out[k], (unsigned long long)hist[k]);
+}
+
+// all pairs: block = RDF_TILE particles i; j tiles through shared memory
+__global__ void __launch_bounds__(RDF_TILE) k_rdf_allpairs(RdfArgs a) {
+    extern __shared__ unsigned char smraw[];
+    float4 *tile = (float4 *)smraw;
+    unsigned *hist = (unsigned *)(tile + RDF_TILE);
+    const int total = a.nt * a.nt * a.bins;
+    const bool sh = total <= RDF_SMEM_MAX_BINS;
+    if (sh)
+        for (int k = threadIdx.x; k < total; k += blockDim.x) hist[k] = 0;
+    const int i = blockIdx.x * RDF_TILE + threadIdx.x;
+    const bool act = i < a.n;
+    const float4 pi = act ? a.pos[i] : make_float4(0, 0, 0, 0);
+    const int ti = ptype_of(pi);
+    for (int j0 = 0; j0 < a.n; j0 += RDF_TILE) {
+        __syncthreads();
+        const int jl = j0 + threadIdx.x;
+        if (jl < a.n) tile[threadIdx.x] = a.pos[jl];
+        __syncthreads();
+        const int jn = min(RDF_TILE, a.n - j0);
+        if (act)
+            for (int q = 0; q < jn; q++) {
+                if (j0 + q == i) continue;
+                rdf_pair(a, tile[q], pi, ti, hist, sh);
+            }
+    }
+    if (sh) flush_hist(a, hist, total);
+}
+
+// cell-based pair search for r_max < L/3
+__global__ void k_bin_cells(const float4 *pos, int n, float Lx, float Ly, float Lz, int ncx, int ncy, int ncz,
+                            int *pcell, int *prank, int *count) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    const float r[3] = {p.x, p.y, p.z};
+    const float L[3] = {Lx, Ly, Lz};
+    const int nc[3] = {ncx, ncy, ncz};
+    int c[3];
+    for (int k = 0; k < 3; k++) {
+        float f = (r[k] / L[k] + 0.5f) * nc[k];
+        int ci = (int)floorf(f);
+        if (!(f == f)) ci = 0;
+        ci %= nc[k];
+        if (ci < 0) ci += nc[k];
+        c[k] = ci;
+    }
+    const int cid = (c[2] * ncy + c[1]) * ncx + c[0];
+    pcell[i] = cid;
+    prank[i] = atomicAdd(&count[cid], 1);
+}
+
+__global__ void k_cells_scan_serial(const int *count, int *start, int ncell) {
+    // small cell grids only (r_max >= a few sigma): a single thread is enough
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        int s = 0;
+        for (int c = 0; c < ncell; c++) {
+            start[c] = s;
+            s += count[c];
+        }
+        start[ncell] = s;
+    }
+}
+
+__global__ void k_cells_scatter(const int *pcell, const int *prank, const int *start, int *perm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    perm[start[pcell[i]] + prank[i]] = i;
+}
+
+__global__ void __launch_bounds__(RDF_TILE) k_rdf_cells(RdfArgs a, const int *perm, const int *start, int ncx,
+                                                        int ncy, int ncz) {
+    extern __shared__ unsigned char smraw[];
+    unsigned *hist = (unsigned *)smraw;
+    const int total = a.nt * a.nt * a.bins;
+    const bool sh = total <= RDF_SMEM_MAX_BINS;
+    if (sh) {
+        for (int k = threadIdx.x; k < total; k += blockDim.x) hist[k] = 0;
+        __syncthreads();
+    }
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < a.n) {
+        const int i = perm[s];
+        const float4 pi = a.pos[i];
+        const int ti = ptype_of(pi);
+        // cell of particle i from its slot: find via position (same formula as k_bin_cells)
+        const float r[3] = {pi.x, pi.y, pi.z};
+        const float L[3] = {a.Lx, a.Ly, a.Lz};
+        const int nc[3] = {ncx, ncy, ncz};
+        int c[3];
+        for (int k = 0; k < 3; k++) {
+            float f = (r[k] / L[k] + 0.5f) * nc[k];
+            int ci = (int)floorf(f);
+            if (!(f == f)) ci = 0;
+            ci %= nc[k];
+            if (ci < 0) ci += nc[k];
+            c[k] = ci;
+        }
+        for (int dz = -1; dz <= 1; dz++)
+            for (int dy = -1; dy <= 1; dy++)
+                for (int dx = -1; dx <= 1; dx++) {
+                    const int x = (c[0] + dx + ncx) % ncx, y = (c[1] + dy + ncy) % ncy, z = (c[2] + dz + ncz) % ncz;
+                    const int cid = (z * ncy + y) * ncx + x;
+                    for (int q = start[cid]; q < start[cid + 1]; q++) {
+                        const int j = perm[q];
+                        if (j == i) continue;
+                        rdf_pair(a, a.pos[j], pi, ti, hist, sh);
+                    }
+                }
+    }
+    if (sh) flush_hist(a, hist, total);
+}
+
+// ---------------------------------------------------------------------------
+// S(q)
+// ---------------------------------------------------------------------------
+constexpr int SQ_TILE = 32;      // particles per shared-memory tile
+constexpr int SQ_THREADS = 256;  // q-vectors per block
+constexpr int SQ_CHUNK = 8192;   // particles per block (grid y)
+
+struct SqArgs {
+    const float4 *pos;
+    const int *orig;
+    const float *ff;  // user order, may be null
+    int n, nq;
+    const int *nvec;  // nq x 3
+    int kmin[3], klen[3];
+    float invL[3];
+    double *acc;  // nq x 2
+};
+
+__global__ void __launch_bounds__(SQ_THREADS) k_sq(SqArgs a) {
+    extern __shared__ float2 tab[];  // [SQ_TILE][klen0 + klen1 + klen2]
+    __shared__ float wsh[SQ_TILE];
+    const int row = a.klen[0] + a.klen[1] + a.klen[2];
+    const int q = blockIdx.x * SQ_THREADS + threadIdx.x;
+    int nx = 0, ny = 0, nz = 0;
+    if (q < a.nq) {
+        nx = a.nvec[3 * q] - a.kmin[0];
+        ny = a.nvec[3 * q + 1] - a.kmin[1] + a.klen[0];
+        nz = a.nvec[3 * q + 2] - a.kmin[2] + a.klen[0] + a.klen[1];
+    }
+    double sr = 0.0, si = 0.0;
+    const int p_begin = blockIdx.y * SQ_CHUNK;
+    const int p_end = min(a.n, p_begin + SQ_CHUNK);
+    for (int p0 = p_begin; p0 < p_end; p0 += SQ_TILE) {
+        const int np = min(SQ_TILE, p_end - p0);
+        __syncthreads();
+        // tabulate e_d(k) = exp(2 pi i k x_d / L_d)
+        for (int e = threadIdx.x; e < np * row; e += SQ_THREADS) {
+            const int pl = e / row, col = e % row;
+            const float4 p = a.pos[p0 + pl];
+            int d, k;
+            if (col < a.klen[0]) {
+                d = 0;
+                k = col + a.kmin[0];
+            } else if (col < a.klen[0] + a.klen[1]) {
+                d = 1;
+                k = col - a.klen[0] + a.kmin[1];
+            } else {
+                d = 2;
+                k = col - a.klen[0] - a.klen[1] + a.kmin[2];
+            }
+            const float x = d == 0 ? p.x : (d == 1 ? p.y : p.z);
+            float s, c;
+            sincospif(2.0f * (float)k * (x * a.invL[d]), &s, &c);
+            tab[pl * row + col] = make_float2(c, s);
+        }
+        if (threadIdx.x < np) {
+            const int slot = p0 + threadIdx.x;
+            wsh[threadIdx.x] = a.ff ? a.ff[a.orig[slot]] : 1.0f;
+        }
+        __syncthreads();
+        if (q < a.nq) {
+            float tr = 0.f, ti = 0.f;
+            for (int pl = 0; pl < np; pl++) {
+                const float2 ex = tab[pl * row + nx], ey = tab[pl * row + ny], ez = tab[pl * row + nz];
+                const float xr = ex.x * ey.x - ex.y * ey.y, xi = ex.x * ey.y + ex.y * ey.x;
+                const float w = wsh[pl];
+                tr += w * (xr * ez.x - xi * ez.y);
+                ti += w * (xr * ez.y + xi * ez.x);
+            }
+            sr += tr;
+            si += ti;
+        }
+    }
+    if (q < a.nq) {
+        atomicAdd(&a.acc[2 * q], sr);
+        atomicAdd(&a.acc[2 * q + 1], si);
+    }
+}
+
+__global__ void k_pack_pos(int n, const float *r, const int *pt, float4 *pos, int *orig) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    pos[i] = make_float4(r[3 * i], r[3 * i + 1], r[3 * i + 2], __int_as_float(pt ? pt[i] : 0));
+    orig[i] = i;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// host implementations working on device-resident positions
+// ---------------------------------------------------------------------------
+static int rdf_device(gdb_sim *h, cudaStream_t st, const float4 *pos, int n, const float *box, int nt, int bins,
+                      double r_max, uint64_t *out_host) {
+    if (bins < 1 || nt < 1) return aset(h, GDB_ERR_ARG, "rdf: bins and ntypes must be positive");
+    float minL = fminf(box[0], fminf(box[1], box[2]));
+    // the reference: min_box_dim float32, (min_box_dim / 2) float64
+    const double half = (double)minL / 2.0;
+    if (r_max <= 0.0) r_max = half;
+    if (r_max > half) return aset(h, GDB_ERR_ARG, "rdf: r_max must not exceed min(L)/2");
+    RdfArgs a;
+    a.pos = pos;
+    a.n = n;
+    a.nt = nt;
+    a.bins = bins;
+    a.Lx = box[0];
+    a.Ly = box[1];
+    a.Lz = box[2];
+    a.r_max = r_max;
+    a.width = r_max / (double)bins;
+    a.r_max_sq = r_max * r_max;
+    {
+        const char *fm = getenv("GDB_NBLIST_FMA");
+        a.fma = (fm && fm[0] == '0') ? 0 : 1;
+    }
+    const size_t total = (size_t)nt * nt * bins;
+    unsigned long long *dout = nullptr;
+    ACK(cudaMallocAsync(&dout, total * sizeof(unsigned long long), st));
+    ACK(cudaMemsetAsync(dout, 0, total * sizeof(unsigned long long), st));
+    a.out = dout;
+    const bool sh = total <= (size_t)RDF_SMEM_MAX_BINS;
+    int nc[3];
+    bool cells = true;
+    for (int k = 0; k < 3; k++) {
+        // edge slightly above r_max so float32 rounding of the cell
+        // coordinate can never separate a pair closer than r_max by two cells
+        nc[k] = (int)floor(box[k] / (r_max * (1.0 + 1e-4)));
+        if (nc[k] < 3) cells = false;
+    }
+    if (!cells) {
+        const size_t smem = RDF_TILE * sizeof(float4) + (sh ? total * sizeof(unsigned) : 0);
+        ACK(cudaFuncSetAttribute(k_rdf_allpairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_rdf_allpairs<<<(n + RDF_TILE - 1) / RDF_TILE, RDF_TILE, smem, st>>>(a);
+        ACK(cudaGetLastError());
+    } else {
+        const long long ncell = (long long)nc[0] * nc[1] * nc[2];
+        int *count = nullptr, *start = nullptr, *pcell = nullptr, *prank = nullptr, *perm = nullptr;
+        ACK(cudaMallocAsync(&count, ncell * sizeof(int), st));
+        ACK(cudaMallocAsync(&start, (ncell + 1) * sizeof(int), st));
+        ACK(cudaMallocAsync(&pcell, (size_t)n * sizeof(int), st));
+        ACK(cudaMallocAsync(&prank, (size_t)n * sizeof(int), st));
+        ACK(cudaMallocAsync(&perm, (size_t)n * sizeof(int), st));
+        ACK(cudaMemsetAsync(count, 0, ncell * sizeof(int), st));
+        const int g = (n + 255) / 256;
+        k_bin_cells<<<g, 256, 0, st>>>(pos, n, box[0], box[1], box[2], nc[0], nc[1], nc[2], pcell, prank, count);
+        k_cells_scan_serial<<<1, 1, 0, st>>>(count, start, (int)ncell);
+        k_cells_scatter<<<g, 256, 0, st>>>(pcell, prank, start, perm, n);
+        const size_t smem = sh ? total * sizeof(unsigned) : 0;
+        ACK(cudaFuncSetAttribute(k_rdf_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        k_rdf_cells<<<(n + RDF_TILE - 1) / RDF_TILE, RDF_TILE, smem, st>>>(a, perm, start, nc[0], nc[1], nc[2]);
+        ACK(cudaGetLastError());
+        ACK(cudaFreeAsync(count, st));
+        ACK(cudaFreeAsync(start, st));
+        ACK(cudaFreeAsync(pcell, st));
+        ACK(cudaFreeAsync(prank, st));
+        ACK(cudaFreeAsync(perm, st));
+    }
+    std::vector<unsigned long long> tmp(total);
+    ACK(cudaMemcpyAsync(tmp.data(), dout, total * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    ACK(cudaFreeAsync(dout, st));
+    ACK(cudaStreamSynchronize(st));
+    for (size_t k = 0; k < total; k++) out_host[k] += tmp[k];
+    return GDB_OK;
+}
+
+static int sq_device(gdb_sim *h, cudaStream_t st, const float4 *pos, const int *orig, int n, const float *ff_host,
+                     const float *box, int nq, const int32_t *nvec_host, double *re, double *im) {
+    if (nq < 1) return GDB_OK;
+    SqArgs a;
+    a.pos = pos;
+    a.orig = orig;
+    a.n = n;
+    a.nq = nq;
+    for (int d = 0; d < 3; d++) {
+        int lo = nvec_host[d], hi = nvec_host[d];
+        for (int q = 0; q < nq; q++) {
+            lo = nvec_host[3 * q + d] < lo ? nvec_host[3 * q + d] : lo;
+            hi = nvec_host[3 * q + d] > hi ? nvec_host[3 * q + d] : hi;
+        }
+        a.kmin[d] = lo;
+        a.klen[d] = hi - lo + 1;
+        a.invL[d] = 1.0f / box[d];
+    }
+    const int row = a.klen[0] + a.klen[1] + a.klen[2];
+    const size_t smem = (size_t)SQ_TILE * row * sizeof(float2);
+    if (smem > 200 * 1024) return aset(h, GDB_ERR_ARG, "sq: n_vectors span too wide");
+    int *dn = nullptr;
+    float *dff = nullptr;
+    double *acc = nullptr;
+    ACK(cudaMallocAsync(&dn, (size_t)nq * 3 * sizeof(int), st));
+    ACK(cudaMallocAsync(&acc, (size_t)nq * 2 * sizeof(double), st));
+    ACK(cudaMemcpyAsync(dn, nvec_host, (size_t)nq * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
+    ACK(cudaMemsetAsync(acc, 0, (size_t)nq * 2 * sizeof(double), st));
+    double nf = 0.0;
+    if (ff_host) {
+        ACK(cudaMallocAsync(&dff, (size_t)n * sizeof(float), st));
+        ACK(cudaMemcpyAsync(dff, ff_host, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
+        for (int i = 0; i < n; i++) nf += ff_host[i];
+    } else {
+        nf = n;
+    }
+    a.nvec = dn;
+    a.ff = dff;
+    a.acc = acc;
+    ACK(cudaFuncSetAttribute(k_sq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    dim3 grid((nq + SQ_THREADS - 1) / SQ_THREADS, (n + SQ_CHUNK - 1) / SQ_CHUNK);
+    k_sq<<<grid, SQ_THREADS, smem, st>>>(a);
+    ACK(cudaGetLastError());
+    std::vector<double> tmp((size_t)nq * 2);
+    ACK(cudaMemcpyAsync(tmp.data(), acc, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACK(cudaFreeAsync(dn, st));
+    ACK(cudaFreeAsync(acc, st));
+    if (dff) ACK(cudaFreeAsync(dff, st));
+    ACK(cudaStreamSynchronize(st));
+    const double norm = 1.0 / sqrt(nf);
+    for (int q = 0; q < nq; q++) {
+        re[q] = tmp[2 * q] * norm;
+        im[q] = tmp[2 * q + 1] * norm;
+    }
+    return GDB_OK;
+}
+
+extern "C" {
+
+int gdb_rdf_update(gdb_sim *h, int bins, double r_max, uint64_t *out) {
+    if (!h || !out) return aset(h, GDB_ERR_ARG, "gdb_rdf_update: NULL argument");
+    if (!gdb_internal_uploaded(h)) return aset(h, GDB_ERR_STATE, "state not uploaded");
+    ACK(cudaSetDevice(gdb_internal_dev(h)));
+    return rdf_device(h, gdb_internal_stream(h), gdb_internal_pos(h), gdb_internal_n(h), gdb_internal_box(h),
+                      gdb_internal_ntypes(h), bins, r_max, out);
+}
+
+int gdb_sq_update(gdb_sim *h, int nq, const int32_t *n_vectors, const float *ff, double *rho_re, double *rho_im) {
+    if (!h || !n_vectors || !rho_re || !rho_im) return aset(h, GDB_ERR_ARG, "gdb_sq_update: NULL argument");
+    if (!gdb_internal_uploaded(h)) return aset(h, GDB_ERR_STATE, "state not uploaded");
+    ACK(cudaSetDevice(gdb_internal_dev(h)));
+    return sq_device(h, gdb_internal_stream(h), gdb_internal_pos(h), gdb_internal_orig(h), gdb_internal_n(h), ff,
+                     gdb_internal_box(h), nq, n_vectors, rho_re, rho_im);
+}
+
+int gdb_rdf_compute(int n, const float *r, const int32_t *ptype, const float box[3], int ntypes, int bins,
+                    double r_max, uint64_t *out) {
+    gdb_sim *h = nullptr;
+    if (n < 1 || !r || !box || !out || ntypes < 1) return aset(h, GDB_ERR_ARG, "gdb_rdf_compute: bad arguments");
+    if (ptype)
+        for (int i = 0; i < n; i++)
+            if (ptype[i] < 0 || ptype[i] >= ntypes) return aset(h, GDB_ERR_ARG, "gdb_rdf_compute: type out of range");
+    cudaStream_t st;
+    ACK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    float *dr = nullptr;
+    int *dpt = nullptr, *orig = nullptr;
+    float4 *pos = nullptr;
+    int rc = GDB_OK;
+    do {
+        cudaError_t e;
+        if ((e = cudaMallocAsync(&dr, (size_t)n * 3 * sizeof(float), st)) ||
+            (e = cudaMallocAsync(&pos, (size_t)n * sizeof(float4), st)) ||
+            (e = cudaMallocAsync(&orig, (size_t)n * sizeof(int), st)) ||
+            (ptype && (e = cudaMallocAsync(&dpt, (size_t)n * sizeof(int), st))) ||
+            (e = cudaMemcpyAsync(dr, r, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, st)) ||
+            (ptype && (e = cudaMemcpyAsync(dpt, ptype, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st)))) {
+            rc = aset(h, GDB_ERR_CUDA, "gdb_rdf_compute: staging", e);
+            break;
+        }
+        k_pack_pos<<<(n + 255) / 256, 256, 0, st>>>(n, dr, dpt, pos, orig);
+        rc = rdf_device(h, st, pos, n, box, ntypes, bins, r_max, out);
+    } while (0);
+    if (dr) cudaFreeAsync(dr, st);
+    if (pos) cudaFreeAsync(pos, st);
+    if (orig) cudaFreeAsync(orig, st);
+    if (dpt) cudaFreeAsync(dpt, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], int nq, const int32_t *n_vectors,
+                   double *rho_re, double *rho_im) {
+    gdb_sim *h = nullptr;
+    if (n < 1 || !r || !box || !n_vectors || !rho_re || !rho_im) return aset(h, GDB_ERR_ARG, "gdb_sq_compute: bad arguments");
+    cudaStream_t st;
+    ACK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    float *dr = nullptr;
+    int *orig = nullptr;
+    float4 *pos = nullptr;
+    int rc = GDB_OK;
+    do {
+        cudaError_t e;
+        if ((e = cudaMallocAsync(&dr, (size_t)n * 3 * sizeof(float), st)) ||
+            (e = cudaMallocAsync(&pos, (size_t)n * sizeof(float4), st)) ||
+            (e = cudaMallocAsync(&orig, (size_t)n * sizeof(int), st)) ||
+            (e = cudaMemcpyAsync(dr, r, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, st))) {
+            rc = aset(h, GDB_ERR_CUDA, "gdb_sq_compute: staging", e);
+            break;
+        }
+        k_pack_pos<<<(n + 255) / 256, 256, 0, st>>>(n, dr, nullptr, pos, orig);
+        rc = sq_device(h, st, pos, orig, n, ff, box, nq, n_vectors, rho_re, rho_im);
+    } while (0);
+    if (dr) cudaFreeAsync(dr, st);
+    if (pos) cudaFreeAsync(pos, st);
+    if (orig) cudaFreeAsync(orig, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,202 @@
+/*
+ * gamdb200.h -- C ABI of libgamdb200.so, the B200 (sm_100a) implementation of
+ * gamdpy's simulation hot path: pair-potential forces/virial/energy over a
+ * neighbour list (N-squared or cell-list build), the NVE leapfrog and NVT
+ * Nose-Hoover steps, the ScalarSaver/MomentumReset runtime actions, and the
+ * radial-distribution and structure-factor calculators.
+ *
+ * Plain C: opaque handles, host pointers and sizes, int status codes
+ * (GDB_OK == 0).  No torch or CUDA types appear in the signatures.  A handle
+ * owns all of its device memory and one CUDA stream; calls on one handle must
+ * come from one host thread at a time.
+ *
+ * Host arrays use gamdpy's layout (gamdpy/configuration/Configuration.py:
+ * 141-146, colarray.py:45): positions/velocities/forces (N, 3) float32 row
+ * major, masses (N,) float32, types (N,) int32, images (N, 3) int32, all in
+ * the user's particle order.  Internally particles are kept in cell order
+ * (cell-list mode); every download returns the user's order.
+ *
+ * Each entry point names the reference interface it replaces (paths relative
+ * to the gamdpy project root).
+ */
+#ifndef GAMDB200_H
+#define GAMDB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GDB_OK 0
+#define GDB_ERR_ARG 1      /* bad argument (shape, kind, NULL handle) */
+#define GDB_ERR_CUDA 2     /* a CUDA runtime call failed; see gdb_get_last_error */
+#define GDB_ERR_STATE 3    /* call order (e.g. run before upload) */
+#define GDB_ERR_NBLIST 4   /* neighbour-list overflow (count >= max_nbs) */
+#define GDB_ERR_NUMERIC 5  /* non-finite position seen by a kernel */
+#define GDB_ERR_UNSUPPORTED 6
+
+/* status-word bits (gdb_status_word), set by kernels, cleared by gdb_clear_status */
+#define GDB_STATUS_NBLIST_OVERFLOW 0x1u
+#define GDB_STATUS_BARRIER_TIMEOUT 0x2u
+#define GDB_STATUS_NAN 0x4u
+#define GDB_STATUS_BAD_ARG 0x8u
+
+/* potentials: gamdpy/interactions/potential_functions/ */
+#define GDB_POT_LJ_SIGMA_EPSILON 0 /* LJ_12_6_sigma_epsilon.py:6-36, params (sigma, epsilon, cut) */
+#define GDB_POT_LJ_12_6 1          /* LJ_12_6.py:3-41, params (A12, A6, cut) */
+/* cutoff wrappers */
+#define GDB_CUT_SHIFTED_FORCE 0     /* apply_shifted_force_cutoff.py:30-37 */
+#define GDB_CUT_SHIFTED_POTENTIAL 1 /* apply_shifted_potential_cutoff.py:42-47 */
+/* neighbour lists */
+#define GDB_NBLIST_NSQ 0   /* interactions/nblist.py NbList2 */
+#define GDB_NBLIST_CELLS 1 /* interactions/nblist_linked_lists.py NbListLinkedLists */
+/* integrators */
+#define GDB_INTEGRATOR_NVE 0 /* integrators/NVE.py */
+#define GDB_INTEGRATOR_NVT 1 /* integrators/NVT.py */
+/* NVT target temperature T(t): misc/make_function.py */
+#define GDB_TFUNC_CONSTANT 0 /* make_function_constant :6-13, tparams = {T} */
+#define GDB_TFUNC_RAMP 1     /* make_function_ramp :16-34, tparams = {T0, t0, T1, t1} */
+
+/* column order of gdb_get_scalar_rows: sums over particles per saved step */
+#define GDB_SCALAR_U 0
+#define GDB_SCALAR_W 1
+#define GDB_SCALAR_LAPU 2
+#define GDB_SCALAR_K 3
+#define GDB_SCALAR_FSQ 4
+#define GDB_NUM_SCALARS 5
+
+typedef struct gdb_sim gdb_sim;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int gdb_version(void);
+
+/* Number of visible CUDA devices. */
+int gdb_device_count(int *count);
+
+/* Create a simulation of n particles and ntypes particle types on `device`.
+ * Replaces Configuration.copy_to_device's allocations and the per-object
+ * cuda.to_device calls of PairPotential/NbList/integrators
+ * (configuration/Configuration.py:227-234, interactions/nblist.py:14-18). */
+int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out);
+int gdb_sim_destroy(gdb_sim *h);
+
+/* Orthorhombic box lengths (simulation_boxes/orthorhombic.py:25-29). */
+int gdb_set_box(gdb_sim *h, const float lengths[3]);
+
+/* Host -> device copy of the full state (Configuration.copy_to_device,
+ * configuration/Configuration.py:227-234).  r_im may be NULL (zeros).
+ * Marks the neighbour list for rebuild. */
+int gdb_upload_state(gdb_sim *h, const float *r, const float *v, const float *m, const int32_t *ptype,
+                     const int32_t *r_im);
+
+/* Device -> host copy (Configuration.copy_to_host, Configuration.py:236-243).
+ * Any pointer may be NULL.  Synchronises the handle's stream. */
+int gdb_download_state(gdb_sim *h, float *r, float *v, float *f, int32_t *r_im);
+
+/* Per-particle scalars of the last force evaluation / integration step in
+ * gamdpy's columns (Configuration.py:109-131).  Any pointer may be NULL. */
+int gdb_download_scalars(gdb_sim *h, float *U, float *W, float *lapU, float *K, float *Fsq);
+
+/* Pair potential table (PairPotential.convert_user_params,
+ * interactions/pair_potential.py:23-51): params is ntypes*ntypes rows of
+ * nparams float32 (row-major [i][j][p]); the last parameter is the cut. */
+int gdb_set_pair_potential(gdb_sim *h, int kind, int cutmode, int ntypes, const float *params, int nparams);
+
+/* Neighbour-list algorithm, skin and capacity (PairPotential.get_params,
+ * pair_potential.py:84-97; compute_plan['nblist'], ['skin']). */
+int gdb_set_nblist(gdb_sim *h, int kind, float skin, int max_nbs);
+
+/* Threads per particle (compute_plan['tp'], simulation/get_default_compute_plan.py:55-63)
+ * and particles per thread block (compute_plan['pb']).  0 = choose. */
+int gdb_set_plan(gdb_sim *h, int tp, int pb);
+
+/* Integrators: NVE.get_params (integrators/NVE.py:29-31);
+ * NVT.get_params (integrators/NVT.py:33-37). */
+int gdb_set_integrator_nve(gdb_sim *h, float dt);
+int gdb_set_integrator_nvt(gdb_sim *h, float dt, float tau, int tfunc, const float *tparams);
+/* NVT.thermostat_state = {xi, sumK} (integrators/NVT.py:30). */
+int gdb_get_thermostat_state(gdb_sim *h, float state[2]);
+int gdb_set_thermostat_state(gdb_sim *h, const float state[2]);
+
+/* Runtime actions compiled into the step: ScalarSaver(steps_between_output)
+ * (runtime_actions/scalar_saver.py:270-304) and MomentumReset(steps_between_reset)
+ * (runtime_actions/momentum_reset.py:400-408); 0 disables. */
+int gdb_set_runtime_actions(gdb_sim *h, int scalar_every, int momentum_every);
+
+/* ConfigurationSaver (runtime_actions/configuration_saver.py:21-141): keep
+ * positions and images at steps 0, 1, 2, 4, ..., 2^k of every timeblock
+ * (log-spaced, taken before that step's integration) in conf_per_block frames
+ * of layout (conf_per_block, 2, n, 3) float32 = {r, r_im as float} in user
+ * order.  conf_per_block = int(log2(steps_per_timeblock)) + 2; 0 disables. */
+int gdb_set_configuration_saver(gdb_sim *h, int conf_per_block);
+/* Frames saved during the last timeblock (same layout as above). */
+int gdb_get_saved_configurations(gdb_sim *h, float *out, int conf_per_block);
+
+/* One evaluation of the interactions on the current state: neighbour-list
+ * check/rebuild, then forces, U, W, lapU (Evaluator.evaluate,
+ * tools/Evaluator.py:82-94; interactions/pair_potential.py:250-268). */
+int gdb_eval_forces(gdb_sim *h);
+
+/* One timeblock: `steps` integration steps plus the final force evaluation
+ * (simulation/Simulation.py:306-346 via integrate_self :271-282).  time_zero
+ * is the simulated time at the block start.  Returns GDB_ERR_NBLIST on
+ * overflow and GDB_ERR_NUMERIC on non-finite positions.  If ms != NULL the
+ * block's device time (CUDA events) is stored there. */
+int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms);
+
+/* Measurement: build a list for the current state, then launch the fused
+ * step kernel `reps` times alone (no rebuild chain, runtime actions off)
+ * between CUDA events on the handle's stream; *ms_per_launch = average
+ * duration.  Advances the state; intended for benchmarks (the reference
+ * times whole timeblocks with CUDA events, simulation/Simulation.py:404-448). */
+int gdb_time_step_kernel(gdb_sim *h, int reps, float *ms_per_launch);
+
+/* Mean and maximum neighbour count of the current list (per particle). */
+int gdb_nblist_stats(gdb_sim *h, double *mean_count, int *max_count);
+
+/* ScalarSaver rows of the last timeblock: rows x GDB_NUM_SCALARS doubles
+ * (sums over particles, float64).  rows = steps / scalar_every. */
+int gdb_get_scalar_rows(gdb_sim *h, double *out, int rows);
+
+/* Neighbour list in gamdpy's layout (interactions/nblist.py:8): (n, max_nbs+1)
+ * int32, user indices, count in the last column. */
+int gdb_get_nblist(gdb_sim *h, int32_t *out, int max_nbs);
+
+/* gamdpy's nbflag (nblist.py:9): {update pending, max count if overflowed
+ * else 0, number of rebuilds}. */
+int gdb_get_nbflag(gdb_sim *h, int32_t out[3]);
+
+/* Status bits set by kernels since the last clear; gdb_clear_status resets. */
+uint32_t gdb_status_word(gdb_sim *h);
+int gdb_clear_status(gdb_sim *h);
+
+/* Last error message of the handle (or of the library when h == NULL). */
+int gdb_get_last_error(gdb_sim *h, char *buf, int n);
+
+/* Radial distribution counts of the current state, added into out
+ * (ntypes x ntypes x bins uint64, exact integer counts).  r_max <= 0 means
+ * min(L)/2, the reference's range (calculators/calculator_radial_distribution.py:
+ * 76-107, update :111-119). */
+int gdb_rdf_update(gdb_sim *h, int bins, double r_max, uint64_t *out);
+
+/* Collective density of the current state for q = 2 pi n / L
+ * (calculators/calculator_structure_factor.py:131-156 GPU kernel, :185-203
+ * CPU backends): rho_q = N_f^-1/2 sum_i f_i exp(i q.r_i), N_f = sum f_i.
+ * n_vectors: nq x 3 int32; ff: n float32 in user order or NULL (all 1). */
+int gdb_sq_update(gdb_sim *h, int nq, const int32_t *n_vectors, const float *ff, double *rho_re,
+                  double *rho_im);
+
+/* Stand-alone calculators on host arrays (no handle): same semantics as the
+ * two calls above, for callers that only hold a configuration
+ * (CalculatorRadialDistribution.update / CalculatorStructureFactor.update). */
+int gdb_rdf_compute(int n, const float *r, const int32_t *ptype, const float box[3], int ntypes, int bins,
+                    double r_max, uint64_t *out);
+int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], int nq, const int32_t *n_vectors,
+                   double *rho_re, double *rho_im);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

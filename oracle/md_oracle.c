@@ -1,0 +1,522 @@
+/*
+ * md_oracle.c -- CPU restatement of gamdpy's simulation hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library in
+ * gamdpy_b200/csrc: only tests/, __graft_entry__.smoke() and bench.py's
+ * cpu_baseline / --impl reference leg may load it.  The product path never
+ * calls it and has no CPU fallback.
+ *
+ * Every function restates one piece of the reference (gamdpy, pure Python +
+ * numba) and cites the file:line it follows, relative to the gamdpy project
+ * root.  Arithmetic is float32 where gamdpy's numba kernels are float32 and
+ * float64 where numba's typing rules promote (Python int/float literals mixed
+ * with float32 give float64 under numba).  Compile with -ffp-contract=off so
+ * that no multiply-add is fused implicitly; the one place where the GPU build
+ * of gamdpy may fuse (the distance accumulation) is selected explicitly by the
+ * `fma` argument.
+ *
+ * Parity of this restatement is pinned against outputs of gamdpy itself run
+ * on the CPU (the .npz fixtures in tests/golden, generated by tests/golden/make_golden.py).
+ *
+ * Reductions the reference does with float32 atomics (ScalarSaver sums, the
+ * Nose-Hoover kinetic-energy sum) are accumulated here in float64 in a fixed
+ * order; the CUDA library does the same, so both are run-to-run deterministic.
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define ORC_POT_LJ_SIGMA_EPSILON 0 /* potential_functions/LJ_12_6_sigma_epsilon.py:6-36 */
+#define ORC_POT_LJ_12_6 1          /* potential_functions/LJ_12_6.py:3-41 */
+#define ORC_CUT_SF 0               /* apply_shifted_force_cutoff.py:30-37 */
+#define ORC_CUT_SP 1               /* apply_shifted_potential_cutoff.py:42-47 */
+#define ORC_CUT_NONE 2             /* potential used unwrapped */
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+void orc_set_num_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}
+
+/* numba lowers `x ** k` with an integer literal k by binary exponentiation in
+ * the operand's type (numba/cpython/numbers.py static_power_impl); this is
+ * that loop for float32. */
+static float powi_f32(float a, int k) {
+    float result = 1.0f;
+    while (k) {
+        if (k & 1) result = result * a;
+        a = a * a;
+        k >>= 1;
+    }
+    return result;
+}
+
+/* LJ_12_6_sigma_epsilon.py:26-36: params (sigma, epsilon, ...). */
+static void lj_sigma_epsilon(float dist, const float *p, float *u, float *s, float *umm) {
+    float sigma = p[0], epsilon = p[1];
+    float OneOdist = 1.0f / dist;
+    float sigmaOdist = sigma * OneOdist;
+    float x12 = powi_f32(sigmaOdist, 12), x6 = powi_f32(sigmaOdist, 6);
+    float o2 = powi_f32(OneOdist, 2);
+    *u = 4.0f * epsilon * (x12 - x6);
+    *s = 24.0f * epsilon * (2.0f * x12 - x6) * o2;
+    *umm = 24.0f * epsilon * (26.0f * x12 - 7.0f * x6) * o2;
+}
+
+/* LJ_12_6.py:71-78: params (A12, A6, ...). */
+static void lj_12_6(float dist, const float *p, float *u, float *s, float *umm) {
+    float A12 = p[0], A6 = p[1];
+    float inv = 1.0f / dist;
+    *u = A12 * powi_f32(inv, 12) + A6 * powi_f32(inv, 6);
+    *s = 12.0f * A12 * powi_f32(inv, 14) + 6.0f * A6 * powi_f32(inv, 8);
+    *umm = 156.0f * A12 * powi_f32(inv, 14) + 42.0f * A6 * powi_f32(inv, 8);
+}
+
+static void raw_pot(int kind, float dist, const float *p, float *u, float *s, float *umm) {
+    if (kind == ORC_POT_LJ_12_6) lj_12_6(dist, p, u, s, umm);
+    else lj_sigma_epsilon(dist, p, u, s, umm);
+}
+
+/* Cutoff wrappers.  The cut is the last parameter (params[-1]); np = number
+ * of parameters including the cut.
+ *   SF: apply_shifted_force_cutoff.py:30-37   u -= u_c - s_c*cut*(r-cut); s -= s_c
+ *   SP: apply_shifted_potential_cutoff.py:42-47  u -= u_c
+ * Both re-evaluate the potential at the cut on every call, as the reference. */
+void orc_pair_potential(int kind, int cutmode, float dist, const float *p, int np, float out[3]) {
+    float u, s, umm;
+    raw_pot(kind, dist, p, &u, &s, &umm);
+    if (cutmode != ORC_CUT_NONE) {
+        float cut = p[np - 1];
+        float uc, sc, ummc;
+        raw_pot(kind, cut, p, &uc, &sc, &ummc);
+        if (cutmode == ORC_CUT_SF) {
+            u -= uc - sc * cut * (dist - cut);
+            s -= sc;
+        } else {
+            u -= uc;
+        }
+    }
+    out[0] = u;
+    out[1] = s;
+    out[2] = umm;
+}
+
+/* simulation_boxes/orthorhombic.py:43-57 (dist_sq_dr_function) and :59-73
+ * (dist_sq_function): dr = ri - rj, minimum image via 2*dr vs +-L, and
+ * dist_sq accumulated in k order.  fma=1 evaluates the accumulation as
+ * fmaf(dr, dr, dist_sq), the form libNVVM produces with its default
+ * contraction; fma=0 rounds the product first (numba on the CPU). */
+static inline float dist_sq_dr(const float *ri, const float *rj, const float *box, float *dr, int fma) {
+    float dsq = 0.0f;
+    for (int k = 0; k < 3; k++) {
+        float d = ri[k] - rj[k];
+        float L = box[k];
+        d += (2.0f * d > L) ? -L : ((2.0f * d < -L) ? L : 0.0f);
+        if (dr) dr[k] = d;
+        if (fma) dsq = fmaf(d, d, dsq);
+        else {
+            float p = d * d;
+            dsq = dsq + p;
+        }
+    }
+    return dsq;
+}
+
+float orc_dist_sq(const float *ri, const float *rj, const float *box, float *dr, int fma) {
+    return dist_sq_dr(ri, rj, box, dr, fma);
+}
+
+/* orthorhombic.py:75-86 */
+void orc_apply_pbc(float *r, int *img, const float *box) {
+    for (int k = 0; k < 3; k++) {
+        if (r[k] * 2.0f > box[k]) { r[k] -= box[k]; img[k] += 1; }
+        if (r[k] * 2.0f < -box[k]) { r[k] += box[k]; img[k] -= 1; }
+    }
+}
+
+/* nblist.py:88-127 (NbList2.nblist_update, full list, no exclusions):
+ * j != i and dist_sq < (max_cut+skin)^2.  Output in gamdpy's layout: row i of
+ * nbl (n x (max_nbs+1)) holds the neighbours, the count is in the last column.
+ * Neighbours are appended in ascending j (the reference's order is set by
+ * atomics and is not deterministic; only the set is compared).
+ * Returns the largest count seen (overflow when >= max_nbs, nblist.py:140). */
+int orc_nblist_nsq(int n, const float *r, const float *box, float cut_plus_skin, int max_nbs,
+                   int32_t *nbl, int fma) {
+    int maxcount = 0;
+    const float cps2 = cut_plus_skin * cut_plus_skin;
+#pragma omp parallel for schedule(dynamic, 16) reduction(max : maxcount)
+    for (int i = 0; i < n; i++) {
+        int32_t *row = nbl + (size_t)i * (max_nbs + 1);
+        int c = 0;
+        for (int j = 0; j < n; j++) {
+            if (j == i) continue;
+            float d2 = dist_sq_dr(r + 3 * (size_t)j, r + 3 * (size_t)i, box, NULL, fma);
+            if (d2 < cps2) {
+                if (c < max_nbs) row[c] = j;
+                c++;
+            }
+        }
+        row[max_nbs] = c;
+        if (c > maxcount) maxcount = c;
+    }
+    return maxcount;
+}
+
+/* nblist_linked_lists.py:36-42: cells per dimension = int(L / ((max_cut+skin)/2)),
+ * asserted > 4 (and > 6 in x).  Returns 0 and fills nc, or -1 when the assert
+ * of the reference would fail. */
+int orc_cells_per_dimension(const float *box, float max_cut, float skin, int *nc) {
+    /* max_cut and skin are np.float32 (pair_potential.py:49, compute_plan);
+     * (max_cut + skin)/2 is float32 arithmetic divided by a Python int ->
+     * numpy float32 on the host; lengths[i] / that -> float32; int() truncates. */
+    float min_cell = (max_cut + skin) / 2.0f;
+    for (int k = 0; k < 3; k++) {
+        float q = box[k] / min_cell;
+        nc[k] = (int)q;
+        if (nc[k] <= 4) return -1;
+        if (k == 0 && nc[k] <= 6) return -1;
+    }
+    return 0;
+}
+
+/* nblist_linked_lists.py:127: cell = int(floor((x + 0.5*L) * nc / L)) % nc.
+ * 0.5 is a float64 literal, so numba evaluates the whole expression in
+ * float64; % on integers follows Python (result has the divisor's sign). */
+static inline int cell_coord(float x, float L, int nc) {
+    double v = ((double)x + 0.5 * (double)L) * (double)nc / (double)L;
+    long long c = (long long)floor(v);
+    long long m = c % nc;
+    if (m < 0) m += nc;
+    return (int)m;
+}
+
+void orc_cell_coords(int n, const float *r, const float *box, const int *nc, int32_t *cells_out) {
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) cells_out[3 * i + k] = cell_coord(r[3 * i + k], box[k], nc[k]);
+}
+
+/* NbListLinkedLists: put_particles_in_cells (nblist_linked_lists.py:117-131)
+ * pushes every particle on the head of its cell's chain; the build
+ * (:133-183) walks a 5x5x5 stencil of cells and the chains in them; clear
+ * (:196-218) resets.  The chain order of the reference depends on atomics;
+ * here particles are pushed in ascending index, so each chain is in
+ * descending index.  Only the per-particle sets are compared.  Returns the
+ * largest count, or -1 if the cell grid fails the reference's asserts. */
+int orc_nblist_cells(int n, const float *r, const float *box, float max_cut, float skin, int max_nbs,
+                     int32_t *nbl, int fma) {
+    int nc[3];
+    if (orc_cells_per_dimension(box, max_cut, skin, nc) != 0) return -1;
+    size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+    int32_t *head = (int32_t *)malloc(ncell * sizeof(int32_t));
+    int32_t *next = (int32_t *)malloc((size_t)n * sizeof(int32_t));
+    int32_t *mc = (int32_t *)malloc((size_t)n * 3 * sizeof(int32_t));
+    for (size_t c = 0; c < ncell; c++) head[c] = -1;
+    for (int i = 0; i < n; i++) {
+        for (int k = 0; k < 3; k++) mc[3 * i + k] = cell_coord(r[3 * i + k], box[k], nc[k]);
+        size_t idx = ((size_t)mc[3 * i] * nc[1] + mc[3 * i + 1]) * nc[2] + mc[3 * i + 2];
+        next[i] = head[idx];
+        head[idx] = i;
+    }
+    const float cut_plus_skin = max_cut + skin;
+    const float cps2 = cut_plus_skin * cut_plus_skin;
+    int maxcount = 0;
+#pragma omp parallel for schedule(dynamic, 64) reduction(max : maxcount)
+    for (int i = 0; i < n; i++) {
+        int32_t *row = nbl + (size_t)i * (max_nbs + 1);
+        int c = 0;
+        for (int ix = -2; ix < 3; ix++)
+            for (int iy = -2; iy < 3; iy++)
+                for (int iz = -2; iz < 3; iz++) {
+                    int cx = ((mc[3 * i] + ix) % nc[0] + nc[0]) % nc[0];
+                    int cy = ((mc[3 * i + 1] + iy) % nc[1] + nc[1]) % nc[1];
+                    int cz = ((mc[3 * i + 2] + iz) % nc[2] + nc[2]) % nc[2];
+                    int j = head[((size_t)cx * nc[1] + cy) * nc[2] + cz];
+                    while (j >= 0) {
+                        if (j != i) {
+                            float d2 = dist_sq_dr(r + 3 * (size_t)j, r + 3 * (size_t)i, box, NULL, fma);
+                            if (d2 < cps2) {
+                                c++;
+                                if (c < max_nbs) row[c - 1] = j;
+                            }
+                        }
+                        j = next[j];
+                    }
+                }
+        row[max_nbs] = c;
+        if (c > maxcount) maxcount = c;
+    }
+    free(head);
+    free(next);
+    free(mc);
+    return maxcount;
+}
+
+/* pair_potential.py:164-178 (full-list pairpotential_calculator) inside
+ * calc_forces (:185-246): for each listed neighbour j with
+ * dist_sq < cut_ij^2: f_i -= dr*s; W_i += dr_k^2*s*(0.5/D); U_i += u/2;
+ * lapU_i += (1-D)*s + umm.  Per-particle sums are float32 in list order.
+ * params: nt*nt rows of np floats (last = cut).  Any output pointer may be
+ * NULL.  Fsq (a scalar the integrator computes, NVE.py:79-80) is returned
+ * for the forces just computed if fsq != NULL. */
+void orc_forces(int n, const float *r, const int32_t *ptype, const float *box, const float *params,
+                int np, int nt, int kind, int cutmode, const int32_t *nbl, int max_nbs, float *f,
+                float *U, float *W, float *lapU, float *fsq, int fma) {
+    const float virial_factor = 0.5f / 3.0f; /* numba.float32(0.5/D) */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) {
+        const int32_t *row = nbl + (size_t)i * (max_nbs + 1);
+        int cnt = row[max_nbs];
+        if (cnt > max_nbs) cnt = max_nbs;
+        int ti = ptype ? ptype[i] : 0;
+        float fi[3] = {0.0f, 0.0f, 0.0f};
+        float u_i = 0.0f, w_i = 0.0f, l_i = 0.0f;
+        for (int a = 0; a < cnt; a++) {
+            int j = row[a];
+            int tj = ptype ? ptype[j] : 0;
+            const float *p = params + ((size_t)ti * nt + tj) * np;
+            float cut = p[np - 1];
+            float dr[3];
+            float d2 = dist_sq_dr(r + 3 * (size_t)j, r + 3 * (size_t)i, box, dr, fma);
+            if (d2 < cut * cut) {
+                float o[3];
+                orc_pair_potential(kind, cutmode, sqrtf(d2), p, np, o);
+                float s = o[1];
+                for (int k = 0; k < 3; k++) {
+                    fi[k] = fi[k] - dr[k] * s;
+                    w_i += dr[k] * dr[k] * s * virial_factor;
+                }
+                u_i += 0.5f * o[0];
+                l_i += (1.0f - 3.0f) * s + o[2];
+            }
+        }
+        if (f) for (int k = 0; k < 3; k++) f[3 * (size_t)i + k] = fi[k];
+        if (U) U[i] = u_i;
+        if (W) W[i] = w_i;
+        if (lapU) lapU[i] = l_i;
+        if (fsq) fsq[i] = fi[0] * fi[0] + fi[1] * fi[1] + fi[2] * fi[2];
+    }
+}
+
+/* integrators/NVE.py:59-105: leapfrog; K from the mean of the two half-step
+ * velocities; PBC with image counters.  m is per particle. */
+void orc_nve_step(int n, float *r, float *v, const float *f, const float *m, int32_t *img, const float *box,
+                  float dt, float *K, float *fsq) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) {
+        float my_m = m[i];
+        float k_i = 0.0f, fsq_i = 0.0f;
+        for (int k = 0; k < 3; k++) {
+            float fk = f[3 * (size_t)i + k];
+            fsq_i += fk * fk;
+            float v_mean = 0.0f;
+            v_mean += v[3 * (size_t)i + k];
+            v[3 * (size_t)i + k] += fk / my_m * dt;
+            v_mean += v[3 * (size_t)i + k];
+            v_mean /= 2.0f;
+            k_i += 0.5f * my_m * v_mean * v_mean;
+            r[3 * (size_t)i + k] += v[3 * (size_t)i + k] * dt;
+        }
+        orc_apply_pbc(r + 3 * (size_t)i, img + 3 * (size_t)i, box);
+        if (K) K[i] = k_i;
+        if (fsq) fsq[i] = fsq_i;
+    }
+}
+
+/* integrators/NVT.py:188-224 (step) and :226-237 (update_thermostat_state).
+ * state[0] = xi (float32), the kinetic-energy sum is returned in float64
+ * (the reference accumulates it with float32 atomics into state[1]).
+ * Returns sum_i K_i. */
+double orc_nvt_step(int n, float *r, float *v, const float *f, const float *m, int32_t *img, const float *box,
+                    float dt, float xi, float *K, float *fsq) {
+    float factor = 0.5f * xi * dt;
+    float plus = 1.0f / (1.0f + factor);
+    float minus = 1.0f - factor;
+    double ksum = 0.0;
+    float *kbuf = (float *)malloc((size_t)n * sizeof(float));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) {
+        float my_m = m[i];
+        float k_i = 0.0f, fsq_i = 0.0f;
+        for (int k = 0; k < 3; k++) {
+            float fk = f[3 * (size_t)i + k];
+            fsq_i += fk * fk;
+            float vk = v[3 * (size_t)i + k];
+            vk = plus * (minus * vk + fk / my_m * dt);
+            v[3 * (size_t)i + k] = vk;
+            k_i += 0.5f * my_m * vk * vk;
+            r[3 * (size_t)i + k] += vk * dt;
+        }
+        orc_apply_pbc(r + 3 * (size_t)i, img + 3 * (size_t)i, box);
+        kbuf[i] = k_i;
+        if (K) K[i] = k_i;
+        if (fsq) fsq[i] = fsq_i;
+    }
+    for (int i = 0; i < n; i++) ksum += kbuf[i];
+    free(kbuf);
+    return ksum;
+}
+
+/* NVT.py:231-236: ke_deviation = 2*sumK/(degrees*T) - 1 (float64 under
+ * numba: degrees is an int64), xi += dt*omega2*ke_deviation stored float32. */
+float orc_nvt_thermostat_update(float xi, double ksum, float dt, float omega2, long long degrees, float T) {
+    double ke_dev = 2.0 * ksum / ((double)degrees * (double)T) - 1.0;
+    double nx = (double)xi + (double)(dt * omega2) * ke_dev;
+    return (float)nx;
+}
+
+/* runtime_actions/momentum_reset.py:372-393: v -= (sum m v)/(sum m). */
+void orc_momentum_reset(int n, float *v, const float *m) {
+    double p[3] = {0, 0, 0}, M = 0;
+    for (int i = 0; i < n; i++) {
+        for (int k = 0; k < 3; k++) p[k] += (double)m[i] * v[3 * (size_t)i + k];
+        M += m[i];
+    }
+    float vcm[3];
+    for (int k = 0; k < 3; k++) vcm[k] = (float)(p[k] / M);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < 3; k++) v[3 * (size_t)i + k] -= vcm[k];
+}
+
+/*
+ * One timeblock of the composed step loop (simulation/Simulation.py:330-346,
+ * the kernel-launch form of :306-328): for step in 0..steps:
+ *   neighbour-list check (nblist.py:57-86 / nblist_linked_lists.py:84-115)
+ *   and rebuild; forces; if step < steps: integrate, then post-step actions
+ *   ScalarSaver (scalar_saver.py:270-304) and MomentumReset
+ *   (momentum_reset.py:400-408) in that order.
+ *
+ * integrator: 0 = NVE, 1 = NVT.  nvt_state[0] = xi (in/out).
+ * nblist_kind: 0 = N squared, 1 = linked lists.  r_ref / have_list carry the
+ * list state across calls (have_list = 0 forces a build).
+ * scal_out: (steps/every) x 4 doubles: U, W, K, lapU sums per saved step
+ * (every = 0 disables saving).  Returns the number of rebuilds, or -1 on a
+ * cell-grid error, -2 on neighbour-list overflow.
+ */
+int orc_run_timeblock(int n, float *r, float *v, float *f, const float *m, int32_t *img, const int32_t *ptype,
+                      const float *box, const float *params, int np, int nt, int kind, int cutmode,
+                      int nblist_kind, float skin, int max_nbs, int32_t *nbl, float *r_ref, int *have_list,
+                      int integrator, float dt, float *nvt_state, float omega2, float T, int steps, int every,
+                      int reset_every, float *U, float *W, float *K, double *scal_out, int fma) {
+    float max_cut = 0.0f;
+    for (int a = 0; a < nt * nt; a++)
+        if (params[(size_t)a * np + np - 1] > max_cut) max_cut = params[(size_t)a * np + np - 1];
+    int rebuilds = 0;
+    long long degrees = 3LL * n - 3;
+    float *lap = (float *)malloc((size_t)n * sizeof(float));
+    for (int step = 0; step <= steps; step++) {
+        int need = !*have_list;
+        if (!need) {
+            for (int i = 0; i < n && !need; i++) {
+                float d2 = dist_sq_dr(r + 3 * (size_t)i, r_ref + 3 * (size_t)i, box, NULL, fma);
+                if (d2 > skin * skin * 0.25f) need = 1;
+            }
+        }
+        if (need) {
+            int mx;
+            if (nblist_kind == 0) mx = orc_nblist_nsq(n, r, box, max_cut + skin, max_nbs, nbl, fma);
+            else mx = orc_nblist_cells(n, r, box, max_cut, skin, max_nbs, nbl, fma);
+            if (mx < 0) { free(lap); return -1; }
+            if (mx >= max_nbs) { free(lap); return -2; }
+            memcpy(r_ref, r, (size_t)n * 3 * sizeof(float));
+            *have_list = 1;
+            rebuilds++;
+        }
+        orc_forces(n, r, ptype, box, params, np, nt, kind, cutmode, nbl, max_nbs, f, U, W, lap, NULL, fma);
+        if (step < steps) {
+            if (integrator == 0) {
+                orc_nve_step(n, r, v, f, m, img, box, dt, K, NULL);
+            } else {
+                double ks = orc_nvt_step(n, r, v, f, m, img, box, dt, nvt_state[0], K, NULL);
+                nvt_state[0] = orc_nvt_thermostat_update(nvt_state[0], ks, dt, omega2, degrees, T);
+            }
+            if (every > 0 && step % every == 0) {
+                double su = 0, sw = 0, sk = 0, sl = 0;
+                for (int i = 0; i < n; i++) { su += U[i]; sw += W[i]; sk += K[i]; sl += lap[i]; }
+                double *row = scal_out + (size_t)(step / every) * 4;
+                row[0] = su; row[1] = sw; row[2] = sk; row[3] = sl;
+            }
+            if (reset_every > 0 && step % reset_every == 0) orc_momentum_reset(n, v, m);
+        }
+    }
+    free(lap);
+    return rebuilds;
+}
+
+/* calculators/calculator_radial_distribution.py:76-107: all ordered pairs
+ * i != j with dist_sq < (Lmin/2)^2 counted into bins[ti][tj][int(d/width)].
+ * numba types: min_box_dim float32; (min_box_dim/2)/bins float64; the
+ * comparison against (min_box_dim/2)**2 in float64; dist = sqrt(float32)
+ * in float32; d/width in float64.  Counts are exact integers. */
+void orc_rdf(int n, const float *r, const int32_t *ptype, const float *box, int nt, int bins, uint64_t *out,
+             int fma, double r_max) {
+    float minL = box[0] < box[1] ? box[0] : box[1];
+    minL = minL < box[2] ? minL : box[2];
+    /* r_max <= 0: the reference's range min(L)/2; otherwise a shorter range
+     * with the same arithmetic (used to check the library's cell search) */
+    double half = r_max > 0.0 ? r_max : (double)minL / 2.0;
+    double width = half / (double)bins;
+    double half_sq = half * half;
+    size_t tot = (size_t)nt * nt * bins;
+    memset(out, 0, tot * sizeof(uint64_t));
+#pragma omp parallel
+    {
+        uint64_t *loc = (uint64_t *)calloc(tot, sizeof(uint64_t));
+#pragma omp for schedule(dynamic, 16)
+        for (int i = 0; i < n; i++) {
+            int ti = ptype ? ptype[i] : 0;
+            for (int j = 0; j < n; j++) {
+                if (j == i) continue;
+                float d2 = dist_sq_dr(r + 3 * (size_t)j, r + 3 * (size_t)i, box, NULL, fma);
+                if ((double)d2 < half_sq) {
+                    float d = sqrtf(d2);
+                    if ((double)d < half) {
+                        long long b = (long long)((double)d / width);
+                        if (b >= bins) b = bins - 1;
+                        int tj = ptype ? ptype[j] : 0;
+                        loc[((size_t)ti * nt + tj) * bins + b] += 1;
+                    }
+                }
+            }
+        }
+#pragma omp critical
+        for (size_t a = 0; a < tot; a++) out[a] += loc[a];
+        free(loc);
+    }
+}
+
+/* calculators/calculator_structure_factor.py:185-196 ('CPU multi core'):
+ * rho_q = N_f^-1/2 sum_n f_n exp(i q.r_n), N_f = sum f_n.  Evaluated here
+ * in float64 throughout (the reference: float32 q.r, complex64 sums).
+ * ff may be NULL (all ones). */
+void orc_sq(int n, const float *r, const float *ff, int nq, const float *q, double *re, double *im) {
+    double nf = 0.0;
+    for (int i = 0; i < n; i++) nf += ff ? ff[i] : 1.0;
+    double norm = 1.0 / sqrt(nf);
+#pragma omp parallel for schedule(dynamic, 4)
+    for (int a = 0; a < nq; a++) {
+        double sr = 0.0, si = 0.0;
+        double qx = q[3 * a], qy = q[3 * a + 1], qz = q[3 * a + 2];
+        for (int i = 0; i < n; i++) {
+            double ph = qx * r[3 * (size_t)i] + qy * r[3 * (size_t)i + 1] + qz * r[3 * (size_t)i + 2];
+            double w = ff ? ff[i] : 1.0;
+            sr += w * cos(ph);
+            si += w * sin(ph);
+        }
+        re[a] = sr * norm;
+        im[a] = si * norm;
+    }
+}

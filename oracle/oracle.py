@@ -1,0 +1,229 @@
+"""ctypes front end of the CPU oracle (md_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()``
+and by ``bench.py``'s CPU-baseline leg, always as the checker or the timed CPU
+reference, never as part of the product path (gamdpy_b200 does not import it).
+
+Arrays follow gamdpy's host layout: positions (N, 3) float32, types (N,)
+int32, parameter tables (ntypes, ntypes, nparams) float32 with the cut last
+(gamdpy/interactions/pair_potential.py:40-47), neighbour lists (N, max_nbs+1)
+int32 with the count in the last column (gamdpy/interactions/nblist.py:8).
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+POT_LJ_SIGMA_EPSILON = 0
+POT_LJ_12_6 = 1
+CUT_SF = 0
+CUT_SP = 1
+CUT_NONE = 2
+
+_lib = None
+
+
+def build():
+    """Compile md_oracle.c into liboracle.so (make, in this directory)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        P = ctypes.c_void_p
+        i, f, d = ctypes.c_int, ctypes.c_float, ctypes.c_double
+        L.orc_num_threads.restype = i
+        L.orc_set_num_threads.argtypes = [i]
+        L.orc_pair_potential.argtypes = [i, i, f, P, i, P]
+        L.orc_dist_sq.argtypes = [P, P, P, P, i]
+        L.orc_dist_sq.restype = f
+        L.orc_apply_pbc.argtypes = [P, P, P]
+        L.orc_nblist_nsq.argtypes = [i, P, P, f, i, P, i]
+        L.orc_nblist_nsq.restype = i
+        L.orc_cells_per_dimension.argtypes = [P, f, f, P]
+        L.orc_cells_per_dimension.restype = i
+        L.orc_cell_coords.argtypes = [i, P, P, P, P]
+        L.orc_nblist_cells.argtypes = [i, P, P, f, f, i, P, i]
+        L.orc_nblist_cells.restype = i
+        L.orc_forces.argtypes = [i, P, P, P, P, i, i, i, i, P, i, P, P, P, P, P, i]
+        L.orc_nve_step.argtypes = [i, P, P, P, P, P, P, f, P, P]
+        L.orc_nvt_step.argtypes = [i, P, P, P, P, P, P, f, f, P, P]
+        L.orc_nvt_step.restype = d
+        L.orc_nvt_thermostat_update.argtypes = [f, d, f, f, ctypes.c_longlong, f]
+        L.orc_nvt_thermostat_update.restype = f
+        L.orc_momentum_reset.argtypes = [i, P, P]
+        L.orc_run_timeblock.argtypes = [i, P, P, P, P, P, P, P, P, i, i, i, i, i, f, i, P, P, P, i, f,
+                                        P, f, f, i, i, i, P, P, P, P, i]
+        L.orc_run_timeblock.restype = i
+        L.orc_rdf.argtypes = [i, P, P, P, i, i, P, i, d]
+        L.orc_sq.argtypes = [i, P, P, i, P, P, P]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def num_threads():
+    return lib().orc_num_threads()
+
+
+def set_num_threads(n):
+    lib().orc_set_num_threads(int(n))
+
+
+def param_table(params):
+    """gamdpy's user params [p0, p1, ..., cut] (scalars or ntypes x ntypes)
+    -> (nt, nt, np) float32 table (pair_potential.py:23-51)."""
+    mats = [np.atleast_2d(np.asarray(p, dtype=np.float32)) for p in params]
+    nt = max(m.shape[0] for m in mats)
+    mats = [np.broadcast_to(m, (nt, nt)) for m in mats]
+    return np.ascontiguousarray(np.stack(mats, axis=-1), dtype=np.float32)
+
+
+def pair_potential(dist, p, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF):
+    p = _f32(p)
+    out = np.zeros(3, np.float32)
+    lib().orc_pair_potential(kind, cutmode, float(dist), _p(p), len(p), _p(out))
+    return out
+
+
+def dist_sq(ri, rj, box, fma=0):
+    ri, rj, box = _f32(ri), _f32(rj), _f32(box)
+    dr = np.zeros(3, np.float32)
+    d2 = lib().orc_dist_sq(_p(ri), _p(rj), _p(box), _p(dr), fma)
+    return np.float32(d2), dr
+
+
+def apply_pbc(r, img, box):
+    r, img, box = _f32(r).copy(), _i32(img).copy(), _f32(box)
+    lib().orc_apply_pbc(_p(r), _p(img), _p(box))
+    return r, img
+
+
+def nblist_nsq(r, box, cut_plus_skin, max_nbs, fma=0):
+    r, box = _f32(r), _f32(box)
+    nbl = np.zeros((len(r), max_nbs + 1), np.int32)
+    mx = lib().orc_nblist_nsq(len(r), _p(r), _p(box), float(cut_plus_skin), max_nbs, _p(nbl), fma)
+    return nbl, mx
+
+
+def cells_per_dimension(box, max_cut, skin):
+    nc = np.zeros(3, np.int32)
+    ok = lib().orc_cells_per_dimension(_p(_f32(box)), float(max_cut), float(skin), _p(nc))
+    return nc if ok == 0 else None
+
+
+def cell_coords(r, box, nc):
+    r, box, nc = _f32(r), _f32(box), _i32(nc)
+    out = np.zeros((len(r), 3), np.int32)
+    lib().orc_cell_coords(len(r), _p(r), _p(box), _p(nc), _p(out))
+    return out
+
+
+def nblist_cells(r, box, max_cut, skin, max_nbs, fma=0):
+    r, box = _f32(r), _f32(box)
+    nbl = np.zeros((len(r), max_nbs + 1), np.int32)
+    mx = lib().orc_nblist_cells(len(r), _p(r), _p(box), float(max_cut), float(skin), max_nbs, _p(nbl), fma)
+    if mx == -1:
+        raise ValueError("cell grid too small (gamdpy asserts > 4 cells per dimension, > 6 in x)")
+    return nbl, mx
+
+
+def forces(r, ptype, box, table, nbl, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF, fma=0):
+    r, box, table, nbl = _f32(r), _f32(box), _f32(table), _i32(nbl)
+    n = len(r)
+    nt, _, npar = table.shape
+    pt = _i32(ptype) if ptype is not None else np.zeros(n, np.int32)
+    f = np.zeros((n, 3), np.float32)
+    U, W, lap, fsq = (np.zeros(n, np.float32) for _ in range(4))
+    lib().orc_forces(n, _p(r), _p(pt), _p(box), _p(table), npar, nt, kind, cutmode, _p(nbl),
+                     nbl.shape[1] - 1, _p(f), _p(U), _p(W), _p(lap), _p(fsq), fma)
+    return {"f": f, "U": U, "W": W, "lapU": lap, "Fsq": fsq}
+
+
+def rdf(r, ptype, box, bins, fma=0, r_max=0.0):
+    r, box = _f32(r), _f32(box)
+    n = len(r)
+    pt = _i32(ptype) if ptype is not None else np.zeros(n, np.int32)
+    nt = int(pt.max()) + 1
+    out = np.zeros((nt, nt, bins), np.uint64)
+    lib().orc_rdf(n, _p(r), _p(pt), _p(box), nt, bins, _p(out), fma, float(r_max))
+    return out
+
+
+def sq(r, q, ff=None):
+    r, q = _f32(r), _f32(q)
+    ffa = _f32(ff) if ff is not None else None
+    re = np.zeros(len(q), np.float64)
+    im = np.zeros(len(q), np.float64)
+    lib().orc_sq(len(r), _p(r), _p(ffa), len(q), _p(q), _p(re), _p(im))
+    return re + 1j * im
+
+
+class Run:
+    """State of one oracle simulation, advanced one timeblock at a time with
+    the reference's composed loop (gamdpy/simulation/Simulation.py:330-346)."""
+
+    def __init__(self, r, v, m, ptype, box, table, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF,
+                 nblist="N squared", skin=0.5, max_nbs=300, integrator="NVE", dt=0.005,
+                 temperature=None, tau=None, every=0, reset_every=0, fma=0):
+        n = len(r)
+        self.n = n
+        self.r = _f32(r).copy()
+        self.v = _f32(v).copy()
+        self.m = np.broadcast_to(np.asarray(m, np.float32), (n,)).copy()
+        self.ptype = _i32(ptype).copy() if ptype is not None else np.zeros(n, np.int32)
+        self.box = _f32(box).copy()
+        self.table = _f32(table)
+        self.kind, self.cutmode = kind, cutmode
+        self.nblist_kind = 0 if nblist == "N squared" else 1
+        self.skin, self.max_nbs = float(skin), int(max_nbs)
+        self.integrator = 0 if integrator == "NVE" else 1
+        self.dt = np.float32(dt)
+        self.T = np.float32(temperature or 0.0)
+        self.omega2 = np.float32(4.0 * np.pi * np.pi / tau / tau) if tau else np.float32(0)
+        self.every, self.reset_every, self.fma = int(every), int(reset_every), int(fma)
+        self.f = np.zeros((n, 3), np.float32)
+        self.img = np.zeros((n, 3), np.int32)
+        self.U, self.W, self.K = (np.zeros(n, np.float32) for _ in range(3))
+        self.nbl = np.zeros((n, self.max_nbs + 1), np.int32)
+        self.r_ref = np.zeros((n, 3), np.float32)
+        self.have_list = ctypes.c_int(0)
+        self.state = np.zeros(2, np.float32)
+        self.rebuilds = 0
+
+    def run_timeblock(self, steps):
+        nsave = steps // self.every if self.every else 0
+        scal = np.zeros((max(nsave, 1), 4), np.float64)
+        nt, _, npar = self.table.shape
+        rc = lib().orc_run_timeblock(
+            self.n, _p(self.r), _p(self.v), _p(self.f), _p(self.m), _p(self.img), _p(self.ptype),
+            _p(self.box), _p(self.table), npar, nt, self.kind, self.cutmode, self.nblist_kind,
+            self.skin, self.max_nbs, _p(self.nbl), _p(self.r_ref), ctypes.byref(self.have_list),
+            self.integrator, float(self.dt), _p(self.state), float(self.omega2), float(self.T),
+            int(steps), self.every, self.reset_every, _p(self.U), _p(self.W), _p(self.K),
+            _p(scal), self.fma)
+        if rc == -1:
+            raise ValueError("cell grid too small")
+        if rc == -2:
+            raise RuntimeError("neighbour list overflow")
+        self.rebuilds += rc
+        return scal[:nsave]

@@ -1,0 +1,121 @@
+"""Host-side API: gamdpy's names, shapes and known answers, without a GPU."""
+import numpy as np
+import pytest
+
+import gamdpy_b200 as gp
+from conftest import golden
+
+
+def test_potential_function_known_answers():
+    """tests/test_potential_functions.py:9-10 of the reference."""
+    assert gp.LJ_12_6(1, [2, 3]) == (5.0, 42.0, 438.0)
+    assert gp.LJ_12_6_sigma_epsilon(1, [2, 3]) == (48384.0, 585216.0, 7635456.0)
+
+
+@pytest.mark.parametrize("tag,wrap", [("sf", gp.apply_shifted_force_cutoff),
+                                      ("sp", gp.apply_shifted_potential_cutoff)])
+def test_cutoff_wrappers_match_reference(tag, wrap):
+    d = golden("known_answers")
+    pot = wrap(gp.LJ_12_6_sigma_epsilon)
+    got = np.array([pot(np.float32(x), np.array([1.0, 1.0, 2.5], np.float32)) for x in d[f"{tag}_r"]])
+    assert np.array_equal(got.astype(np.float64), d[f"{tag}_lj"])
+    assert pot._gdb_cutmode == (0 if tag == "sf" else 1)
+
+
+def test_simbox_known_answers():
+    """tests/test_simbox.py:5-50 of the reference."""
+    box = gp.Orthorhombic(D=3, lengths=np.array([3, 4, 5]))
+    ri, rj = np.array([2.5, 3, 4]), np.array([0.5, 0.5, 0.5])
+    dr = 0 * ri
+    assert box.get_dist_sq_dr_function()(ri, rj, box.lengths, dr) == 5.5
+    assert np.all(dr == np.array([-1, -1.5, -1.5]))
+    assert box.get_dist_sq_function()(ri, rj, box.lengths) == 5.5
+    r, img = np.array([4, 5, 6]), np.array([0, 1, 2])
+    box.get_apply_PBC()(r, img, box.lengths)
+    assert np.all(r == 1) and np.all(img == np.array([1, 2, 3]))
+    assert box.get_volume_function()(box.lengths) == 60
+    r_current = np.array([1, 1, 1])
+    assert box.get_dist_moved_sq_function()(r_current, r_current + 0.75 * box.lengths, box.lengths,
+                                            box.lengths) == 3.125
+    f = box.get_dist_moved_exceeds_limit_function()
+    assert not f(r_current, r_current + 0.5, box.lengths, box.lengths, 2.0, 1.0)
+    assert f(r_current, r_current + 0.75, box.lengths, box.lengths, 2.0, 1.0)
+
+
+def test_velocities_reproduce_reference_rng():
+    """Configuration.randomize_velocities uses gamdpy's RNG call order: the
+    golden run's initial velocities came from gamdpy with the same seed."""
+    d = golden("lj256_nve")
+    c = gp.Configuration(D=3)
+    c["r"] = np.zeros((256, 3), np.float32)
+    c["m"] = 1.0
+    c.randomize_velocities(temperature=0.7, seed=0)
+    assert np.array_equal(c["v"], d["v0"])
+
+
+def test_lattice_matches_reference_layout():
+    pos, box = gp.configuration.make_lattice(gp.unit_cells.FCC, cells=[2, 3, 4], rho=0.973)
+    assert pos.shape == (96, 3)
+    assert np.allclose(np.prod(box) * 0.973, 96)
+    assert np.all(pos >= -box / 2) and np.all(pos < box / 2)
+    # first cell = unit-cell fractional coordinates (C-order cell enumeration)
+    a = box[0] / 2
+    assert np.allclose(pos[1] - pos[0], [0.5 * a, 0.5 * a, 0.0])
+
+
+def test_configuration_columns():
+    c = gp.Configuration(D=3, N=10, compute_flags={"lapU": True, "Fsq": True})
+    assert c.vector_columns == ["r", "v", "f"]
+    assert c.scalar_columns == ["U", "W", "lapU", "K", "Fsq", "m"]
+    assert c["r"].shape == (10, 3) and c["m"].shape == (10,)
+    with pytest.raises(ValueError):
+        c["q"] = 1
+
+
+def test_default_compute_plan_for_b200():
+    c = gp.Configuration(D=3)
+    c.make_lattice(gp.unit_cells.FCC, cells=[8, 8, 8], rho=0.973)
+    plan = gp.get_default_compute_plan(c)
+    assert plan["nblist"] == "N squared" and plan["gridsync"]
+    big = gp.Configuration(D=3, N=65536)
+    assert gp.get_default_compute_plan(big)["nblist"] == "linked lists"
+
+
+def test_param_table_and_untagged_potential_rejected():
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon),
+                          params=[[[1.0, 0.8], [0.8, 0.88]], [[1.0, 1.5], [1.5, 0.5]], [[2.5, 2.0], [2.0, 2.2]]],
+                          max_num_nbs=100)
+    table, max_cut = pp.table()
+    assert table.shape == (2, 2, 3) and max_cut == np.float32(2.5)
+    rec, mc = pp.convert_user_params()
+    assert rec[0, 1][1] == np.float32(1.5)
+    bad = gp.PairPotential(lambda r, p: (0, 0, 0), params=[1.0, 1.0, 2.5], max_num_nbs=10)
+    with pytest.raises(NotImplementedError):
+        bad.kernel_kind()
+
+
+def test_runtime_action_validation():
+    with pytest.raises(ValueError):
+        gp.ScalarSaver(-1)
+    with pytest.raises(ValueError):
+        gp.MomentumReset(1.5)
+    out = gp.simulation.Output()
+    conf = gp.Configuration(D=3, N=4)
+    ss = gp.ScalarSaver(4)
+    with pytest.raises(ValueError):
+        ss.setup(conf, 2, 4, out)
+    ss.setup(conf, 2, 16, out)
+    assert out["scalars"].shape == (2, 4, 3) and out.attrs["scalar_names"] == ["U", "W", "K"]
+    rows = np.arange(20, dtype=np.float64).reshape(4, 5)
+    ss.update_from_rows(1, rows, out, 1.0)
+    U, K = gp.extract_scalars(out, ["U", "K"], first_block=1)
+    assert np.array_equal(U, rows[:, 0]) and np.array_equal(K, rows[:, 3])
+
+
+def test_workload_builders():
+    from gamdpy_b200 import workloads
+    c = workloads.ka_configuration(2048, seed=1)
+    assert c.N == 2048 and abs(c.N / c.get_volume() - 1.2) < 1e-4
+    assert (c.ptype == 1).sum() == 2048 // 5
+    assert np.all(np.abs(c["r"]) <= c.simbox.lengths / 2 + 1e-6)
+    assert abs(np.sum(c["v"] ** 2) / (3 * (c.N - 1)) - 0.45) < 1e-4

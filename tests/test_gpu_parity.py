@@ -1,0 +1,295 @@
+"""GPU parity: libgamdb200 (through its C ABI) against gamdpy's golden outputs
+and the CPU oracle.
+
+Bars: neighbour sets and RDF counts bit-exact; forces/energies within 1e-5
+relative RMS of gamdpy's float32 path; short trajectories within float32
+round-off of gamdpy's; S(q) within 1e-4 of the float64 oracle.
+"""
+import numpy as np
+import pytest
+
+import gamdpy_b200 as gp
+from conftest import golden, rel_rms, sorted_rows
+from gamdpy_b200 import _lib, workloads
+
+pytestmark = pytest.mark.gpu
+
+FORCE_TOL = 1e-5
+
+
+def make_sim(r, box, ptype, table, kind=_lib.POT_LJ_SIGMA_EPSILON, cutmode=_lib.CUT_SHIFTED_FORCE,
+             nblist=_lib.NBLIST_NSQ, skin=0.5, max_nbs=300, v=None, tp=0):
+    n = len(r)
+    sim = _lib.Sim(n, table.shape[0])
+    sim.set_box(box)
+    sim.set_pair_potential(kind, cutmode, table)
+    sim.set_nblist(nblist, skin, max_nbs)
+    sim.set_plan(tp)
+    sim.set_nve(0.005)
+    v = np.zeros((n, 3), np.float32) if v is None else v
+    sim.upload(r, v, np.ones(n, np.float32), ptype if ptype is not None else np.zeros(n, np.int32))
+    return sim
+
+
+def table_of(d):
+    from oracle import oracle as O
+    return O.param_table([d["sigma"], d["epsilon"], d["cut"]])
+
+
+@pytest.mark.parametrize("name,tp", [("lj256_sf", 0), ("lj256_sp", 0), ("lj256_sf", 1), ("lj256_sf", 4)])
+def test_nsq_list_and_forces_vs_gamdpy(name, tp):
+    d = golden(name)
+    cm = _lib.CUT_SHIFTED_FORCE if str(d["cutoff"]) == "SF" else _lib.CUT_SHIFTED_POTENTIAL
+    sim = make_sim(d["r"], d["box"], d["ptype"], table_of(d), cutmode=cm, skin=float(d["skin"]), tp=tp)
+    sim.eval_forces()
+    counts, flat = sorted_rows(sim.nblist(300))
+    assert np.array_equal(counts, d["nb_counts"])
+    assert np.array_equal(flat, d["nb_flat"])
+    f = sim.download()["f"]
+    sc = sim.download_scalars()
+    assert rel_rms(f, d["f"]) < FORCE_TOL
+    for k in ("U", "W", "lapU"):
+        assert rel_rms(sc[k], d[k]) < FORCE_TOL, k
+
+
+@pytest.mark.parametrize("tp", [0, 1, 2, 8])
+def test_cell_list_and_forces_vs_gamdpy(tp):
+    d = golden("ka1372_cells")
+    sim = make_sim(d["r"], d["box"], d["ptype"], table_of(d), nblist=_lib.NBLIST_CELLS, skin=float(d["skin"]),
+                   tp=tp)
+    sim.eval_forces()
+    counts, flat = sorted_rows(sim.nblist(300))
+    assert np.array_equal(counts, d["nb_counts"])
+    assert np.array_equal(flat, d["nb_flat"])
+    f = sim.download()["f"]
+    sc = sim.download_scalars()
+    assert rel_rms(f, d["f"]) < FORCE_TOL
+    for k in ("U", "W", "lapU"):
+        assert rel_rms(sc[k], d[k]) < FORCE_TOL, k
+
+
+@pytest.mark.parametrize("n,nblist", [(4000, _lib.NBLIST_NSQ), (30000, _lib.NBLIST_CELLS),
+                                      (8000, _lib.NBLIST_CELLS)])
+def test_lists_vs_oracle_larger(oracle, n, nblist):
+    """Bit-exact sets at sizes the golden runs do not reach, against the
+    oracle in the same (fused) distance form."""
+    conf = workloads.ka_configuration(n, seed=7, jitter=0.2)
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    sim = make_sim(conf["r"], conf.simbox.lengths, conf.ptype, table, nblist=nblist, skin=0.3)
+    sim.eval_forces()
+    got = sim.nblist(300)
+    ref, _ = oracle.nblist_nsq(conf["r"], conf.simbox.lengths, float(np.float32(2.5) + np.float32(0.3)), 300,
+                               fma=1)
+    c1, f1 = sorted_rows(got)
+    c2, f2 = sorted_rows(ref)
+    assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
+    res = oracle.forces(conf["r"], conf.ptype, conf.simbox.lengths, table, ref, fma=1)
+    assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
+
+
+def run_api_trajectory(d):
+    """Golden trajectory through the public API (Simulation + runtime actions)."""
+    n = len(d["r0"])
+    conf = gp.Configuration(D=3)
+    conf["r"] = d["r0"].copy()
+    conf["v"] = d["v0"].copy()
+    conf.simbox = gp.Orthorhombic(3, d["box"])
+    conf["m"] = 1.0
+    conf.ptype[:] = d["ptype"]
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon),
+                          params=[d["sigma"], d["epsilon"], d["cut"]], max_num_nbs=300)
+    if str(d["integrator"]) == "NVE":
+        integ = gp.integrators.NVE(dt=float(d["dt"]))
+    else:
+        integ = gp.integrators.NVT(temperature=float(d["temperature"]), tau=float(d["tau"]), dt=float(d["dt"]))
+    actions = [gp.ScalarSaver(int(d["every"]))]
+    if int(d["reset"]):
+        actions.append(gp.MomentumReset(int(d["reset"])))
+    plan = {"pb": 4, "tp": 1, "skin": float(d["skin"]), "UtilizeNIII": False, "gridsync": False,
+            "nblist": str(d["nblist"])}
+    sim = gp.Simulation(conf, pp, integ, actions, num_timeblocks=int(d["blocks"]),
+                        steps_per_timeblock=int(d["steps"]), compute_plan=plan, storage="memory")
+    xi_test = integ.d_thermostat_state.copy_to_host()[0] if str(d["integrator"]) == "NVT" else 0.0
+    for _ in sim.run_timeblocks():
+        pass
+    return sim, conf, integ, xi_test
+
+
+@pytest.mark.parametrize("name", ["lj256_nve", "ka1372_nvt"])
+def test_trajectory_vs_gamdpy(name):
+    d = golden(name)
+    sim, conf, integ, xi_test = run_api_trajectory(d)
+    if str(d["integrator"]) == "NVT":
+        assert abs(xi_test - d["xi_after_test"][0]) <= 1e-5 * max(1.0, abs(xi_test))
+        assert abs(integ.thermostat_state[0] - d["thermostat_state"][0]) <= 1e-5 * abs(d["thermostat_state"][0])
+    assert np.abs(conf["r"] - d["r"]).max() < 1e-5
+    assert np.array_equal(conf.r_im, d["r_im"])
+    for k in ("v", "f", "U", "W", "K"):
+        assert rel_rms(conf[k], d[k]) < FORCE_TOL, k
+    out = sim.output
+    assert list(out.attrs["scalar_names"]) == list(d["scalar_names"])
+    ref = d["scalars"]
+    got = out["scalars"]
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max()
+
+
+def test_rdf_bit_exact_vs_gamdpy():
+    d = golden("rdf")
+    for tag in ("lj256", "ka1372"):
+        conf = gp.Configuration(D=3)
+        conf["r"] = d[f"{tag}_r"].copy()
+        conf.simbox = gp.Orthorhombic(3, d[f"{tag}_box"])
+        conf.ptype[:] = d[f"{tag}_ptype"]
+        calc = gp.CalculatorRadialDistribution(conf, bins=100)
+        calc.update()
+        assert np.array_equal(calc.rdf_list[0], d[f"{tag}_bins_numba"]), tag
+    # the normalised reading agrees with gamdpy's read()
+    conf = gp.Configuration(D=3)
+    conf["r"] = d["lj256_r"].copy()
+    conf.simbox = gp.Orthorhombic(3, d["lj256_box"])
+    calc = gp.CalculatorRadialDistribution(conf, bins=100)
+    calc.update()
+    assert np.allclose(calc.read()["rdf"], d["lj256_read_rdf"], rtol=1e-12)
+
+
+def test_rdf_short_range_cells_vs_oracle(oracle):
+    """r_max < L/3 takes the cell path: the same counts as the oracle's all
+    pairs; r_max = L/2 takes the all-pairs path."""
+    conf = workloads.ka_configuration(20000, seed=3, jitter=0.3)
+    L = conf.simbox.lengths
+    got = _lib.rdf_compute(conf["r"], conf.ptype, L, 2, 500, r_max=5.0)
+    ref = oracle.rdf(conf["r"], conf.ptype, L, 500, fma=1, r_max=5.0)
+    assert got.sum() > 0 and np.array_equal(got, ref)
+    allpairs = _lib.rdf_compute(conf["r"], conf.ptype, L, 2, 500)
+    assert np.array_equal(allpairs, oracle.rdf(conf["r"], conf.ptype, L, 500, fma=1))
+
+
+def test_rdf_device_path_matches_host_path():
+    d = golden("ka1372_cells")
+    conf = gp.Configuration(D=3)
+    conf["r"] = d["r"].copy()
+    conf.simbox = gp.Orthorhombic(3, d["box"])
+    conf.ptype[:] = d["ptype"]
+    conf["m"] = 1.0
+    sim = make_sim(d["r"], d["box"], d["ptype"], table_of(d), nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.eval_forces()  # reorders particles by cell on the device
+    out = np.zeros((2, 2, 100), np.uint64)
+    sim.rdf_update(100, 0.0, out)
+    assert np.array_equal(out.astype(np.float64), golden("rdf")["ka1372_bins_numba"])
+
+
+def test_sq_vs_gamdpy_and_oracle(oracle):
+    d = golden("sq")
+    rho = _lib.sq_compute(d["r"], d["box"], d["n_vectors"])
+    ref64 = oracle.sq(d["r"], d["q"])
+    assert np.abs(rho - ref64).max() < 1e-4 * max(1.0, np.abs(ref64).max())
+    assert np.abs(rho - d["multi_rho_q"]).max() < 2e-3 * max(1.0, np.abs(ref64).max())
+    # form factors, through the calculator API
+    conf = gp.Configuration(D=3)
+    conf["r"] = d["r"].copy()
+    conf.simbox = gp.Orthorhombic(3, d["box"])
+    calc = gp.CalculatorStructureFactor(conf, atomic_form_factors=d["ff"])
+    calc.generate_q_vectors(q_max=6.0)
+    calc.update()
+    raw = calc.read(None)
+    assert np.allclose(raw["q"], d["ff_q"])
+    assert np.abs(raw["rho_q"][0] - d["ff_rho_q"]).max() < 2e-3 * max(1.0, np.abs(d["ff_rho_q"]).max())
+
+
+def test_sq_negative_and_large_n_vectors(oracle):
+    conf = workloads.ka_configuration(5000, seed=2)
+    L = conf.simbox.lengths
+    rng = np.random.default_rng(0)
+    nv = rng.integers(-12, 13, size=(300, 3))
+    rho = _lib.sq_compute(conf["r"], L, nv)
+    q = (2 * np.pi * nv / L).astype(np.float32)
+    ref = oracle.sq(conf["r"], q)
+    assert np.abs(rho - ref).max() < 1e-4 * max(1.0, np.abs(ref).max())
+
+
+def test_overflow_raises_like_gamdpy():
+    d = golden("lj256_sf")
+    conf = gp.Configuration(D=3)
+    conf["r"] = d["r"].copy()
+    conf.simbox = gp.Orthorhombic(3, d["box"])
+    conf["m"] = 1.0
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon), params=[1.0, 1.0, 2.5],
+                          max_num_nbs=40)
+    ev = gp.Evaluator(conf, pp, compute_plan={"pb": 8, "tp": 1, "skin": 0.5, "nblist": "N squared"})
+    with pytest.raises(Exception, match="Neighbor-list is invalid"):
+        ev.evaluate()
+
+
+def test_nan_position_reports_error_not_fault():
+    d = golden("ka1372_cells")
+    r = d["r"].copy()
+    r[5] = np.nan
+    sim = make_sim(r, d["box"], d["ptype"], table_of(d), nblist=_lib.NBLIST_CELLS, skin=0.3)
+    with pytest.raises(_lib.GdbError):
+        sim.run(0.0, 3)
+    assert sim.status() & _lib.STATUS_NAN
+
+
+def test_runs_are_bitwise_reproducible():
+    conf = workloads.ka_configuration(4000, seed=5)
+    outs = []
+    for _ in range(2):
+        c = workloads.ka_configuration(4000, seed=5)
+        sim = gp.Simulation(c, workloads.ka_pair_potential(), gp.integrators.NVT(0.45, 0.2, 0.005),
+                            [gp.ScalarSaver(10), gp.MomentumReset(50)], num_timeblocks=2, steps_per_timeblock=200,
+                            compute_plan={"pb": 64, "tp": 4, "skin": 0.3, "nblist": "linked lists"},
+                            storage="memory")
+        for _ in sim.run_timeblocks():
+            pass
+        outs.append((c["r"].copy(), c["v"].copy(), sim.output["scalars"].copy()))
+    for a, b in zip(outs[0], outs[1]):
+        assert np.array_equal(a, b)
+    assert conf.N == 4000
+
+
+def test_nve_energy_conservation():
+    """tests/test_LJ_nxyz.py:10-111 of the reference: LJ rho 0.8442, T0 1.44,
+    shifted force, dt 0.005, 2 x 4096 steps: var(E)/N < 1e-4 and
+    Tkin, Tconf in (0.67, 0.72)."""
+    conf = gp.Configuration(D=3, compute_flags={"Fsq": True, "lapU": True})
+    conf.make_lattice(gp.unit_cells.FCC, cells=[8, 8, 8], rho=0.8442)
+    conf["m"] = 1.0
+    conf.randomize_velocities(temperature=1.44, seed=0)
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon), params=[1.0, 1.0, 2.5],
+                          max_num_nbs=1000)
+    sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.005),
+                        [gp.MomentumReset(100), gp.ConfigurationSaver(),
+                         gp.ScalarSaver(8, {"Fsq": True, "lapU": True, "stresses": False})],
+                        num_timeblocks=2, steps_per_timeblock=4096, storage="memory")
+    for _ in sim.run_timeblocks():
+        pass
+    U, W, lapU, Fsq, K = gp.extract_scalars(sim.output, ["U", "W", "lapU", "Fsq", "K"], first_block=1)
+    N = conf.N
+    E = U + K
+    var_e = np.var(E) / N
+    half = len(U) // 2
+    Tkin = np.mean(2 * K[half:] / 3 / (N - 1))
+    Tconf = np.mean(Fsq[half:] / lapU[half:])
+    assert var_e < 1e-4
+    assert 0.67 < Tkin < 0.72
+    assert 0.67 < Tconf < 0.72
+    frames = sim.output["block"]
+    assert frames.shape == (2, 14, 2, N, 3)
+    assert np.abs(frames[1, -1, 0] - conf["r"]).max() < 1e-6  # step 4096 frame = final positions
+
+
+def test_kob_andersen_reference_state_point():
+    """examples/kablj.py:102-131 compares with RUMD3 at rho 1.2, T 0.8:
+    u = -6.346, w = 5.534 per particle; short run, loose bands."""
+    conf = workloads.ka_configuration(4000, temperature=0.8, seed=11)
+    sim = gp.Simulation(conf, workloads.ka_pair_potential(), gp.integrators.NVT(0.8, 0.2, 0.005),
+                        [gp.ScalarSaver(16), gp.MomentumReset(100)], num_timeblocks=6,
+                        steps_per_timeblock=2048, compute_plan={"pb": 64, "tp": 4, "skin": 0.3,
+                                                               "nblist": "linked lists"}, storage="memory")
+    for _ in sim.run_timeblocks():
+        pass
+    U, W = gp.extract_scalars(sim.output, ["U", "W"], first_block=2)
+    u, w = np.mean(U) / conf.N, np.mean(W) / conf.N
+    assert abs(u - (-6.346)) < 0.05, u
+    assert abs(w - 5.534) < 0.15, w

@@ -1,0 +1,133 @@
+"""The CPU oracle against gamdpy's own outputs (tests/golden, produced by
+tests/golden/make_golden.py from the reference run on the CPU) and against the
+known answers of gamdpy's tests.  This pins the oracle the GPU parity tests
+then use."""
+import numpy as np
+import pytest
+
+from conftest import golden, rel_rms, sorted_rows
+
+
+def test_known_answers(oracle):
+    """tests/test_potential_functions.py:9-10 and the cutoff wrappers on a grid."""
+    d = golden("known_answers")
+    got = oracle.pair_potential(1, [2, 3, 100], kind=oracle.POT_LJ_12_6, cutmode=oracle.CUT_NONE)
+    assert tuple(got) == (5.0, 42.0, 438.0) == tuple(d["lj_12_6_1_23"])
+    got = oracle.pair_potential(1, [2, 3, 100], kind=oracle.POT_LJ_SIGMA_EPSILON, cutmode=oracle.CUT_NONE)
+    assert tuple(got) == (48384.0, 585216.0, 7635456.0) == tuple(d["lj_se_1_23"])
+    for tag, cm in (("sf", oracle.CUT_SF), ("sp", oracle.CUT_SP)):
+        for key, prm in (("lj", [1.0, 1.0, 2.5]), ("ka", [0.8, 1.5, 2.0])):
+            got = np.array([oracle.pair_potential(x, prm, cutmode=cm) for x in d[f"{tag}_r"]])
+            # bit-identical to numba's float32 evaluation
+            assert np.array_equal(got.astype(np.float64), d[f"{tag}_{key}"])
+
+
+def test_minimum_image_known_answer(oracle):
+    """tests/test_simbox.py:10-19: dist_sq 5.5, dr (-1, -1.5, -1.5)."""
+    d2, dr = oracle.dist_sq([2.5, 3, 4], [0.5, 0.5, 0.5], [3, 4, 5])
+    assert d2 == 5.5 == float(golden("known_answers")["mic_dist_sq"])
+    assert np.array_equal(dr, [-1, -1.5, -1.5])
+
+
+def test_pbc_known_answer(oracle):
+    """tests/test_simbox.py:21-33."""
+    r, img = oracle.apply_pbc([4, 5, 6], [0, 1, 2], [3, 4, 5])
+    assert np.array_equal(r, [1, 1, 1]) and np.array_equal(img, [1, 2, 3])
+    r, img = oracle.apply_pbc([-4, -5, -6], [0, 1, 2], [3, 4, 5])
+    assert np.array_equal(r, [-1, -1, -1]) and np.array_equal(img, [-1, 0, 1])
+
+
+@pytest.mark.parametrize("name", ["lj256_sf", "lj256_sp"])
+def test_nsq_list_and_forces(oracle, name):
+    d = golden(name)
+    nbl, mx = oracle.nblist_nsq(d["r"], d["box"], float(np.float32(d["cut"].max()) + np.float32(d["skin"])), 300)
+    counts, flat = sorted_rows(nbl)
+    assert np.array_equal(counts, d["nb_counts"])
+    assert np.array_equal(flat, d["nb_flat"])
+    cm = oracle.CUT_SF if str(d["cutoff"]) == "SF" else oracle.CUT_SP
+    res = oracle.forces(d["r"], d["ptype"], d["box"], oracle.param_table([d["sigma"], d["epsilon"], d["cut"]]),
+                        nbl, cutmode=cm)
+    for k in ("f", "U", "W", "lapU"):
+        assert rel_rms(res[k], d[k]) < 2e-6, k
+
+
+def test_cell_list_and_forces(oracle):
+    d = golden("ka1372_cells")
+    nbl, mx = oracle.nblist_cells(d["r"], d["box"], float(d["cut"].max()), float(d["skin"]), 300)
+    counts, flat = sorted_rows(nbl)
+    assert np.array_equal(counts, d["nb_counts"])
+    assert np.array_equal(flat, d["nb_flat"])
+    # the N^2 build gives the same sets (tests/test_linked_lists_nblist.py:104-106)
+    nbl2, _ = oracle.nblist_nsq(d["r"], d["box"], float(np.float32(d["cut"].max()) + np.float32(d["skin"])), 300)
+    c2, f2 = sorted_rows(nbl2)
+    assert np.array_equal(c2, counts) and np.array_equal(f2, flat)
+    res = oracle.forces(d["r"], d["ptype"], d["box"], oracle.param_table([d["sigma"], d["epsilon"], d["cut"]]), nbl)
+    for k in ("f", "U", "W", "lapU"):
+        assert rel_rms(res[k], d[k]) < 3e-6, k
+
+
+def test_fma_variant_changes_nothing_here(oracle):
+    """The fused distance form (libNVVM's default contraction) gives the same
+    sets on these fixtures; it only matters within one ulp of (rc+skin)^2."""
+    d = golden("ka1372_cells")
+    a, _ = oracle.nblist_cells(d["r"], d["box"], float(d["cut"].max()), float(d["skin"]), 300, fma=0)
+    b, _ = oracle.nblist_cells(d["r"], d["box"], float(d["cut"].max()), float(d["skin"]), 300, fma=1)
+    assert np.array_equal(sorted_rows(a)[1], sorted_rows(b)[1])
+
+
+def run_golden_trajectory(oracle, d):
+    tab = oracle.param_table([d["sigma"], d["epsilon"], d["cut"]])
+    nvt = str(d["integrator"]) == "NVT"
+    run = oracle.Run(d["r0"], d["v0"], 1.0, d["ptype"], d["box"], tab, nblist=str(d["nblist"]),
+                     skin=float(d["skin"]), max_nbs=300, integrator=str(d["integrator"]), dt=float(d["dt"]),
+                     temperature=float(d["temperature"]) if nvt else None, tau=float(d["tau"]) if nvt else None,
+                     every=int(d["every"]), reset_every=int(d["reset"]))
+    # Simulation.__init__ runs one test step on the device copy
+    # (gamdpy/simulation/Simulation.py:200-211); the thermostat keeps its update
+    run.run_timeblock(1)
+    xi_test = float(run.state[0])
+    run.r[:] = d["r0"]
+    run.v[:] = d["v0"]
+    run.img[:] = 0
+    run.have_list.value = 0
+    rows = np.array([run.run_timeblock(int(d["steps"])) for _ in range(int(d["blocks"]))])
+    return run, rows, xi_test
+
+
+@pytest.mark.parametrize("name", ["lj256_nve", "ka1372_nvt"])
+def test_trajectory(oracle, name):
+    d = golden(name)
+    run, rows, xi_test = run_golden_trajectory(oracle, d)
+    assert abs(xi_test - float(d["xi_after_test"][0])) <= 1e-5 * max(1.0, abs(xi_test))
+    assert abs(run.state[0] - d["thermostat_state"][0]) <= 1e-5 * max(1.0, abs(run.state[0]))
+    assert np.abs(run.r - d["r"]).max() < 1e-5
+    assert np.array_equal(run.img, d["r_im"])
+    for k, got in (("v", run.v), ("f", run.f), ("U", run.U), ("W", run.W), ("K", run.K)):
+        assert rel_rms(got, d[k]) < 1e-5, k
+    cols = {"U": 0, "W": 1, "K": 2}
+    for c, nm in enumerate(d["scalar_names"]):
+        ref = d["scalars"][:, :, c]
+        assert np.abs(rows[:, :, cols[str(nm)]] - ref).max() <= 2e-6 * np.abs(ref).max(), nm
+
+
+def test_rdf_bit_exact(oracle):
+    """Integer counts equal gamdpy's (numba-typed evaluation and the
+    simulator run of the kernel itself)."""
+    d = golden("rdf")
+    for tag in ("lj256", "ka1372"):
+        got = oracle.rdf(d[f"{tag}_r"], d[f"{tag}_ptype"], d[f"{tag}_box"], 100)
+        assert np.array_equal(got.astype(np.float64), d[f"{tag}_bins_numba"]), tag
+    assert np.array_equal(d["lj256_bins_simulator"], d["lj256_bins_numba"])
+
+
+def test_sq_against_reference_backends(oracle):
+    d = golden("sq")
+    q = d["q"]
+    got = oracle.sq(d["r"], q)
+    for key in ("multi", "single"):
+        ref = d[f"{key}_rho_q"]
+        # gamdpy evaluates in complex64 (float32 q.r): agreement to ~1e-4
+        assert np.abs(got - ref).max() < 2e-3 * max(1.0, np.abs(ref).max()), key
+        assert rel_rms(np.abs(got) ** 2, d[f"{key}_S"]) < 1e-3, key
+    got = oracle.sq(d["r"], d["ff_q"], d["ff"])
+    assert np.abs(got - d["ff_rho_q"]).max() < 2e-3 * max(1.0, np.abs(d["ff_rho_q"]).max())
