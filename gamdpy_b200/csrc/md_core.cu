@@ -459,6 +459,7 @@ struct StepArgs {
     int tfunc;
     float tp0, tp1, tp2, tp3;
     int every, reset_every;
+    int nrows;            // ScalarSaver rows allocated (writes beyond are dropped)
     float *conf;          // ConfigurationSaver frames (conf_per_block, 2, n, 3) or null
     int conf_per_block;
     const int *orig;      // user index of each slot
@@ -719,7 +720,7 @@ __global__ void __launch_bounds__(GDB_BLOCK) k_step(StepArgs a, PairTable tab) {
                 ctrl->xi = (float)((double)ctrl->xi + (double)(a.dt * a.omega2) * dev);
                 ctrl->sumK = (float)tot[0];
             }
-            if (rec) {  // scalar_saver.py:274-288
+            if (rec && step / a.every < a.nrows) {  // scalar_saver.py:274-288
                 double *row = a.rows + (size_t)(step / a.every) * GDB_NUM_SCALARS;
                 row[GDB_SCALAR_U] = tot[1];
                 row[GDB_SCALAR_W] = tot[2];
@@ -994,6 +995,7 @@ static StepArgs make_args(gdb_sim *h, int mode) {
     a.tp3 = h->tparams[3];
     a.every = h->scalar_every;
     a.reset_every = h->momentum_every;
+    a.nrows = h->rows ? h->rows_cap : 0;
     a.conf = h->conf;
     a.conf_per_block = h->conf_per_block;
     a.orig = h->orig;
