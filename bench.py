@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--n", type=int, default=1_048_576)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--block", type=int, default=500, help="steps per timeblock")
+    p.add_argument("--profile", action="store_true",
+                   help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
+    p.add_argument("--tp", type=int, default=0, help="lanes per particle (0 = library default)")
     return p.parse_args()
 
 
@@ -210,7 +213,7 @@ def main():
     pp = workloads.ka_pair_potential(max_num_nbs=300)
     integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
     block = min(args.block, max(1, args.steps))
-    plan = {"pb": 64, "tp": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False, "nblist": "linked lists"}
+    plan = {"pb": 64, "tp": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False, "nblist": "linked lists"}
     sim = gp.Simulation(conf, pp, integ, [gp.ScalarSaver(max(1, block // 8))], num_timeblocks=8,
                         steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
     dev = sim._sim
@@ -221,6 +224,13 @@ def main():
     # ---- timed: K steps, device-resident inputs ---------------------------
     nblocks = max(1, args.steps // block)
     steps = nblocks * block
+    if args.profile:
+        ms = sum(dev.run(float(b * block * 0.005), block) for b in range(nblocks))
+        mean_nbs, max_nbs = dev.nblist_stats()
+        print(json.dumps({"profile": True, "n": n, "steps": steps, "ms_per_step": ms / steps,
+                          "mats": n * steps / ms / 1e3, "mean_neighbours": mean_nbs,
+                          "tp": args.tp, "step_kernel_ms": dev.time_step_kernel(20)}), flush=True)
+        return
     clocks = ClockSampler(local)
     barrier(pg)
     clocks.start()

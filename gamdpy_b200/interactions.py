@@ -40,8 +40,8 @@ def _param_table(params_user):
     PairPotential.convert_user_params (pair_potential.py:23-51)."""
     mats = []
     for p in params_user:
-        if np.isscalar(p):
-            mats.append(np.ones((1, 1)) * p)
+        if np.ndim(p) == 0:
+            mats.append(np.ones((1, 1)) * float(p))
         else:
             mats.append(np.array(p, dtype=np.float32))
     nt = mats[0].shape[0]
