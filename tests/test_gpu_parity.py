@@ -134,21 +134,32 @@ def test_trajectory_vs_gamdpy(name):
     assert np.abs(got - ref).max() <= 2e-6 * np.abs(ref).max()
 
 
-def test_rdf_bit_exact_vs_gamdpy():
+def _rdf_conf(d, tag):
+    conf = gp.Configuration(D=3)
+    conf["r"] = d[f"{tag}_r"].copy()
+    conf.simbox = gp.Orthorhombic(3, d[f"{tag}_box"])
+    conf.ptype[:] = d[f"{tag}_ptype"]
+    return conf
+
+
+def test_rdf_bit_exact_vs_gamdpy(oracle, monkeypatch):
+    """Unfused distance form: the counts of gamdpy itself (run on the CPU,
+    where numba does not contract).  Default fused form (gamdpy's numba.cuda
+    build on B200 contracts, tests/golden/numba_contraction.json): the oracle's
+    fused counts."""
     d = golden("rdf")
     for tag in ("lj256", "ka1372"):
-        conf = gp.Configuration(D=3)
-        conf["r"] = d[f"{tag}_r"].copy()
-        conf.simbox = gp.Orthorhombic(3, d[f"{tag}_box"])
-        conf.ptype[:] = d[f"{tag}_ptype"]
-        calc = gp.CalculatorRadialDistribution(conf, bins=100)
+        calc = gp.CalculatorRadialDistribution(_rdf_conf(d, tag), bins=100)
+        calc.update()
+        fused = oracle.rdf(d[f"{tag}_r"], d[f"{tag}_ptype"], d[f"{tag}_box"], 100, fma=1)
+        assert np.array_equal(calc.rdf_list[0], fused.astype(np.float64)), tag
+    monkeypatch.setenv("GDB_NBLIST_FMA", "0")
+    for tag in ("lj256", "ka1372"):
+        calc = gp.CalculatorRadialDistribution(_rdf_conf(d, tag), bins=100)
         calc.update()
         assert np.array_equal(calc.rdf_list[0], d[f"{tag}_bins_numba"]), tag
     # the normalised reading agrees with gamdpy's read()
-    conf = gp.Configuration(D=3)
-    conf["r"] = d["lj256_r"].copy()
-    conf.simbox = gp.Orthorhombic(3, d["lj256_box"])
-    calc = gp.CalculatorRadialDistribution(conf, bins=100)
+    calc = gp.CalculatorRadialDistribution(_rdf_conf(d, "lj256"), bins=100)
     calc.update()
     assert np.allclose(calc.read()["rdf"], d["lj256_read_rdf"], rtol=1e-12)
 
@@ -165,7 +176,7 @@ def test_rdf_short_range_cells_vs_oracle(oracle):
     assert np.array_equal(allpairs, oracle.rdf(conf["r"], conf.ptype, L, 500, fma=1))
 
 
-def test_rdf_device_path_matches_host_path():
+def test_rdf_device_path_matches_host_path(oracle):
     d = golden("ka1372_cells")
     conf = gp.Configuration(D=3)
     conf["r"] = d["r"].copy()
@@ -176,7 +187,7 @@ def test_rdf_device_path_matches_host_path():
     sim.eval_forces()  # reorders particles by cell on the device
     out = np.zeros((2, 2, 100), np.uint64)
     sim.rdf_update(100, 0.0, out)
-    assert np.array_equal(out.astype(np.float64), golden("rdf")["ka1372_bins_numba"])
+    assert np.array_equal(out, oracle.rdf(d["r"], d["ptype"], d["box"], 100, fma=1))
 
 
 def test_sq_vs_gamdpy_and_oracle(oracle):
@@ -280,16 +291,31 @@ def test_nve_energy_conservation():
 
 
 def test_kob_andersen_reference_state_point():
-    """examples/kablj.py:102-131 compares with RUMD3 at rho 1.2, T 0.8:
-    u = -6.346, w = 5.534 per particle; short run, loose bands."""
-    conf = workloads.ka_configuration(4000, temperature=0.8, seed=11)
-    sim = gp.Simulation(conf, workloads.ka_pair_potential(), gp.integrators.NVT(0.8, 0.2, 0.005),
-                        [gp.ScalarSaver(16), gp.MomentumReset(100)], num_timeblocks=6,
-                        steps_per_timeblock=2048, compute_plan={"pb": 64, "tp": 4, "skin": 0.3,
-                                                               "nblist": "linked lists"}, storage="memory")
+    """examples/kablj.py of the reference: KA (shifted potential) at rho 1.2,
+    N 2000, melted at T 2 and ramped to 0.8, then 32 x 2048 production steps;
+    asserts |u - (-6.346)| < 0.01 and |w - 5.534| < 0.03 per particle (RUMD3,
+    examples/kablj.py:120-131)."""
+    N, rho, T, dt = 2000, 1.2, 0.8, 0.004
+    conf = gp.Configuration(D=3, compute_flags={"Fsq": True, "lapU": True, "Vol": True})
+    conf.make_positions(N=N, rho=rho)
+    conf["m"] = 1.0
+    conf.randomize_velocities(temperature=2.0)
+    conf.ptype[::5] = 1
+    pp = gp.PairPotential(gp.apply_shifted_potential_cutoff(gp.LJ_12_6_sigma_epsilon),
+                          params=[workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT], max_num_nbs=1000)
+    blocks, steps = 32, 2048
+    run_time = dt * blocks * steps
+    ramp = gp.make_function_ramp(value0=2.0, x0=run_time / 8, value1=T, x1=run_time / 4)
+    sim = gp.Simulation(conf, pp, gp.integrators.NVT(temperature=ramp, tau=0.2, dt=dt), [gp.MomentumReset(100)],
+                        num_timeblocks=blocks, steps_per_timeblock=steps, storage="memory")
     for _ in sim.run_timeblocks():
         pass
-    U, W = gp.extract_scalars(sim.output, ["U", "W"], first_block=2)
-    u, w = np.mean(U) / conf.N, np.mean(W) / conf.N
-    assert abs(u - (-6.346)) < 0.05, u
-    assert abs(w - 5.534) < 0.15, w
+    sim = gp.Simulation(conf, pp, gp.integrators.NVT(temperature=T, tau=0.2, dt=dt),
+                        [gp.MomentumReset(100), gp.ScalarSaver(16, {"Fsq": True, "lapU": True})],
+                        num_timeblocks=blocks, steps_per_timeblock=steps, storage="memory")
+    for _ in sim.run_timeblocks():
+        pass
+    U, W = gp.extract_scalars(sim.output, ["U", "W"], first_block=0)
+    mu, mw = np.mean(U) / N, np.mean(W) / N
+    assert abs(mu - (-6.346)) < 0.01, mu
+    assert abs(mw - 5.534) < 0.03, mw
