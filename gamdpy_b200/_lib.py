@@ -76,6 +76,7 @@ SIGNATURES = {
     "gdb_sq_update": ([_P, _i, _P, _P, _P, _P], _i),
     "gdb_rdf_compute": ([_i, _P, _P, _P, _i, _i, _d, _P], _i),
     "gdb_sq_compute": ([_i, _P, _P, _P, _i, _P, _P, _P], _i),
+    "gdb_sq_compute_noalloc": ([_i, _P, _P, _P, _i, _P, _i, _P, _P, _P], _i),
 }
 
 _lib = None

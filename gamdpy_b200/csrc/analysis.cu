@@ -24,6 +24,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <mutex>
 #include <vector>
 
 #include "../../include/gamdb200.h"
@@ -428,7 +429,168 @@ static int sq_device(gdb_sim *h, cudaStream_t st, const float4 *pos, const int *
     return GDB_OK;
 }
 
+// ---------------------------------------------------------------------------
+// S(q) with no device allocation
+//
+// For callers that cannot let this library call cudaMalloc: applications
+// whose own allocator or fixed memory pool owns the GPU's memory, code with
+// a hard device-memory budget, and call sites where allocating is not
+// allowed while they run.  The caller passes device inputs and outputs; the
+// only scratch (the float64 accumulators) is the file-scope array below,
+// which every GPU that loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+#define GDB_SQ_NOALLOC_MAX_Q 65536  // q-vectors per call
+#define GDB_SQ_NOALLOC_MAX_N 48     // largest |n| component (shared table 32 x 291 float2 = 74.5 KB)
+#define SQNA_TAIL (2 * GDB_SQ_NOALLOC_MAX_Q)
+
+// [0, 2 nq): (re, im) accumulators; [TAIL]: sum of form factors; [TAIL+1]:
+// 1.0 when an n-vector component is outside [-n_max, n_max].  Shared by all
+// calls on a device: calls that overlap on the GPU race on it.
+static __device__ __align__(256) double g_sq_scratch[SQNA_TAIL + 32];
+
+namespace {
+
+std::mutex g_sq_scratch_mu;
+double *g_sq_scratch_addr[256] = {nullptr};
+
+// Device address of g_sq_scratch on the current device, looked up once per
+// device (host code cannot use the symbol itself as a device address).
+int sq_scratch_address(int dev, double **out) {
+    std::lock_guard<std::mutex> lock(g_sq_scratch_mu);
+    if (dev < 0 || dev >= 256) return GDB_ERR_ARG;
+    if (!g_sq_scratch_addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_sq_scratch) != cudaSuccess || !p) return GDB_ERR_CUDA;
+        g_sq_scratch_addr[dev] = (double *)p;
+    }
+    *out = g_sq_scratch_addr[dev];
+    return GDB_OK;
+}
+
+__global__ void k_sqna_clear(double *s, int nq) {
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < 2 * nq; k += gridDim.x * blockDim.x) s[k] = 0.0;
+    if (blockIdx.x == 0 && threadIdx.x < 2) s[SQNA_TAIL + threadIdx.x] = 0.0;
+}
+
+__global__ void k_sqna_weight_sum(const float *ff, int n, double *s) {
+    __shared__ double sm[32];
+    double v = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) v += ff ? ff[i] : 1.0;
+    v = warp_sum(v);
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double w = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+        w = warp_sum(w);
+        if (threadIdx.x == 0) atomicAdd(&s[SQNA_TAIL], w);
+    }
+}
+
+// Same tabulated-phase method as k_sq; positions are the caller's (n, 3)
+// float32 array, n-vector components lie in [-nmax, nmax].
+__global__ void __launch_bounds__(SQ_THREADS) k_sqna(const float *__restrict__ r, const float *__restrict__ ff, int n,
+                                                     const int *__restrict__ nvec, int nq, int nmax, float ilx,
+                                                     float ily, float ilz, double *s) {
+    extern __shared__ float2 tab[];
+    __shared__ float wsh[SQ_TILE];
+    const int span = 2 * nmax + 1, row = 3 * span;
+    const int q = blockIdx.x * SQ_THREADS + threadIdx.x;
+    bool ok = q < nq;
+    int nx = 0, ny = 0, nz = 0;
+    if (ok) {
+        const int a = nvec[3 * q], b = nvec[3 * q + 1], c = nvec[3 * q + 2];
+        if (a < -nmax || a > nmax || b < -nmax || b > nmax || c < -nmax || c > nmax) {
+            s[SQNA_TAIL + 1] = 1.0;
+            ok = false;
+        } else {
+            nx = a + nmax;
+            ny = b + nmax + span;
+            nz = c + nmax + 2 * span;
+        }
+    }
+    const float il[3] = {ilx, ily, ilz};
+    double sr = 0.0, si = 0.0;
+    const int p_begin = blockIdx.y * SQ_CHUNK;
+    const int p_end = min(n, p_begin + SQ_CHUNK);
+    for (int p0 = p_begin; p0 < p_end; p0 += SQ_TILE) {
+        const int np = min(SQ_TILE, p_end - p0);
+        __syncthreads();
+        for (int e = threadIdx.x; e < np * row; e += SQ_THREADS) {
+            const int pl = e / row, col = e % row;
+            const int d = col / span, k = col % span - nmax;
+            const float x = r[3 * (size_t)(p0 + pl) + d];
+            float sn, cs;
+            sincospif(2.0f * (float)k * (x * il[d]), &sn, &cs);
+            tab[pl * row + col] = make_float2(cs, sn);
+        }
+        if (threadIdx.x < np) wsh[threadIdx.x] = ff ? ff[p0 + threadIdx.x] : 1.0f;
+        __syncthreads();
+        if (ok) {
+            float tr = 0.f, ti = 0.f;
+            for (int pl = 0; pl < np; pl++) {
+                const float2 ex = tab[pl * row + nx], ey = tab[pl * row + ny], ez = tab[pl * row + nz];
+                const float xr = ex.x * ey.x - ex.y * ey.y, xi = ex.x * ey.y + ex.y * ey.x;
+                const float w = wsh[pl];
+                tr += w * (xr * ez.x - xi * ez.y);
+                ti += w * (xr * ez.y + xi * ez.x);
+            }
+            sr += tr;
+            si += ti;
+        }
+    }
+    if (ok) {
+        atomicAdd(&s[2 * q], sr);
+        atomicAdd(&s[2 * q + 1], si);
+    }
+}
+
+__global__ void k_sqna_finish(const double *s, int nq, double *re, double *im) {
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nq) return;
+    const double norm = 1.0 / sqrt(s[SQNA_TAIL]);
+    re[q] = s[2 * q] * norm;
+    im[q] = s[2 * q + 1] * norm;
+}
+
+}  // namespace
+
 extern "C" {
+
+int gdb_sq_compute_noalloc(int n, const float *r_dev, const float *ff_dev, const float box[3], int nq,
+                           const int32_t *n_vectors_dev, int n_max, double *rho_re_dev, double *rho_im_dev,
+                           void *stream) {
+    gdb_sim *h = nullptr;
+    if (n < 1 || nq < 1 || !r_dev || !box || !n_vectors_dev || !rho_re_dev || !rho_im_dev)
+        return aset(h, GDB_ERR_ARG, "gdb_sq_compute_noalloc: bad arguments");
+    if (nq > GDB_SQ_NOALLOC_MAX_Q)
+        return aset(h, GDB_ERR_ARG, "gdb_sq_compute_noalloc: more than 65536 q-vectors");
+    if (n_max < 0 || n_max > GDB_SQ_NOALLOC_MAX_N)
+        return aset(h, GDB_ERR_ARG, "gdb_sq_compute_noalloc: n_max must be in [0, 48]");
+    if (!(box[0] > 0.f && box[1] > 0.f && box[2] > 0.f))
+        return aset(h, GDB_ERR_ARG, "gdb_sq_compute_noalloc: non-positive box length");
+    int dev = 0;
+    ACK(cudaGetDevice(&dev));
+    double *s = nullptr;
+    int rc = sq_scratch_address(dev, &s);
+    if (rc) return aset(h, rc, "gdb_sq_compute_noalloc: scratch address lookup failed");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int span = 2 * n_max + 1;
+    const size_t smem = (size_t)SQ_TILE * 3 * span * sizeof(float2);
+    ACK(cudaFuncSetAttribute(k_sqna, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_sqna_clear<<<(2 * nq + 255) / 256, 256, 0, st>>>(s, nq);
+    k_sqna_weight_sum<<<64, 256, 0, st>>>(ff_dev, n, s);
+    dim3 grid((nq + SQ_THREADS - 1) / SQ_THREADS, (n + SQ_CHUNK - 1) / SQ_CHUNK);
+    k_sqna<<<grid, SQ_THREADS, smem, st>>>(r_dev, ff_dev, n, n_vectors_dev, nq, n_max, 1.0f / box[0],
+                                           1.0f / box[1], 1.0f / box[2], s);
+    k_sqna_finish<<<(nq + 255) / 256, 256, 0, st>>>(s, nq, rho_re_dev, rho_im_dev);
+    ACK(cudaGetLastError());
+    double flag = 0.0;
+    ACK(cudaMemcpyAsync(&flag, s + SQNA_TAIL + 1, sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACK(cudaStreamSynchronize(st));
+    if (flag != 0.0)
+        return aset(h, GDB_ERR_ARG, "gdb_sq_compute_noalloc: an n-vector component is outside [-n_max, n_max]");
+    return GDB_OK;
+}
 
 int gdb_rdf_update(gdb_sim *h, int bins, double r_max, uint64_t *out) {
     if (!h || !out) return aset(h, GDB_ERR_ARG, "gdb_rdf_update: NULL argument");

@@ -196,6 +196,23 @@ int gdb_rdf_compute(int n, const float *r, const int32_t *ptype, const float box
 int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], int nq, const int32_t *n_vectors,
                    double *rho_re, double *rho_im);
 
+/* S(q) without any device allocation.  No counterpart in the reference: it
+ * serves callers that cannot let the library call cudaMalloc -- programs whose
+ * own allocator or pre-reserved pool owns the GPU's memory, code under a hard
+ * device-memory budget, and call sites where allocating is not allowed.
+ * Inputs and outputs are the caller's DEVICE arrays: r_dev (n, 3) float32,
+ * ff_dev (n,) float32 or NULL (all 1), n_vectors_dev (nq, 3) int32 with every
+ * component in [-n_max, n_max], rho_re_dev / rho_im_dev (nq,) float64.  box is
+ * a host array.  stream is a cudaStream_t (NULL = default stream); the call
+ * waits for its work to finish.  Limits: nq <= 65536, n_max <= 48.
+ * Scratch is one static device array of 0.5 MiB that every GPU loading the
+ * library keeps until exit; it is shared by all calls, so calls that overlap
+ * on the GPU race.  The first call on a device looks up the array's address
+ * and should come before any stream capture. */
+int gdb_sq_compute_noalloc(int n, const float *r_dev, const float *ff_dev, const float box[3], int nq,
+                           const int32_t *n_vectors_dev, int n_max, double *rho_re_dev, double *rho_im_dev,
+                           void *stream);
+
 #ifdef __cplusplus
 }
 #endif
