@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--profile", action="store_true",
                    help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
     p.add_argument("--tp", type=int, default=0, help="lanes per particle (0 = library default)")
+    p.add_argument("--trace", action="store_true", help="with --profile: phase trace of the persistent kernel")
     return p.parse_args()
 
 
@@ -157,6 +158,29 @@ def ncu_traffic_per_atom_step():
     return None
 
 
+def trace_summary(tags, ns):
+    """Per-phase times from the persistent kernel's barrier trace (tags:
+    1 step, 2 evaluation, 3 rebuild phase, 4 rebuild done, 5 start)."""
+    step_us, rebuild_us, phase_us = [], [], []
+    start = None
+    for k in range(1, len(tags)):
+        dt = (ns[k] - ns[k - 1]) / 1e3
+        if tags[k] == 1 and tags[k - 1] in (1, 4):
+            step_us.append(dt)
+        if tags[k] == 3 and tags[k - 1] in (1, 5) and start is None:
+            start = ns[k - 1]
+        if tags[k] in (3, 4):
+            phase_us.append(dt)
+        if tags[k] == 4 and start is not None:
+            rebuild_us.append((ns[k] - start) / 1e3)
+            start = None
+    med = lambda x: float(np.median(x)) if x else None
+    return {"entries": int(len(tags)), "steps": len(step_us), "step_us_median": med(step_us),
+            "step_us_mean": float(np.mean(step_us)) if step_us else None, "rebuilds": len(rebuild_us),
+            "rebuild_us_median": med(rebuild_us),
+            "rebuild_phase_us": [round(x, 1) for x in phase_us[:5]]}
+
+
 def cpu_reference(args, n, steps, seed=0):
     """The oracle on the host cores: ka workload, `steps` steps after one
     build.  Returns (MATS, threads, seconds)."""
@@ -213,7 +237,8 @@ def main():
     pp = workloads.ka_pair_potential(max_num_nbs=300)
     integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
     block = min(args.block, max(1, args.steps))
-    plan = {"pb": 64, "tp": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False, "nblist": "linked lists"}
+    plan = {"pb": 64, "tp": 1, "lanes": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
+            "nblist": "linked lists"}
     sim = gp.Simulation(conf, pp, integ, [gp.ScalarSaver(max(1, block // 8))], num_timeblocks=8,
                         steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
     dev = sim._sim
@@ -225,11 +250,17 @@ def main():
     nblocks = max(1, args.steps // block)
     steps = nblocks * block
     if args.profile:
+        if args.trace:
+            dev.set_trace(1 << 20)
         ms = sum(dev.run(float(b * block * 0.005), block) for b in range(nblocks))
         mean_nbs, max_nbs = dev.nblist_stats()
-        print(json.dumps({"profile": True, "n": n, "steps": steps, "ms_per_step": ms / steps,
-                          "mats": n * steps / ms / 1e3, "mean_neighbours": mean_nbs,
-                          "tp": args.tp, "step_kernel_ms": dev.time_step_kernel(20)}), flush=True)
+        out = {"profile": True, "n": n, "steps": steps, "ms_per_step": ms / steps, "mats": n * steps / ms / 1e3,
+               "mean_neighbours": mean_nbs, "tp": args.tp}
+        if args.trace:
+            out["trace"] = trace_summary(*dev.trace(1 << 20))
+            dev.set_trace(0)
+        out["step_kernel_ms"] = dev.time_step_kernel(20)
+        print(json.dumps(out), flush=True)
         return
     clocks = ClockSampler(local)
     barrier(pg)

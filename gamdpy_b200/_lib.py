@@ -64,6 +64,8 @@ SIGNATURES = {
     "gdb_get_saved_configurations": ([_P, _P, _i], _i),
     "gdb_eval_forces": ([_P], _i),
     "gdb_sim_run": ([_P, _d, _i, _P], _i),
+    "gdb_set_trace": ([_P, _i], _i),
+    "gdb_get_trace": ([_P, _P, _i, _P], _i),
     "gdb_time_step_kernel": ([_P, _i, _P], _i),
     "gdb_nblist_stats": ([_P, _P, _P], _i),
     "gdb_get_scalar_rows": ([_P, _P, _i], _i),
@@ -235,6 +237,17 @@ class Sim:
         ms = ctypes.c_float(0.0)
         self.call("gdb_sim_run", float(time_zero), int(steps), ctypes.byref(ms))
         return ms.value
+
+    def set_trace(self, capacity):
+        self.call("gdb_set_trace", int(capacity))
+
+    def trace(self, capacity=1 << 16):
+        """Phase trace entries as (tag, ns) arrays; restarts the trace."""
+        buf = np.zeros(capacity, np.uint64)
+        cnt = ctypes.c_int(0)
+        self.call("gdb_get_trace", ptr(buf), int(capacity), ctypes.byref(cnt))
+        buf = buf[: cnt.value]
+        return (buf >> np.uint64(56)).astype(np.int64), (buf & np.uint64((1 << 56) - 1)).astype(np.int64)
 
     def time_step_kernel(self, reps):
         ms = ctypes.c_float(0.0)

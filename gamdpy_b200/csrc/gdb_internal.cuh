@@ -10,10 +10,9 @@
 //   frc     float4 (fx, fy, fz, 0)         written by force-only evaluations
 //   rref    float4 positions at the last neighbour-list build
 //   orig    int    user index of each slot
-//   nbl     int    neighbour list, "sliced ELL": entry k of particle i lives at
-//                  (k / tp) * (stride * tp) + i * tp + (k % tp), so the tp lanes
-//                  that share a particle and the consecutive particles of a warp
-//                  read one contiguous 128-byte line per iteration
+//   nbl     int    neighbour list in chunks of four: entry k of particle i lives
+//                  at (k / 4) * (stride * 4) + i * 4 + (k % 4); one int4 load
+//                  gives four neighbours, a warp reads 512 contiguous bytes
 //   nbc     int    neighbour counts
 //   pscal   float  per-particle U, W, lapU, K, Fsq (5 planes of n)
 #pragma once
@@ -52,6 +51,7 @@ struct PairTable {
 // Device control block (one per simulation).
 struct DevCtrl {
     int rebuild;       // 1 = neighbour list must be rebuilt before the next force evaluation
+    int rebuild_next;  // set during a persistent step, promoted to `rebuild` at the barrier
     int maxcount;      // largest neighbour count of the last build
     int nrebuild;      // number of builds (gamdpy nbflag[2])
     unsigned status;   // GDB_STATUS_* bits
@@ -63,10 +63,29 @@ struct DevCtrl {
     float xi;          // Nose-Hoover friction (NVT.thermostat_state[0])
     float sumK;        // last kinetic-energy sum (float copy, NVT.thermostat_state[1] analogue)
     double time_zero;  // simulated time at the start of the timeblock
+    double evalU, evalW;  // sums of the last force-only evaluation
+    unsigned bar_count;   // grid barrier of the persistent kernel
+    unsigned bar_gen;
+    int abort;            // set when a barrier wait timed out
+    unsigned long long *trace;  // optional phase trace: (tag << 56) | globaltimer ns
+    int trace_cap;
+    int trace_len;
 };
 
-__device__ __forceinline__ int nb_index(int i, int k, int tp, int stride) {
-    return (k / tp) * (stride * tp) + i * tp + (k % tp);
+// Phase trace (block 0, thread 0 of the persistent kernel): one entry per
+// barrier with a tag naming the phase that just finished.
+enum TraceTag { TR_STEP = 1, TR_EVAL = 2, TR_REBUILD_PHASE = 3, TR_REBUILD_DONE = 4, TR_START = 5 };
+
+__device__ __forceinline__ void trace_mark(DevCtrl *c, int tag) {
+    if (c->trace && blockIdx.x == 0 && threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        const int k = c->trace_len;
+        if (k < c->trace_cap) {
+            c->trace[k] = ((unsigned long long)tag << 56) | (t & 0x00ffffffffffffffULL);
+            c->trace_len = k + 1;
+        }
+    }
 }
 
 // Minimum-image displacement of one component exactly as

@@ -36,15 +36,11 @@
 
 #include "../../include/gamdb200.h"
 #include "gdb_internal.cuh"
+#include "md_phases.cuh"
 
 using namespace gdb;
 
 namespace {
-
-constexpr int NQ = 9;  // K, U, W, lapU, Fsq, px, py, pz, m
-constexpr int SCAN_CHUNK = 2048;
-constexpr int MODE_STEP = 0;
-constexpr int MODE_EVAL = 1;
 
 char g_lib_error[512] = "";
 
@@ -93,9 +89,13 @@ struct gdb_sim {
     int partial_cap = 0;
     double *rows = nullptr;
     int rows_cap = 0;
+    unsigned long long *trace = nullptr;
+    int trace_cap = 0;
     float *conf = nullptr;  // ConfigurationSaver frames
     int conf_per_block = 0;
     int cur = 0;
+    int num_sms = 148;
+    bool persistent = true;
     bool uploaded = false;
     // graphs: [parity] for chunks of GRAPH_STEPS steps
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -133,617 +133,176 @@ static int set_err(gdb_sim *h, int code, const char *fmt, ...) {
     } while (0)
 
 // ---------------------------------------------------------------------------
-// kernels: neighbour list
+// standalone kernels (one phase each; the rebuild chain returns at once
+// unless the rebuild flag is set) -- launched in a CUDA graph
 // ---------------------------------------------------------------------------
-
-// N^2 build (interactions/nblist.py:88-143): one warp per particle, lanes
-// stride over j; ballot + popc append the hits in ascending j, so the list is
-// deterministic.  Full list, no exclusions.
 template <bool FMA>
-__global__ void __launch_bounds__(GDB_BLOCK) k_nbl_nsq(const float4 *__restrict__ pos, int n, float Lx, float Ly,
-                                                       float Lz, float cps2, int *__restrict__ nbl,
-                                                       int *__restrict__ nbc, int stride, int tp, int max_nbs,
-                                                       DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    const int lane = threadIdx.x & 31;
-    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (i >= n) return;
-    const float4 pi = pos[i];
-    int count = 0;
-    for (int j0 = 0; j0 < n; j0 += 32) {
-        const int j = j0 + lane;
-        bool hit = false;
-        if (j < n && j != i) {
-            const float4 pj = pos[j];
-            hit = dist_sq_exact<FMA>(pj, pi, Lx, Ly, Lz) < cps2;
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (hit) {
-            const int k = count + __popc(m & ((1u << lane) - 1u));
-            if (k < max_nbs) nbl[nb_index(i, k, tp, stride)] = j;
-        }
-        count += __popc(m);
-    }
-    if (lane == 0) {
-        nbc[i] = count;
-        atomicMax(&ctrl->maxcount, count);
-    }
+__global__ void __launch_bounds__(GDB_BLOCK) k_nbl_nsq(SimArgs a, int cur) {
+    if (!a.ctrl->rebuild) return;
+    phase_nbl_nsq<FMA, true>(a, cur);
 }
-
-// Cell coordinate as nblist_linked_lists.py:127 (float64 arithmetic, Python
-// modulo).  Non-finite coordinates map to cell 0 and raise the NAN bit.
-__device__ __forceinline__ int cell_coord(float x, float L, int nc, DevCtrl *ctrl) {
-    double v = ((double)x + 0.5 * (double)L) * (double)nc / (double)L;
-    if (!(v > -1e9 && v < 1e9)) {
-        atomicOr(&ctrl->status, GDB_STATUS_NAN);
-        return 0;
-    }
-    long long c = (long long)floor(v);
-    long long m = c % nc;
-    if (m < 0) m += nc;
-    return (int)m;
+__global__ void __launch_bounds__(GDB_BLOCK) k_cell_assign(SimArgs a, int cur) {
+    if (!a.ctrl->rebuild) return;
+    phase_cell_assign<true>(a, cur);
 }
-
-__global__ void k_cell_assign(const float4 *__restrict__ pos, int n, float Lx, float Ly, float Lz, int ncx,
-                              int ncy, int ncz, int *__restrict__ pcell, int *__restrict__ prank,
-                              int *__restrict__ cell_count, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const float4 p = pos[i];
-    const int cx = cell_coord(p.x, Lx, ncx, ctrl);
-    const int cy = cell_coord(p.y, Ly, ncy, ctrl);
-    const int cz = cell_coord(p.z, Lz, ncz, ctrl);
-    // linear index with x fastest: the x-neighbours of a cell are contiguous
-    const int c = (cz * ncy + cy) * ncx + cx;
-    pcell[i] = c;
-    prank[i] = atomicAdd(&cell_count[c], 1);
+__global__ void __launch_bounds__(GDB_BLOCK) k_scan_partial(SimArgs a) {
+    if (!a.ctrl->rebuild) return;
+    phase_scan_partial(a);
 }
-
-// Block-wide exclusive scan of SCAN_CHUNK ints (8 per thread).
-__device__ __forceinline__ void chunk_scan(const int *in, int len, int base, int *out_excl, int add, int *total,
-                                           int *sm /* 32 */) {
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    int v[8];
-    int s = 0;
-#pragma unroll
-    for (int q = 0; q < 8; q++) {
-        const int idx = base + t * 8 + q;
-        v[q] = idx < len ? in[idx] : 0;
-        s += v[q];
-    }
-    int incl = s;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int y = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += y;
-    }
-    if (lane == 31) sm[warp] = incl;
-    __syncthreads();
-    if (warp == 0) {
-        int w = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0;
-        int wi = w;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const int y = __shfl_up_sync(0xffffffffu, wi, o);
-            if (lane >= o) wi += y;
-        }
-        sm[lane] = wi - w;  // exclusive prefix of warp totals
-        if (lane == 31 && total) *total = wi;
-    }
-    __syncthreads();
-    if (out_excl) {
-        int run = add + sm[warp] + incl - s;
-#pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int idx = base + t * 8 + q;
-            if (idx < len) out_excl[idx] = run;
-            run += v[q];
-        }
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(GDB_BLOCK) k_scan_top(SimArgs a) {
+    if (!a.ctrl->rebuild) return;
+    block_scan_chunks(a);
 }
-
-__global__ void __launch_bounds__(GDB_BLOCK) k_scan_partial(const int *__restrict__ in, int len, int *__restrict__ bsum,
-                                                            DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    __shared__ int sm[32];
-    __shared__ int tot;
-    chunk_scan(in, len, blockIdx.x * SCAN_CHUNK, nullptr, 0, &tot, sm);
-    if (threadIdx.x == 0) bsum[blockIdx.x] = tot;
+__global__ void __launch_bounds__(GDB_BLOCK) k_scan_final(SimArgs a) {
+    if (!a.ctrl->rebuild) return;
+    phase_scan_final(a);
 }
-
-// Exclusive scan of the block sums in one block (nb <= 8 * 1024 * ... handled
-// by looping over chunks serially).
-__global__ void __launch_bounds__(GDB_BLOCK) k_scan_top(int *__restrict__ bsum, int nb, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    __shared__ int sm[32];
-    __shared__ int tot;
-    int carry = 0;
-    for (int base = 0; base < nb; base += SCAN_CHUNK) {
-        chunk_scan(bsum, nb, base, bsum, carry, &tot, sm);
-        carry += tot;
-        __syncthreads();
-    }
+__global__ void __launch_bounds__(GDB_BLOCK) k_scatter(SimArgs a) {
+    if (!a.ctrl->rebuild) return;
+    phase_scatter(a);
 }
-
-__global__ void __launch_bounds__(GDB_BLOCK) k_scan_final(const int *__restrict__ in, int len,
-                                                          const int *__restrict__ bsum, int *__restrict__ out,
-                                                          int n, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    __shared__ int sm[32];
-    chunk_scan(in, len, blockIdx.x * SCAN_CHUNK, out, bsum[blockIdx.x], nullptr, sm);
-    if (blockIdx.x == 0 && threadIdx.x == 0) out[len] = n;
+__global__ void __launch_bounds__(GDB_BLOCK) k_sort_cells(SimArgs a) {
+    if (!a.ctrl->rebuild) return;
+    phase_sort_cells(a);
 }
-
-__global__ void k_scatter(const int *__restrict__ pcell, const int *__restrict__ prank,
-                          const int *__restrict__ cell_start, int *__restrict__ perm, int n, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    perm[cell_start[pcell[i]] + prank[i]] = i;
+__global__ void __launch_bounds__(GDB_BLOCK) k_gather(SimArgs a, int cur) {
+    if (!a.ctrl->rebuild) return;
+    phase_gather(a, cur);
 }
-
-// Order every cell's particles by user index: the atomics of k_cell_assign
-// rank them arbitrarily, this makes the layout (and every sum) deterministic.
-__global__ void k_sort_cells(const int *__restrict__ cell_start, int ncell, int *__restrict__ perm,
-                             const int *__restrict__ orig, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncell) return;
-    const int a = cell_start[c], b = cell_start[c + 1];
-    for (int x = a + 1; x < b; x++) {
-        const int v = perm[x];
-        const int key = orig[v];
-        int y = x - 1;
-        while (y >= a && orig[perm[y]] > key) {
-            perm[y + 1] = perm[y];
-            y--;
-        }
-        perm[y + 1] = v;
-    }
-}
-
-__global__ void k_gather(const int *__restrict__ perm, int n, const float4 *__restrict__ pos,
-                         const float4 *__restrict__ vel, const int4 *__restrict__ img, const int *__restrict__ orig,
-                         const float *__restrict__ pscal, const int *__restrict__ pcell, float4 *__restrict__ pos_t,
-                         float4 *__restrict__ vel_t, int4 *__restrict__ img_t, int *__restrict__ orig_t,
-                         float *__restrict__ pscal_t, int *__restrict__ scell, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const int i = perm[s];
-    pos_t[s] = pos[i];
-    vel_t[s] = vel[i];
-    img_t[s] = img[i];
-    orig_t[s] = orig[i];
-    scell[s] = pcell[i];
-    // K and Fsq planes (3, 4) travel with the particle; U, W, lapU are rewritten
-    // by the next force evaluation
-    pscal_t[3 * (size_t)n + s] = pscal[3 * (size_t)n + i];
-    pscal_t[4 * (size_t)n + s] = pscal[4 * (size_t)n + i];
-}
-
-// Cell-list build (nblist_linked_lists.py:133-183 semantics: every particle
-// of the 5x5x5 stencil of cells with dist_sq < (max_cut+skin)^2, j != i).
-// Particles are sorted by cell with x fastest, so the five x-cells of one
-// (dy, dz) row are one contiguous slot range (two at the x wrap).  Grids with
-// fewer than five cells in a dimension visit each cell once.
 template <bool FMA>
-__global__ void __launch_bounds__(GDB_BLOCK) k_nbl_cells(const float4 *__restrict__ pos, const int *__restrict__ scell,
-                                                         const int *__restrict__ cell_start, int n, float Lx, float Ly,
-                                                         float Lz, int ncx, int ncy, int ncz, float cps2,
-                                                         int *__restrict__ nbl, int *__restrict__ nbc, int stride,
-                                                         int tp, int max_nbs, DevCtrl *ctrl) {
-    if (!ctrl->rebuild) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n) return;
-    const float4 pi = pos[s];
-    const int c = scell[s];
-    const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
-    const int ry = ncy < 5 ? ncy : 5, rz = ncz < 5 ? ncz : 5;
-    const int oy = ncy < 5 ? 0 : cy - 2, oz = ncz < 5 ? 0 : cz - 2;
-    int count = 0;
-    for (int a = 0; a < rz; a++) {
-        int z = oz + a;
-        z = (z % ncz + ncz) % ncz;
-        for (int b = 0; b < ry; b++) {
-            int y = oy + b;
-            y = (y % ncy + ncy) % ncy;
-            const int rowbase = (z * ncy + y) * ncx;
-            // x segments
-            int seg_lo[2], seg_hi[2], nseg;
-            if (ncx <= 5) {
-                seg_lo[0] = rowbase;
-                seg_hi[0] = rowbase + ncx;
-                nseg = 1;
-            } else {
-                const int x0 = cx - 2, x1 = cx + 2;
-                if (x0 >= 0 && x1 < ncx) {
-                    seg_lo[0] = rowbase + x0;
-                    seg_hi[0] = rowbase + x1 + 1;
-                    nseg = 1;
-                } else if (x0 < 0) {
-                    seg_lo[0] = rowbase + x0 + ncx;
-                    seg_hi[0] = rowbase + ncx;
-                    seg_lo[1] = rowbase;
-                    seg_hi[1] = rowbase + x1 + 1;
-                    nseg = 2;
-                } else {
-                    seg_lo[0] = rowbase + x0;
-                    seg_hi[0] = rowbase + ncx;
-                    seg_lo[1] = rowbase;
-                    seg_hi[1] = rowbase + x1 - ncx + 1;
-                    nseg = 2;
-                }
-            }
-            for (int q = 0; q < nseg; q++) {
-                const int j0 = cell_start[seg_lo[q]], j1 = cell_start[seg_hi[q]];
-                for (int j = j0; j < j1; j++) {
-                    if (j == s) continue;
-                    const float4 pj = pos[j];
-                    if (dist_sq_exact<FMA>(pj, pi, Lx, Ly, Lz) < cps2) {
-                        if (count < max_nbs) nbl[nb_index(s, count, tp, stride)] = j;
-                        count++;
-                    }
-                }
-            }
-        }
-    }
-    nbc[s] = count;
-    atomicMax(&ctrl->maxcount, count);
+__global__ void __launch_bounds__(GDB_BLOCK) k_nbl_cells(SimArgs a) {
+    if (!a.ctrl->rebuild) return;
+    phase_nbl_cells<FMA>(a);
+}
+__global__ void __launch_bounds__(GDB_BLOCK) k_finish_cells(SimArgs a, int cur) {
+    if (!a.ctrl->rebuild) return;
+    phase_finish_cells(a, cur);
+}
+__global__ void k_rebuild_done(DevCtrl *ctrl) {
+    if (ctrl->rebuild) rebuild_done(ctrl);
 }
 
-// Last kernel of a rebuild: move the reordered state into place (cell mode),
-// record r_ref, clear the cell counters for the next build, and (last block)
-// clear the rebuild flag and count the build (gamdpy nbflag[0], nbflag[2]).
-template <bool CELLS>
-__global__ void k_rebuild_finish(int n, float4 *__restrict__ pos, float4 *__restrict__ vel, int4 *__restrict__ img,
-                                 int *__restrict__ orig, float *__restrict__ pscal, const float4 *__restrict__ pos_t,
-                                 const float4 *__restrict__ vel_t, const int4 *__restrict__ img_t,
-                                 const int *__restrict__ orig_t, const float *__restrict__ pscal_t,
-                                 float4 *__restrict__ rref, int *__restrict__ cell_count, int ncell,
-                                 DevCtrl *ctrl) {
-    __shared__ bool last;
-    if (!ctrl->rebuild) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < n) {
-        if (CELLS) {
-            const float4 p = pos_t[s];
-            pos[s] = p;
-            rref[s] = p;
-            vel[s] = vel_t[s];
-            img[s] = img_t[s];
-            orig[s] = orig_t[s];
-            pscal[3 * (size_t)n + s] = pscal_t[3 * (size_t)n + s];
-            pscal[4 * (size_t)n + s] = pscal_t[4 * (size_t)n + s];
-        } else {
-            rref[s] = pos[s];
-        }
-    }
-    if (CELLS)
-        for (int c = s; c < ncell; c += gridDim.x * blockDim.x) cell_count[c] = 0;
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&ctrl->ticket2, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (last && threadIdx.x == 0) {
-        ctrl->rebuild = 0;
-        ctrl->nrebuild += 1;
-        ctrl->ticket2 = 0;
-    }
-}
-
-// ---------------------------------------------------------------------------
-// kernels: fused force + integrate step
-// ---------------------------------------------------------------------------
-struct StepArgs {
-    const float4 *pos;
-    float4 *pos_next;
-    float4 *vel;
-    int4 *img;
-    const float4 *rref;
-    float4 *frc;
-    const int *nbl;
-    const int *nbc;
-    float *pscal;
-    double *partials;
-    double *rows;
-    DevCtrl *ctrl;
-    int n, stride, max_nbs;
-    float Lx, Ly, Lz;
-    float skin2q;  // skin*skin*0.25 (nblist.py / orthorhombic.py:131)
-    float dt;
-    float omega2;
-    long long dof;  // N*D - D (NVT.py:35)
-    int tfunc;
-    float tp0, tp1, tp2, tp3;
-    int every, reset_every;
-    int nrows;            // ScalarSaver rows allocated (writes beyond are dropped)
-    float *conf;          // ConfigurationSaver frames (conf_per_block, 2, n, 3) or null
-    int conf_per_block;
-    const int *orig;      // user index of each slot
-};
-
-// ConfigurationSaver save slot of a step (runtime_actions/configuration_saver.py:
-// 115-141): step 0 -> 0, step 2^b -> b + 1, others -> -1.
-__device__ __forceinline__ int conf_save_index(int step) {
-    if (step == 0) return 0;
-    if (step & (step - 1)) return -1;
-    return 32 - __clz(step);
-}
-
-__device__ __forceinline__ double target_temperature(const StepArgs &a, double t) {
-    if (a.tfunc == GDB_TFUNC_RAMP) {  // misc/make_function.py:27-32
-        if (t < a.tp1) return a.tp0;
-        if (t < a.tp3) return a.tp0 + (t - a.tp1) * ((double)(a.tp2 - a.tp0) / (double)(a.tp3 - a.tp1));
-        return a.tp2;
-    }
-    return a.tp0;
-}
-
-// Loop over particle i's neighbours (lane `sub` of TP): pair_potential.py:223-231
-// with the full-list calculator :164-178.
-template <int TP, bool NT1, bool REC>
-__device__ __forceinline__ void neighbour_loop(const StepArgs &a, const PairEntry *tab, int nt, int i, int sub,
-                                               float4 pi, float &fx, float &fy, float &fz, float &u, float &w,
-                                               float &l) {
-    const int ti = NT1 ? 0 : ptype_of(pi);
-    const int cnt = min(a.nbc[i], a.max_nbs);
-    const int *row = a.nbl + (size_t)i * TP + sub;
-    const size_t slice = (size_t)a.stride * TP;
-    const PairEntry *trow = tab + ti * nt;
-    const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
-    const float hLx = 0.5f * Lx, hLy = 0.5f * Ly, hLz = 0.5f * Lz;
-    int kk = 0;
-#pragma unroll 2
-    for (int k = sub; k < cnt; k += TP, kk++) {
-        const int j = __ldg(row + kk * slice);
-        const float4 pj = __ldg(a.pos + j);
-        float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
-        dx = dx > hLx ? dx - Lx : (dx < -hLx ? dx + Lx : dx);
-        dy = dy > hLy ? dy - Ly : (dy < -hLy ? dy + Ly : dy);
-        dz = dz > hLz ? dz - Lz : (dz < -hLz ? dz + Lz : dz);
-        const float d2 = dx * dx + dy * dy + dz * dz;
-        const PairEntry &e = NT1 ? tab[0] : trow[ptype_of(pj)];
-        if (d2 < e.cut2) {
-            const float inv2 = __fdividef(1.0f, d2);
-            const float x2 = e.c * inv2;
-            const float x6 = x2 * x2 * x2;
-            const float x12 = x6 * x6;
-            const float s = (e.cs12 * x12 + e.cs6 * x6) * inv2 - e.sc;
-            fx -= dx * s;
-            fy -= dy * s;
-            fz -= dz * s;
-            if (REC) {
-                const float r = sqrtf(d2);
-                const float uu = e.cu12 * x12 + e.cu6 * x6 - e.uc + e.sccut * (r - e.cut);
-                u += 0.5f * uu;
-                w += d2 * s * (1.0f / 6.0f);
-                l += -2.0f * s + (e.cm12 * x12 + e.cm6 * x6) * inv2;
-            }
-        }
-    }
-}
-
-template <int TP, bool NT1, int INTEG, int MODE>
-__global__ void __launch_bounds__(GDB_BLOCK) k_step(StepArgs a, PairTable tab) {
-    __shared__ PairEntry s_tab[NT1 ? 1 : GDB_MAX_TYPES * GDB_MAX_TYPES];
-    __shared__ double s_red[NQ * 32];
-    __shared__ bool s_last;
-    const int nt = tab.nt;
+template <bool NT1>
+__device__ __forceinline__ void load_table(const PairTable &tab, PairEntry *s_tab) {
     if (NT1) {
         if (threadIdx.x == 0) s_tab[0] = tab.e[0];
     } else {
-        for (int t = threadIdx.x; t < nt * nt; t += blockDim.x) s_tab[t] = tab.e[t];
+        for (int t = threadIdx.x; t < tab.nt * tab.nt; t += blockDim.x) s_tab[t] = tab.e[t];
     }
     __syncthreads();
+}
 
+// one step (or the force-only evaluation); the last block to finish does
+// the float64 bookkeeping
+// register budget: 64 per thread (4 blocks/SM) for one lane per particle,
+// 80 (3 blocks/SM) when lanes share a particle (measured best on B200)
+#define GDB_STEP_MINBLOCKS(TP) ((TP) == 1 ? 4 : 3)
+
+template <int TP, bool NT1, int INTEG, int MODE>
+__global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_step(SimArgs a, PairTable tab, int cur) {
+    __shared__ PairEntry s_tab[NT1 ? 1 : GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    __shared__ bool s_last;
+    load_table<NT1>(tab, s_tab);
     DevCtrl *ctrl = a.ctrl;
     const int step = ctrl->step;
-    const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
-    const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
-    const int par = step & 1, ppar = par ^ 1;
-    const bool shift_pending = ctrl->pending[ppar] != 0;
-
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    const int i = gt / TP, sub = gt % TP;
-    const bool active = i < a.n;
-    const size_t n = a.n;
-    float fx = 0.f, fy = 0.f, fz = 0.f, u = 0.f, w = 0.f, l = 0.f;
-    float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (active) {
-        pi = a.pos[i];
-        if (rec)
-            neighbour_loop<TP, NT1, true>(a, s_tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
-        else
-            neighbour_loop<TP, NT1, false>(a, s_tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
-    }
-    if (TP > 1) {
-#pragma unroll
-        for (int o = TP / 2; o > 0; o >>= 1) {
-            fx += __shfl_xor_sync(0xffffffffu, fx, o);
-            fy += __shfl_xor_sync(0xffffffffu, fy, o);
-            fz += __shfl_xor_sync(0xffffffffu, fz, o);
-            if (rec) {
-                u += __shfl_xor_sync(0xffffffffu, u, o);
-                w += __shfl_xor_sync(0xffffffffu, w, o);
-                l += __shfl_xor_sync(0xffffffffu, l, o);
-            }
-        }
-    }
-
-    double red[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) red[q] = 0.0;
-    bool moved = false;
-    if (active && sub == 0 && a.conf) {
-        const int si = conf_save_index(step);
-        if (si >= 0 && si < a.conf_per_block) {
-            const int4 im = a.img[i];
-            const int u = a.orig[i];
-            float *fr = a.conf + ((size_t)si * 2) * n * 3;
-            fr[3 * (size_t)u] = pi.x;
-            fr[3 * (size_t)u + 1] = pi.y;
-            fr[3 * (size_t)u + 2] = pi.z;
-            fr += n * 3;
-            fr[3 * (size_t)u] = (float)im.x;
-            fr[3 * (size_t)u + 1] = (float)im.y;
-            fr[3 * (size_t)u + 2] = (float)im.z;
-        }
-    }
-    if (active && sub == 0) {
-        float4 v = a.vel[i];
-        if (shift_pending) {
-            const float *sh = ctrl->shift[ppar];
-            v.x -= sh[0];
-            v.y -= sh[1];
-            v.z -= sh[2];
-        }
-        const float fsq = fx * fx + fy * fy + fz * fz;
-        if (rec) {
-            a.pscal[i] = u;
-            a.pscal[n + i] = w;
-            a.pscal[2 * n + i] = l;
-        }
-        if (MODE == MODE_EVAL) {
-            a.frc[i] = make_float4(fx, fy, fz, 0.f);
-            if (shift_pending) a.vel[i] = v;
-        } else {
-            const float m = v.w;
-            float kin;
-            float r[3] = {pi.x, pi.y, pi.z};
-            float vv[3] = {v.x, v.y, v.z};
-            const float ff[3] = {fx, fy, fz};
-            if (INTEG == GDB_INTEGRATOR_NVE) {  // integrators/NVE.py:78-97
-                kin = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    float v_mean = vv[k];
-                    vv[k] += ff[k] / m * a.dt;
-                    v_mean += vv[k];
-                    v_mean *= 0.5f;
-                    kin += 0.5f * m * v_mean * v_mean;
-                    r[k] += vv[k] * a.dt;
-                }
-            } else {  // integrators/NVT.py:196-215
-                const float factor = 0.5f * ctrl->xi * a.dt;
-                const float plus = 1.0f / (1.0f + factor);
-                const float minus = 1.0f - factor;
-                kin = 0.f;
-#pragma unroll
-                for (int k = 0; k < 3; k++) {
-                    vv[k] = plus * (minus * vv[k] + ff[k] / m * a.dt);
-                    kin += 0.5f * m * vv[k] * vv[k];
-                    r[k] += vv[k] * a.dt;
-                }
-            }
-            // periodic boundaries with image counters (orthorhombic.py:75-86)
-            const float L[3] = {a.Lx, a.Ly, a.Lz};
-            int dimg[3] = {0, 0, 0};
-            bool wrapped = false;
-#pragma unroll
-            for (int k = 0; k < 3; k++) {
-                if (r[k] * 2.0f > L[k]) {
-                    r[k] -= L[k];
-                    dimg[k] += 1;
-                    wrapped = true;
-                }
-                if (r[k] * 2.0f < -L[k]) {
-                    r[k] += L[k];
-                    dimg[k] -= 1;
-                    wrapped = true;
-                }
-            }
-            if (wrapped) {
-                int4 im = a.img[i];
-                im.x += dimg[0];
-                im.y += dimg[1];
-                im.z += dimg[2];
-                a.img[i] = im;
-            }
-            if (!(fabsf(r[0]) <= L[0] && fabsf(r[1]) <= L[1] && fabsf(r[2]) <= L[2]))
-                atomicOr(&ctrl->status, GDB_STATUS_NAN);
-            const float4 pn = make_float4(r[0], r[1], r[2], pi.w);
-            a.pos_next[i] = pn;
-            a.vel[i] = make_float4(vv[0], vv[1], vv[2], m);
-            a.pscal[3 * n + i] = kin;
-            a.pscal[4 * n + i] = fsq;
-            // skin check for the next step (nblist.py:57-86)
-            const float4 rr = a.rref[i];
-            moved = dist_sq_exact<false>(pn, rr, a.Lx, a.Ly, a.Lz) > a.skin2q;
-            red[0] = kin;
-            red[5] = (double)m * vv[0];
-            red[6] = (double)m * vv[1];
-            red[7] = (double)m * vv[2];
-            red[8] = m;
-        }
-        red[1] = u;
-        red[2] = w;
-        red[3] = l;
-        red[4] = fsq;
-    }
-    if (MODE == MODE_STEP) {
-        if (__syncthreads_or(moved) && threadIdx.x == 0) ctrl->rebuild = 1;
-    }
-    const bool need_red = MODE == MODE_STEP && (INTEG == GDB_INTEGRATOR_NVT || rec || reset);
-    if (need_red) {
-        block_sum<NQ>(red, s_red);
-        if (threadIdx.x == 0) {
-#pragma unroll
-            for (int q = 0; q < NQ; q++) a.partials[(size_t)blockIdx.x * NQ + q] = red[q];
-        }
-    }
+    phase_step<TP, NT1, INTEG, MODE, true, false>(a, s_tab, tab.nt, cur, step, s_red);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
     __syncthreads();
     if (!s_last) return;
+    finalize_step<MODE>(a, step, gridDim.x, s_red);
+    if (threadIdx.x == 0) ctrl->ticket = 0;
+}
 
-    // last block: fixed-order float64 reduction of the partials
-    double tot[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) tot[q] = 0.0;
-    if (need_red) {
-        for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-#pragma unroll
-            for (int q = 0; q < NQ; q++) tot[q] += __ldcg(a.partials + (size_t)b * NQ + q);
-        }
-        block_sum<NQ>(tot, s_red);
+// Rebuild inside the persistent kernel: the same phases with grid barriers.
+template <bool FMA>
+__device__ bool rebuild_persistent(const SimArgs &a, int cur) {
+    DevCtrl *c = a.ctrl;
+    auto none = [] {};
+    if (a.nb_kind == GDB_NBLIST_NSQ) {
+        phase_nbl_nsq<FMA, false>(a, cur);
+        const bool ok = grid_barrier(c, [&] {
+            if (threadIdx.x == 0) rebuild_done(c);
+        });
+        trace_mark(c, TR_REBUILD_DONE);
+        return ok;
     }
-    if (threadIdx.x == 0) {
-        if (MODE == MODE_STEP) {
-            const double time = ctrl->time_zero + (double)step * (double)a.dt;
-            if (INTEG == GDB_INTEGRATOR_NVT) {  // NVT.py:226-237
-                const double T = target_temperature(a, time);
-                const double dev = 2.0 * tot[0] / ((double)a.dof * T) - 1.0;
-                ctrl->xi = (float)((double)ctrl->xi + (double)(a.dt * a.omega2) * dev);
-                ctrl->sumK = (float)tot[0];
-            }
-            if (rec && step / a.every < a.nrows) {  // scalar_saver.py:274-288
-                double *row = a.rows + (size_t)(step / a.every) * GDB_NUM_SCALARS;
-                row[GDB_SCALAR_U] = tot[1];
-                row[GDB_SCALAR_W] = tot[2];
-                row[GDB_SCALAR_LAPU] = tot[3];
-                row[GDB_SCALAR_K] = tot[0];
-                row[GDB_SCALAR_FSQ] = tot[4];
-            }
-            if (reset) {  // momentum_reset.py:379-393
-                ctrl->shift[par][0] = (float)(tot[5] / tot[8]);
-                ctrl->shift[par][1] = (float)(tot[6] / tot[8]);
-                ctrl->shift[par][2] = (float)(tot[7] / tot[8]);
-                ctrl->pending[par] = 1;
-            }
-            ctrl->step = step + 1;
+    phase_cell_assign<false>(a, cur);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_scan_partial(a);
+    if (!grid_barrier(c, [&] { block_scan_chunks(a); })) return false;
+    phase_scan_final(a);
+    if (!grid_barrier(c, none)) return false;
+    phase_scatter(a);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_sort_cells(a);
+    if (!grid_barrier(c, none)) return false;
+    phase_gather(a, cur);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_nbl_cells<FMA>(a);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_finish_cells(a, cur);
+    const bool ok = grid_barrier(c, [&] {
+        if (threadIdx.x == 0) rebuild_done(c);
+    });
+    trace_mark(c, TR_REBUILD_DONE);
+    return ok;
+}
+
+// Persistent cooperative kernel: `nsteps` steps starting from pos[cur0], then
+// (if do_eval) the force-only evaluation of the final state -- one timeblock
+// of simulation/Simulation.py:306-328 in one launch.
+template <int TP, bool NT1, int INTEG>
+__global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
+    __shared__ PairEntry s_tab[NT1 ? 1 : GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    load_table<NT1>(tab, s_tab);
+    DevCtrl *ctrl = a.ctrl;
+    int cur = cur0;
+    trace_mark(ctrl, TR_START);
+    for (int s = 0; s < nsteps + do_eval; s++) {
+        if (*(volatile int *)&ctrl->rebuild) {
+            const bool ok = a.fma ? rebuild_persistent<true>(a, cur) : rebuild_persistent<false>(a, cur);
+            if (!ok) return;
         }
-        ctrl->pending[ppar] = 0;
-        ctrl->ticket = 0;
+        const int step = *(volatile int *)&ctrl->step;
+        bool ok;
+        if (s < nsteps) {
+            phase_step<TP, NT1, INTEG, MODE_STEP, false, true>(a, s_tab, tab.nt, cur, step, s_red);
+            ok = grid_barrier(ctrl, [&] {
+                finalize_step<MODE_STEP>(a, step, gridDim.x, s_red);
+                if (threadIdx.x == 0 && ctrl->rebuild_next) {
+                    ctrl->rebuild = 1;
+                    ctrl->rebuild_next = 0;
+                }
+            });
+            cur ^= 1;
+            trace_mark(ctrl, TR_STEP);
+        } else {
+            phase_step<TP, NT1, INTEG, MODE_EVAL, false, true>(a, s_tab, tab.nt, cur, step, s_red);
+            ok = grid_barrier(ctrl, [&] { finalize_step<MODE_EVAL>(a, step, gridDim.x, s_red); });
+            trace_mark(ctrl, TR_EVAL);
+        }
+        if (!ok) return;
     }
 }
 
 __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
     ctrl->step = 0;
     ctrl->time_zero = time_zero;
+    ctrl->bar_count = 0;
+    ctrl->abort = 0;
+    ctrl->ticket = 0;
+    if (ctrl->rebuild_next) {
+        ctrl->rebuild = 1;
+        ctrl->rebuild_next = 0;
+    }
 }
 
 // upload helpers: gamdpy layout -> float4 / int4
@@ -849,26 +408,28 @@ static void free_graphs(gdb_sim *h) {
 
 static int choose_tp(const gdb_sim *h) {
     if (h->tp_req > 0) return h->tp_req;
-    // enough lanes for ~1.5 waves of 148 SMs x 2048 threads
-    const long long want = 148LL * 2048;
+    // about 131k lanes in flight (measured on B200: 1 lane per particle at
+    // N = 1M, 2 at 65k, 32 at 2k)
     int tp = 1;
-    while (tp < 8 && (long long)h->n * tp < want) tp *= 2;
+    while (tp < 32 && (long long)h->n * tp < 131072) tp *= 2;
     return tp;
 }
 
 static int ensure_nblist(gdb_sim *h) {
     const int tp = choose_tp(h);
     const int stride = (h->n + 31) / 32 * 32;
-    const size_t need = (size_t)(h->max_nbs + tp) * stride;
-    if (tp != h->tp || need > h->nbl_elems) {
+    const size_t need = ((size_t)h->max_nbs + NB_CHUNK) * stride;
+    if (need > h->nbl_elems) {
         if (h->nbl) cudaFree(h->nbl);
         h->nbl = nullptr;
         CK(cudaMalloc(&h->nbl, need * sizeof(int)));
         h->nbl_elems = need;
-        h->tp = tp;
-        h->stride = stride;
         free_graphs(h);
         if (h->uploaded) CK(cudaMemsetAsync(&h->ctrl->rebuild, 0xff, sizeof(int), h->st));  // nonzero
+    }
+    if (tp != h->tp) {
+        h->tp = tp;
+        free_graphs(h);
     }
     h->stride = stride;
     if (h->nb_kind == GDB_NBLIST_CELLS) {
@@ -890,6 +451,7 @@ static int ensure_nblist(gdb_sim *h) {
             CK(cudaMalloc(&h->bsum, ((size_t)ncell / SCAN_CHUNK + 2) * sizeof(int)));
             CK(cudaMemsetAsync(h->cell_count, 0, (size_t)ncell * sizeof(int), h->st));
             h->cell_cap = ncell;
+            free_graphs(h);
         }
         if (nc[0] != h->nc[0] || nc[1] != h->nc[1] || nc[2] != h->nc[2]) free_graphs(h);
         memcpy(h->nc, nc, sizeof(nc));
@@ -909,84 +471,52 @@ static int ensure_partials(gdb_sim *h, int nblocks) {
     return GDB_OK;
 }
 
-// Enqueue the (flag-gated) rebuild chain for the current buffer.
-static int enqueue_rebuild(gdb_sim *h) {
-    const int n = h->n;
-    const float cps = h->max_cut + h->skin;  // nblist.py:152 (max_cut+skin, float32)
-    const float cps2 = cps * cps;
-    const float4 *pos = h->pos[h->cur];
-    if (h->nb_kind == GDB_NBLIST_NSQ) {
-        if (h->fma)
-            k_nbl_nsq<true><<<grid_for((long long)n * 32), GDB_BLOCK, 0, h->st>>>(
-                pos, n, h->box[0], h->box[1], h->box[2], cps2, h->nbl, h->nbc, h->stride, h->tp, h->max_nbs, h->ctrl);
-        else
-            k_nbl_nsq<false><<<grid_for((long long)n * 32), GDB_BLOCK, 0, h->st>>>(
-                pos, n, h->box[0], h->box[1], h->box[2], cps2, h->nbl, h->nbc, h->stride, h->tp, h->max_nbs, h->ctrl);
-        CKL();
-        k_rebuild_finish<false><<<grid_for(n), GDB_BLOCK, 0, h->st>>>(
-            n, h->pos[h->cur], h->vel, h->img, h->orig, h->pscal, nullptr, nullptr, nullptr, nullptr, nullptr, h->rref,
-            nullptr, 0, h->ctrl);
-        CKL();
-        return GDB_OK;
-    }
-    const int ncell = h->ncell;
-    const int nchunks = (ncell + SCAN_CHUNK - 1) / SCAN_CHUNK;
-    k_cell_assign<<<grid_for(n), GDB_BLOCK, 0, h->st>>>(pos, n, h->box[0], h->box[1], h->box[2], h->nc[0], h->nc[1],
-                                                        h->nc[2], h->pcell, h->prank, h->cell_count, h->ctrl);
-    CKL();
-    k_scan_partial<<<nchunks, GDB_BLOCK, 0, h->st>>>(h->cell_count, ncell, h->bsum, h->ctrl);
-    CKL();
-    k_scan_top<<<1, GDB_BLOCK, 0, h->st>>>(h->bsum, nchunks, h->ctrl);
-    CKL();
-    k_scan_final<<<nchunks, GDB_BLOCK, 0, h->st>>>(h->cell_count, ncell, h->bsum, h->cell_start, n, h->ctrl);
-    CKL();
-    k_scatter<<<grid_for(n), GDB_BLOCK, 0, h->st>>>(h->pcell, h->prank, h->cell_start, h->perm, n, h->ctrl);
-    CKL();
-    k_sort_cells<<<grid_for(ncell), GDB_BLOCK, 0, h->st>>>(h->cell_start, ncell, h->perm, h->orig, h->ctrl);
-    CKL();
-    k_gather<<<grid_for(n), GDB_BLOCK, 0, h->st>>>(h->perm, n, pos, h->vel, h->img, h->orig, h->pscal, h->pcell,
-                                                   h->pos_tmp, h->vel_tmp, h->img_tmp, h->orig_tmp, h->pscal_tmp,
-                                                   h->scell, h->ctrl);
-    CKL();
-    if (h->fma)
-        k_nbl_cells<true><<<grid_for(n), GDB_BLOCK, 0, h->st>>>(
-            h->pos_tmp, h->scell, h->cell_start, n, h->box[0], h->box[1], h->box[2], h->nc[0], h->nc[1], h->nc[2], cps2,
-            h->nbl, h->nbc, h->stride, h->tp, h->max_nbs, h->ctrl);
-    else
-        k_nbl_cells<false><<<grid_for(n), GDB_BLOCK, 0, h->st>>>(
-            h->pos_tmp, h->scell, h->cell_start, n, h->box[0], h->box[1], h->box[2], h->nc[0], h->nc[1], h->nc[2], cps2,
-            h->nbl, h->nbc, h->stride, h->tp, h->max_nbs, h->ctrl);
-    CKL();
-    k_rebuild_finish<true><<<grid_for(n), GDB_BLOCK, 0, h->st>>>(
-        n, h->pos[h->cur], h->vel, h->img, h->orig, h->pscal, h->pos_tmp, h->vel_tmp, h->img_tmp, h->orig_tmp,
-        h->pscal_tmp, h->rref, h->cell_count, ncell, h->ctrl);
-    CKL();
-    return GDB_OK;
-}
-
-static StepArgs make_args(gdb_sim *h, int mode) {
-    StepArgs a;
-    a.pos = h->pos[h->cur];
-    a.pos_next = h->pos[h->cur ^ 1];
+static SimArgs make_args(gdb_sim *h) {
+    SimArgs a;
+    a.pos0 = h->pos[0];
+    a.pos1 = h->pos[1];
     a.vel = h->vel;
     a.img = h->img;
     a.rref = h->rref;
     a.frc = h->frc;
+    a.pos_tmp = h->pos_tmp;
+    a.vel_tmp = h->vel_tmp;
+    a.img_tmp = h->img_tmp;
+    a.orig = h->orig;
+    a.orig_tmp = h->orig_tmp;
     a.nbl = h->nbl;
     a.nbc = h->nbc;
     a.pscal = h->pscal;
+    a.pscal_tmp = h->pscal_tmp;
+    a.cell_count = h->cell_count;
+    a.cell_start = h->cell_start;
+    a.pcell = h->pcell;
+    a.prank = h->prank;
+    a.perm = h->perm;
+    a.scell = h->scell;
+    a.bsum = h->bsum;
     a.partials = h->partials;
     a.rows = h->rows;
+    a.conf = h->conf;
     a.ctrl = h->ctrl;
     a.n = h->n;
     a.stride = h->stride;
     a.max_nbs = h->max_nbs;
+    a.ncell = h->nb_kind == GDB_NBLIST_CELLS ? h->ncell : 0;
+    a.nchunks = (a.ncell + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    a.ncx = h->nc[0];
+    a.ncy = h->nc[1];
+    a.ncz = h->nc[2];
+    a.nb_kind = h->nb_kind;
+    a.fma = h->fma;
     a.Lx = h->box[0];
     a.Ly = h->box[1];
     a.Lz = h->box[2];
+    const float cps = h->max_cut + h->skin;  // nblist.py:152 (max_cut+skin, float32)
+    a.cps2 = cps * cps;
     a.skin2q = h->skin * h->skin * 0.25f;
     a.dt = h->dt;
-    a.omega2 = h->omega2;
+    a.omega2 = h->integ == GDB_INTEGRATOR_NVT ? h->omega2 : 0.f;
     a.dof = 3LL * h->n - 3;
     a.tfunc = h->tfunc;
     a.tp0 = h->tparams[0];
@@ -996,30 +526,62 @@ static StepArgs make_args(gdb_sim *h, int mode) {
     a.every = h->scalar_every;
     a.reset_every = h->momentum_every;
     a.nrows = h->rows ? h->rows_cap : 0;
-    a.conf = h->conf;
     a.conf_per_block = h->conf_per_block;
-    a.orig = h->orig;
-    (void)mode;
     return a;
 }
 
+// Enqueue the (flag-gated) rebuild chain for the current buffer.
+static int enqueue_rebuild(gdb_sim *h) {
+    const SimArgs a = make_args(h);
+    const int n = h->n, cur = h->cur;
+    if (h->nb_kind == GDB_NBLIST_NSQ) {
+        if (h->fma)
+            k_nbl_nsq<true><<<grid_for((long long)n * 32), GDB_BLOCK, 0, h->st>>>(a, cur);
+        else
+            k_nbl_nsq<false><<<grid_for((long long)n * 32), GDB_BLOCK, 0, h->st>>>(a, cur);
+        CKL();
+    } else {
+        const int g = grid_for(n);
+        k_cell_assign<<<g, GDB_BLOCK, 0, h->st>>>(a, cur);
+        k_scan_partial<<<a.nchunks, GDB_BLOCK, 0, h->st>>>(a);
+        k_scan_top<<<1, GDB_BLOCK, 0, h->st>>>(a);
+        k_scan_final<<<a.nchunks, GDB_BLOCK, 0, h->st>>>(a);
+        k_scatter<<<g, GDB_BLOCK, 0, h->st>>>(a);
+        k_sort_cells<<<grid_for(a.ncell), GDB_BLOCK, 0, h->st>>>(a);
+        k_gather<<<g, GDB_BLOCK, 0, h->st>>>(a, cur);
+        const int gw = grid_for((long long)a.ncell * 32);
+        if (h->fma)
+            k_nbl_cells<true><<<gw, GDB_BLOCK, 0, h->st>>>(a);
+        else
+            k_nbl_cells<false><<<gw, GDB_BLOCK, 0, h->st>>>(a);
+        k_finish_cells<<<g, GDB_BLOCK, 0, h->st>>>(a, cur);
+        CKL();
+    }
+    k_rebuild_done<<<1, 1, 0, h->st>>>(h->ctrl);
+    CKL();
+    return GDB_OK;
+}
+
 template <int TP, bool NT1>
-static void launch_step_tp(gdb_sim *h, const StepArgs &a, int mode, int grid) {
+static void launch_step_tp(gdb_sim *h, const SimArgs &a, int mode, int grid) {
+    const int cur = h->cur;
     if (mode == MODE_EVAL)
-        k_step<TP, NT1, 0, MODE_EVAL><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table);
+        k_step<TP, NT1, 0, MODE_EVAL><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table, cur);
     else if (h->integ == GDB_INTEGRATOR_NVT)
-        k_step<TP, NT1, GDB_INTEGRATOR_NVT, MODE_STEP><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table);
+        k_step<TP, NT1, GDB_INTEGRATOR_NVT, MODE_STEP><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table, cur);
     else
-        k_step<TP, NT1, GDB_INTEGRATOR_NVE, MODE_STEP><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table);
+        k_step<TP, NT1, GDB_INTEGRATOR_NVE, MODE_STEP><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table, cur);
 }
 
 template <bool NT1>
-static void launch_step_nt(gdb_sim *h, const StepArgs &a, int mode, int grid) {
+static void launch_step_nt(gdb_sim *h, const SimArgs &a, int mode, int grid) {
     switch (h->tp) {
         case 1: launch_step_tp<1, NT1>(h, a, mode, grid); break;
         case 2: launch_step_tp<2, NT1>(h, a, mode, grid); break;
         case 4: launch_step_tp<4, NT1>(h, a, mode, grid); break;
-        default: launch_step_tp<8, NT1>(h, a, mode, grid); break;
+        case 8: launch_step_tp<8, NT1>(h, a, mode, grid); break;
+        case 16: launch_step_tp<16, NT1>(h, a, mode, grid); break;
+        default: launch_step_tp<32, NT1>(h, a, mode, grid); break;
     }
 }
 
@@ -1027,13 +589,56 @@ static int enqueue_step(gdb_sim *h, int mode) {
     const int grid = grid_for((long long)h->n * h->tp);
     int rc = ensure_partials(h, grid);
     if (rc) return rc;
-    StepArgs a = make_args(h, mode);
+    const SimArgs a = make_args(h);
     if (h->ntypes == 1)
         launch_step_nt<true>(h, a, mode, grid);
     else
         launch_step_nt<false>(h, a, mode, grid);
     CKL();
     if (mode == MODE_STEP) h->cur ^= 1;
+    return GDB_OK;
+}
+
+// The k_run instantiation for the handle's lanes, type count and integrator.
+template <int TP, bool NT1>
+static const void *run_kernel_tp(int integ) {
+    return integ == GDB_INTEGRATOR_NVT ? (const void *)k_run<TP, NT1, GDB_INTEGRATOR_NVT>
+                                       : (const void *)k_run<TP, NT1, GDB_INTEGRATOR_NVE>;
+}
+template <bool NT1>
+static const void *run_kernel_nt(int tp, int integ) {
+    switch (tp) {
+        case 1: return run_kernel_tp<1, NT1>(integ);
+        case 2: return run_kernel_tp<2, NT1>(integ);
+        case 4: return run_kernel_tp<4, NT1>(integ);
+        case 8: return run_kernel_tp<8, NT1>(integ);
+        case 16: return run_kernel_tp<16, NT1>(integ);
+        default: return run_kernel_tp<32, NT1>(integ);
+    }
+}
+
+// Grid of the persistent kernel: every block resident (cooperative launch).
+static int run_grid(gdb_sim *h, const void *fn, int *grid) {
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GDB_BLOCK, 0));
+    if (occ < 1) return set_err(h, GDB_ERR_CUDA, "persistent kernel cannot be resident");
+    const int needed = grid_for((long long)h->n * h->tp);
+    *grid = std::min(needed, occ * h->num_sms);
+    return GDB_OK;
+}
+
+// One launch of k_run: `steps` steps from pos[cur], then the final evaluation.
+static int launch_run(gdb_sim *h, int steps, int do_eval) {
+    const void *fn = h->ntypes == 1 ? run_kernel_nt<true>(h->tp, h->integ) : run_kernel_nt<false>(h->tp, h->integ);
+    int grid = 0;
+    int rc = run_grid(h, fn, &grid);
+    if (rc) return rc;
+    if ((rc = ensure_partials(h, grid))) return rc;
+    SimArgs a = make_args(h);
+    int cur0 = h->cur, ns = steps, ev = do_eval;
+    void *args[] = {(void *)&a, (void *)&h->table, (void *)&cur0, (void *)&ns, (void *)&ev};
+    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(GDB_BLOCK), args, 0, h->st));
+    h->cur ^= (steps & 1);
     return GDB_OK;
 }
 
@@ -1062,6 +667,8 @@ static int status_to_rc(gdb_sim *h) {
     }
     if (h->h_ctrl->status & GDB_STATUS_NAN)
         return set_err(h, GDB_ERR_NUMERIC, "non-finite or runaway particle position");
+    if (h->h_ctrl->status & GDB_STATUS_BARRIER_TIMEOUT)
+        return set_err(h, GDB_ERR_TIMEOUT, "grid barrier of the persistent step kernel timed out");
     return GDB_OK;
 }
 
@@ -1093,6 +700,12 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (g && g[0] == '0') h->use_graphs = false;
     const char *fm = getenv("GDB_NBLIST_FMA");
     if (fm && fm[0] == '0') h->fma = 0;
+    const char *ps = getenv("GDB_PERSISTENT");
+    if (ps && ps[0] == '0') h->persistent = false;
+    cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
+    int coop = 0;
+    cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
+    if (!coop) h->persistent = false;
     auto fail = [&](cudaError_t e) {
         snprintf(g_lib_error, sizeof(g_lib_error), "gdb_sim_create: %s", cudaGetErrorString(e));
         gdb_sim_destroy(h);
@@ -1144,7 +757,7 @@ int gdb_sim_destroy(gdb_sim *h) {
     void *bufs[] = {h->pos[0], h->pos[1], h->vel,        h->frc,       h->rref,  h->pos_tmp, h->vel_tmp,
                     h->img,    h->img_tmp, h->orig,      h->orig_tmp,  h->nbl,   h->nbc,     h->pscal,
                     h->pscal_tmp, h->cell_count, h->cell_start, h->pcell, h->prank, h->perm, h->scell,
-                    h->bsum,   h->ctrl,   h->partials,   h->rows,  h->conf};
+                    h->bsum,   h->ctrl,   h->partials,   h->rows,  h->conf, h->trace};
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
@@ -1290,8 +903,8 @@ int gdb_set_nblist(gdb_sim *h, int kind, float skin, int max_nbs) {
 
 int gdb_set_plan(gdb_sim *h, int tp, int pb) {
     if (!h) return set_err(h, GDB_ERR_ARG, "NULL handle");
-    if (tp != 0 && tp != 1 && tp != 2 && tp != 4 && tp != 8)
-        return set_err(h, GDB_ERR_ARG, "tp must be 0 (auto), 1, 2, 4 or 8");
+    if (tp != 0 && tp != 1 && tp != 2 && tp != 4 && tp != 8 && tp != 16 && tp != 32)
+        return set_err(h, GDB_ERR_ARG, "tp must be 0 (auto), 1, 2, 4, 8, 16 or 32");
     h->tp_req = tp;
     h->pb_req = pb;
     return GDB_OK;
@@ -1419,35 +1032,66 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
         free_graphs(h);
     }
     if (rows > 0) CK(cudaMemsetAsync(h->rows, 0, (size_t)rows * GDB_NUM_SCALARS * sizeof(double), h->st));
-    {
-        const int grid = grid_for((long long)h->n * h->tp);
-        if ((rc = ensure_partials(h, grid))) return rc;
-    }
+    if ((rc = ensure_partials(h, grid_for((long long)h->n * h->tp)))) return rc;
     CK(cudaMemsetAsync(&h->ctrl->maxcount, 0, sizeof(int), h->st));
     CK(cudaEventRecord(h->ev0, h->st));
     k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
     CKL();
-    const int G = 16;
-    int s = 0;
-    if (h->use_graphs && steps >= G) {
-        h->graph_steps = G;
-        while (s + G <= steps) {
-            if (!h->gexec[h->cur] && (rc = build_graph(h, h->cur, G))) return rc;
-            CK(cudaGraphLaunch(h->gexec[h->cur], h->st));
-            // G is even: the current buffer is unchanged after a chunk
-            s += G;
+    if (h->persistent) {
+        if ((rc = launch_run(h, steps, 1))) return rc;
+    } else {
+        const int G = 16;
+        int s = 0;
+        if (h->use_graphs && steps >= G) {
+            while (s + G <= steps) {
+                if (!h->gexec[h->cur] && (rc = build_graph(h, h->cur, G))) return rc;
+                CK(cudaGraphLaunch(h->gexec[h->cur], h->st));
+                s += G;  // G is even: the current buffer is unchanged after a chunk
+            }
         }
-    }
-    for (; s < steps; s++) {
+        for (; s < steps; s++) {
+            if ((rc = enqueue_rebuild(h))) return rc;
+            if ((rc = enqueue_step(h, MODE_STEP))) return rc;
+        }
         if ((rc = enqueue_rebuild(h))) return rc;
-        if ((rc = enqueue_step(h, MODE_STEP))) return rc;
+        if ((rc = enqueue_step(h, MODE_EVAL))) return rc;
     }
-    if ((rc = enqueue_rebuild(h))) return rc;
-    if ((rc = enqueue_step(h, MODE_EVAL))) return rc;
     CK(cudaEventRecord(h->ev1, h->st));
     if ((rc = read_ctrl(h))) return rc;
     if (ms) CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
     return status_to_rc(h);
+}
+
+int gdb_set_trace(gdb_sim *h, int capacity) {
+    if (!h || capacity < 0) return set_err(h, GDB_ERR_ARG, "bad trace capacity");
+    CK(cudaSetDevice(h->dev));
+    CK(cudaStreamSynchronize(h->st));
+    if (h->trace) cudaFree(h->trace);
+    h->trace = nullptr;
+    h->trace_cap = 0;
+    if (capacity > 0) {
+        CK(cudaMalloc(&h->trace, (size_t)capacity * sizeof(unsigned long long)));
+        h->trace_cap = capacity;
+    }
+    unsigned long long *p = h->trace;
+    int cap = h->trace_cap, zero = 0;
+    CK(cudaMemcpy(&h->ctrl->trace, &p, sizeof(p), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(&h->ctrl->trace_cap, &cap, sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(&h->ctrl->trace_len, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    return GDB_OK;
+}
+
+int gdb_get_trace(gdb_sim *h, unsigned long long *out, int capacity, int *count) {
+    if (!h || !out || !count) return set_err(h, GDB_ERR_ARG, "NULL argument");
+    CK(cudaSetDevice(h->dev));
+    int rc = read_ctrl(h);
+    if (rc) return rc;
+    const int len = std::min(std::min(h->h_ctrl->trace_len, h->trace_cap), capacity);
+    if (len > 0) CK(cudaMemcpy(out, h->trace, (size_t)len * sizeof(unsigned long long), cudaMemcpyDeviceToHost));
+    *count = len;
+    int zero = 0;
+    CK(cudaMemcpy(&h->ctrl->trace_len, &zero, sizeof(int), cudaMemcpyHostToDevice));
+    return GDB_OK;
 }
 
 int gdb_time_step_kernel(gdb_sim *h, int reps, float *ms_per_launch) {
@@ -1463,6 +1107,8 @@ int gdb_time_step_kernel(gdb_sim *h, int reps, float *ms_per_launch) {
     const int saved_every = h->scalar_every, saved_reset = h->momentum_every;
     h->scalar_every = 0;
     h->momentum_every = 0;
+    // one untimed launch: the module's lazy loading of this kernel happens here
+    if ((rc = enqueue_step(h, MODE_STEP))) return rc;
     CK(cudaEventRecord(h->ev0, h->st));
     for (int r = 0; r < reps && rc == GDB_OK; r++) rc = enqueue_step(h, MODE_STEP);
     h->scalar_every = saved_every;
@@ -1514,13 +1160,13 @@ int gdb_get_nblist(gdb_sim *h, int32_t *out, int max_nbs) {
     CK(cudaMemcpyAsync(nbc.data(), h->nbc, N * sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaMemcpyAsync(orig.data(), h->orig, N * sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
-    const int tp = h->tp, stride = h->stride;
+    const size_t stride = h->stride;
     for (size_t s = 0; s < N; s++) {
         const int i = orig[s];
         int32_t *row = out + (size_t)i * (max_nbs + 1);
         const int cnt = nbc[s];
         const int lim = std::min(std::min(cnt, h->max_nbs), max_nbs);
-        for (int k = 0; k < lim; k++) row[k] = orig[nbl[(size_t)(k / tp) * stride * tp + s * tp + (k % tp)]];
+        for (int k = 0; k < lim; k++) row[k] = orig[nbl[(size_t)(k >> 2) * stride * 4 + s * 4 + (k & 3)]];
         row[max_nbs] = cnt;
     }
     return GDB_OK;

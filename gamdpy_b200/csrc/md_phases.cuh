@@ -1,0 +1,761 @@
+// md_phases.cuh -- device phases of one MD time step, and the kernels that
+// run them.
+//
+// Every phase is a grid-stride device function over its items (particles,
+// cells, chunks), so the same code runs
+//   * as one standalone kernel per phase, launched in a CUDA graph (large N), and
+//   * inside k_run, a persistent cooperative kernel that advances a whole
+//     chunk of steps, rebuilds included, with a bounded grid barrier between
+//     phases (gamdpy's gridsync mode, simulation/Simulation.py:306-328).
+//
+// Data written inside k_run by one block and read by another (positions,
+// neighbour lists, cell tables) is read with ordinary coherent loads; the
+// non-coherent read-only path (__ldg) is used only by the standalone kernels,
+// where kernel boundaries order the accesses.
+#pragma once
+
+#include "gdb_internal.cuh"
+
+namespace gdb {
+
+constexpr int NQ = 9;  // block reductions: K, U, W, lapU, Fsq, px, py, pz, m
+constexpr int SCAN_CHUNK = 2048;
+constexpr int MODE_STEP = 0;
+constexpr int MODE_EVAL = 1;
+constexpr int NB_CHUNK = 4;  // neighbour indices stored and loaded 4 at a time (int4)
+
+// Neighbour list layout: entry k of particle i at
+//   (k / 4) * (stride * 4) + i * 4 + (k % 4)
+// so one int4 load gives four consecutive neighbours of a particle and a warp
+// of consecutive particles reads 512 contiguous bytes.
+__device__ __forceinline__ size_t nbl_index(int i, int k, int stride) {
+    return (size_t)(k >> 2) * ((size_t)stride * NB_CHUNK) + (size_t)i * NB_CHUNK + (k & 3);
+}
+
+struct SimArgs {
+    float4 *pos0, *pos1;  // ping-pong position buffers
+    float4 *vel;
+    int4 *img;
+    float4 *rref;
+    float4 *frc;
+    float4 *pos_tmp, *vel_tmp;
+    int4 *img_tmp;
+    int *orig, *orig_tmp;
+    int *nbl, *nbc;
+    float *pscal, *pscal_tmp;  // 5 planes of n: U, W, lapU, K, Fsq
+    int *cell_count, *cell_start, *pcell, *prank, *perm, *scell, *bsum;
+    double *partials, *rows;
+    float *conf;
+    DevCtrl *ctrl;
+    int n, stride, max_nbs;
+    int ncell, nchunks, ncx, ncy, ncz;
+    int nb_kind, fma;
+    float Lx, Ly, Lz;
+    float cps2;    // (max_cut + skin)^2, nblist.py:152
+    float skin2q;  // skin*skin*0.25, orthorhombic.py:131
+    float dt, omega2;
+    long long dof;  // N*D - D (NVT.py:35)
+    int tfunc;
+    float tp0, tp1, tp2, tp3;
+    int every, reset_every, nrows, conf_per_block;
+};
+
+__device__ __forceinline__ float4 *cur_pos(const SimArgs &a, int cur) { return cur ? a.pos1 : a.pos0; }
+
+template <bool NC, typename T>
+__device__ __forceinline__ T load(const T *p) {
+    if (NC) return __ldg(p);
+    return *p;
+}
+
+// ---------------------------------------------------------------------------
+// bounded grid barrier (k_run only; the launch is cooperative, so every block
+// is resident).  The last block to arrive runs `last` with the whole block
+// before releasing the others.  A wait that exceeds ~1 s of SM clock sets
+// GDB_STATUS_BARRIER_TIMEOUT and ctrl->abort; callers return when it fails.
+// ---------------------------------------------------------------------------
+constexpr long long BARRIER_TIMEOUT_CYCLES = 2000000000LL;
+
+template <typename F>
+__device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
+    __shared__ int s_last, s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned gen = *(volatile unsigned *)&c->bar_gen;
+        const unsigned t = atomicAdd(&c->bar_count, 1u);
+        s_last = (t == gridDim.x - 1);
+        s_ok = 1;
+        if (!s_last) {
+            const long long t0 = clock64();
+            while (*(volatile unsigned *)&c->bar_gen == gen) {
+                if (*(volatile int *)&c->abort) {
+                    s_ok = 0;
+                    break;
+                }
+                if (clock64() - t0 > BARRIER_TIMEOUT_CYCLES) {
+                    atomicOr(&c->status, GDB_STATUS_BARRIER_TIMEOUT);
+                    c->abort = 1;
+                    s_ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        last();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            c->bar_count = 0;
+            __threadfence();
+            atomicAdd(&c->bar_gen, 1u);
+        }
+        __syncthreads();
+    }
+    return s_ok != 0;
+}
+
+// ---------------------------------------------------------------------------
+// neighbour-list phases
+// ---------------------------------------------------------------------------
+
+// N^2 build (interactions/nblist.py:88-143): one warp per particle, lanes
+// stride over j, ballot + popc append hits in ascending j (deterministic).
+template <bool FMA, bool NC>
+__device__ void phase_nbl_nsq(const SimArgs &a, int cur) {
+    const float4 *pos = cur_pos(a, cur);
+    const int lane = threadIdx.x & 31;
+    const int warps = (gridDim.x * blockDim.x) >> 5;
+    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += warps) {
+        const float4 pi = load<NC>(pos + i);
+        int count = 0;
+        for (int j0 = 0; j0 < a.n; j0 += 32) {
+            const int j = j0 + lane;
+            bool hit = false;
+            if (j < a.n && j != i) hit = dist_sq_exact<FMA>(load<NC>(pos + j), pi, a.Lx, a.Ly, a.Lz) < a.cps2;
+            const unsigned m = __ballot_sync(0xffffffffu, hit);
+            if (hit) {
+                const int k = count + __popc(m & ((1u << lane) - 1u));
+                if (k < a.max_nbs) a.nbl[nbl_index(i, k, a.stride)] = j;
+            }
+            count += __popc(m);
+        }
+        if (lane == 0) {
+            a.nbc[i] = count;
+            a.rref[i] = pi;
+            atomicMax(&a.ctrl->maxcount, count);
+        }
+    }
+}
+
+// Cell coordinate as nblist_linked_lists.py:127 (float64, Python modulo);
+// non-finite coordinates map to cell 0 and raise the NAN bit.
+__device__ __forceinline__ int cell_coord(float x, float L, int nc, DevCtrl *ctrl) {
+    const double v = ((double)x + 0.5 * (double)L) * (double)nc / (double)L;
+    if (!(v > -1e9 && v < 1e9)) {
+        atomicOr(&ctrl->status, GDB_STATUS_NAN);
+        return 0;
+    }
+    const long long c = (long long)floor(v);
+    long long m = c % nc;
+    if (m < 0) m += nc;
+    return (int)m;
+}
+
+template <bool NC>
+__device__ void phase_cell_assign(const SimArgs &a, int cur) {
+    const float4 *pos = cur_pos(a, cur);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        const float4 p = load<NC>(pos + i);
+        const int cx = cell_coord(p.x, a.Lx, a.ncx, a.ctrl);
+        const int cy = cell_coord(p.y, a.Ly, a.ncy, a.ctrl);
+        const int cz = cell_coord(p.z, a.Lz, a.ncz, a.ctrl);
+        const int c = (cz * a.ncy + cy) * a.ncx + cx;  // x fastest
+        a.pcell[i] = c;
+        a.prank[i] = atomicAdd(&a.cell_count[c], 1);
+    }
+}
+
+// Block-wide exclusive scan of SCAN_CHUNK ints (8 per thread, blockDim 256).
+__device__ __forceinline__ void chunk_scan(const int *in, int len, int base, int *out_excl, int add, int *total,
+                                           int *sm /* 32 */) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    int v[8];
+    int s = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+        const int idx = base + t * 8 + q;
+        v[q] = idx < len ? in[idx] : 0;
+        s += v[q];
+    }
+    int incl = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += y;
+    }
+    if (lane == 31) sm[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        const int w = lane < (int)(blockDim.x >> 5) ? sm[lane] : 0;
+        int wi = w;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += y;
+        }
+        sm[lane] = wi - w;
+        if (lane == 31 && total) *total = wi;
+    }
+    __syncthreads();
+    if (out_excl) {
+        int run = add + sm[warp] + incl - s;
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int idx = base + t * 8 + q;
+            if (idx < len) out_excl[idx] = run;
+            run += v[q];
+        }
+    }
+    __syncthreads();
+}
+
+__device__ void phase_scan_partial(const SimArgs &a) {
+    __shared__ int sm[32];
+    __shared__ int tot;
+    for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x) {
+        chunk_scan(a.cell_count, a.ncell, c * SCAN_CHUNK, nullptr, 0, &tot, sm);
+        if (threadIdx.x == 0) a.bsum[c] = tot;
+        __syncthreads();
+    }
+}
+
+// exclusive scan of the chunk sums, by one block
+__device__ void block_scan_chunks(const SimArgs &a) {
+    __shared__ int sm[32];
+    __shared__ int tot;
+    int carry = 0;
+    for (int base = 0; base < a.nchunks; base += SCAN_CHUNK) {
+        chunk_scan(a.bsum, a.nchunks, base, a.bsum, carry, &tot, sm);
+        carry += tot;
+        __syncthreads();
+    }
+}
+
+__device__ void phase_scan_final(const SimArgs &a) {
+    __shared__ int sm[32];
+    for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x)
+        chunk_scan(a.cell_count, a.ncell, c * SCAN_CHUNK, a.cell_start, a.bsum[c], nullptr, sm);
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.cell_start[a.ncell] = a.n;
+}
+
+__device__ void phase_scatter(const SimArgs &a) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+        a.perm[a.cell_start[a.pcell[i]] + a.prank[i]] = i;
+}
+
+// Order every cell's particles by user index: the atomics of the assignment
+// rank them arbitrarily; this makes the layout and every sum deterministic.
+__device__ void phase_sort_cells(const SimArgs &a) {
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += gridDim.x * blockDim.x) {
+        const int lo = a.cell_start[c], hi = a.cell_start[c + 1];
+        for (int x = lo + 1; x < hi; x++) {
+            const int v = a.perm[x];
+            const int key = a.orig[v];
+            int y = x - 1;
+            while (y >= lo && a.orig[a.perm[y]] > key) {
+                a.perm[y + 1] = a.perm[y];
+                y--;
+            }
+            a.perm[y + 1] = v;
+        }
+    }
+}
+
+__device__ void phase_gather(const SimArgs &a, int cur) {
+    const float4 *pos = cur_pos(a, cur);
+    const size_t n = a.n;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
+        const int i = a.perm[s];
+        a.pos_tmp[s] = pos[i];
+        a.vel_tmp[s] = a.vel[i];
+        a.img_tmp[s] = a.img[i];
+        a.orig_tmp[s] = a.orig[i];
+        a.scell[s] = a.pcell[i];
+        // K and Fsq travel with the particle; U, W, lapU are rewritten by the
+        // next force evaluation
+        a.pscal_tmp[3 * n + s] = a.pscal[3 * n + i];
+        a.pscal_tmp[4 * n + s] = a.pscal[4 * n + i];
+    }
+}
+
+// Cell-list build (nblist_linked_lists.py:133-183 semantics: all particles of
+// the 5x5x5 stencil with dist_sq < (max_cut+skin)^2, j != i).  One warp per
+// cell: the cell's particles share the stencil.  Slots are sorted by cell
+// with x fastest, so the five x-cells of one (dy, dz) row are one contiguous
+// slot range (two at the x wrap); the warp lists the <= 50 ranges with their
+// prefix sums in shared memory and walks the packed candidate sequence 32 at a
+// time, testing each candidate against up to NBW particles of the cell held
+// in registers.  Ballot + popc append in candidate order: deterministic.
+// Grids with fewer than five cells in a dimension visit each cell once.
+constexpr int NBW = 8;        // particles of a cell handled per pass
+constexpr int NB_SEG_MAX = 64; // 25 rows x at most 2 ranges
+
+__device__ __forceinline__ int wrapi(int x, int n) { return ((x % n) + n) % n; }
+
+template <bool FMA>
+__device__ void phase_nbl_cells(const SimArgs &a) {
+    __shared__ int s_lo[GDB_BLOCK / 32][NB_SEG_MAX];
+    __shared__ int s_pre[GDB_BLOCK / 32][NB_SEG_MAX + 1];
+    const float4 *pos = a.pos_tmp;
+    const int ncx = a.ncx, ncy = a.ncy, ncz = a.ncz;
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    int *lo_s = s_lo[wib], *pre_s = s_pre[wib];
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int ry = ncy < 5 ? ncy : 5, rz = ncz < 5 ? ncz : 5;
+    const int nrows = ry * rz;
+    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < a.ncell; c += nwarps) {
+        const int cs = a.cell_start[c], ce = a.cell_start[c + 1];
+        if (cs == ce) continue;
+        const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+        // lane r < nrows builds the x-range(s) of stencil row r
+        int len0 = 0, len1 = 0, lo0 = 0, lo1 = 0;
+        if (lane < nrows) {
+            const int za = lane / ry, yb = lane % ry;
+            const int z = ncz < 5 ? za : wrapi(cz - 2 + za, ncz);
+            const int y = ncy < 5 ? yb : wrapi(cy - 2 + yb, ncy);
+            const int rowbase = (z * ncy + y) * ncx;
+            int l0, h0, l1 = 0, h1 = 0;
+            if (ncx <= 5) {
+                l0 = rowbase;
+                h0 = rowbase + ncx;
+            } else {
+                const int x0 = cx - 2, x1 = cx + 2;
+                if (x0 >= 0 && x1 < ncx) {
+                    l0 = rowbase + x0;
+                    h0 = rowbase + x1 + 1;
+                } else if (x0 < 0) {
+                    l0 = rowbase + x0 + ncx;
+                    h0 = rowbase + ncx;
+                    l1 = rowbase;
+                    h1 = rowbase + x1 + 1;
+                } else {
+                    l0 = rowbase + x0;
+                    h0 = rowbase + ncx;
+                    l1 = rowbase;
+                    h1 = rowbase + x1 - ncx + 1;
+                }
+            }
+            lo0 = a.cell_start[l0];
+            len0 = a.cell_start[h0] - lo0;
+            if (h1 > l1) {
+                lo1 = a.cell_start[l1];
+                len1 = a.cell_start[h1] - lo1;
+            }
+        }
+        // segments in row order: row r gives entries 2r, 2r+1 (second may be empty)
+        const int tot = len0 + len1;
+        int incl = tot;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        const int excl = incl - tot;
+        if (lane < nrows) {
+            lo_s[2 * lane] = lo0;
+            pre_s[2 * lane] = excl;
+            lo_s[2 * lane + 1] = lo1;
+            pre_s[2 * lane + 1] = excl + len0;
+        }
+        const int T = __shfl_sync(0xffffffffu, incl, 31);
+        if (lane == 0) pre_s[2 * nrows] = T;
+        __syncwarp();
+        const int nseg = 2 * nrows;
+        for (int g0 = cs; g0 < ce; g0 += NBW) {
+            const int gn = min(NBW, ce - g0);
+            float4 pi[NBW];
+            int cnt[NBW];
+#pragma unroll
+            for (int p = 0; p < NBW; p++) {
+                pi[p] = p < gn ? pos[g0 + p] : make_float4(0.f, 0.f, 0.f, 0.f);
+                cnt[p] = 0;
+            }
+            for (int v0 = 0; v0 < T; v0 += 32) {
+                const int v = v0 + lane;
+                const bool valid = v < T;
+                int j = 0;
+                float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (valid) {
+                    // last segment whose prefix <= v
+                    int lo = 0, hi = nseg - 1;
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (pre_s[mid] <= v)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    j = lo_s[lo] + (v - pre_s[lo]);
+                    pj = pos[j];
+                }
+#pragma unroll
+                for (int p = 0; p < NBW; p++) {
+                    if (p >= gn) break;
+                    const bool hit = valid && j != g0 + p && dist_sq_exact<FMA>(pj, pi[p], a.Lx, a.Ly, a.Lz) < a.cps2;
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                        const int k = cnt[p] + __popc(m & ((1u << lane) - 1u));
+                        if (k < a.max_nbs) a.nbl[nbl_index(g0 + p, k, a.stride)] = j;
+                    }
+                    cnt[p] += __popc(m);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < NBW; p++) {
+                if (p < gn && lane == p) {
+                    a.nbc[g0 + p] = cnt[p];
+                    atomicMax(&a.ctrl->maxcount, cnt[p]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Move the reordered state into place, record r_ref, clear the cell counters.
+__device__ void phase_finish_cells(const SimArgs &a, int cur) {
+    float4 *pos = cur_pos(a, cur);
+    const size_t n = a.n;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
+        const float4 p = a.pos_tmp[s];
+        pos[s] = p;
+        a.rref[s] = p;
+        a.vel[s] = a.vel_tmp[s];
+        a.img[s] = a.img_tmp[s];
+        a.orig[s] = a.orig_tmp[s];
+        a.pscal[3 * n + s] = a.pscal_tmp[3 * n + s];
+        a.pscal[4 * n + s] = a.pscal_tmp[4 * n + s];
+    }
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += gridDim.x * blockDim.x) a.cell_count[c] = 0;
+}
+
+__device__ __forceinline__ void rebuild_done(DevCtrl *c) {
+    c->rebuild = 0;
+    c->nrebuild += 1;
+}
+
+// ---------------------------------------------------------------------------
+// force + integrate phase
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ double target_temperature(const SimArgs &a, double t) {
+    if (a.tfunc == GDB_TFUNC_RAMP) {  // misc/make_function.py:27-32
+        if (t < a.tp1) return a.tp0;
+        if (t < a.tp3) return a.tp0 + (t - a.tp1) * ((double)(a.tp2 - a.tp0) / (double)(a.tp3 - a.tp1));
+        return a.tp2;
+    }
+    return a.tp0;
+}
+
+// ConfigurationSaver slot of a step (runtime_actions/configuration_saver.py:
+// 115-141): step 0 -> 0, step 2^b -> b + 1, others -> -1.
+__device__ __forceinline__ int conf_save_index(int step) {
+    if (step == 0) return 0;
+    if (step & (step - 1)) return -1;
+    return 32 - __clz(step);
+}
+
+// Minimum image for list pairs (|d| < L): d - L*rint(d/L) equals the
+// reference's 2d-vs-L selection for every pair closer than L/2.
+template <bool REC, int CUT>
+__device__ __forceinline__ void pair_force(const PairEntry &e, float4 pi, float4 pj, bool valid, float Lx, float Ly,
+                                           float Lz, float ilx, float ily, float ilz, float &fx, float &fy, float &fz,
+                                           float &u, float &w, float &l) {
+    float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+    dx -= Lx * rintf(dx * ilx);
+    dy -= Ly * rintf(dy * ily);
+    dz -= Lz * rintf(dz * ilz);
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    if (valid && d2 < e.cut2) {
+        const float inv2 = __fdividef(1.0f, d2);
+        const float x2 = e.c * inv2;
+        const float x6 = x2 * x2 * x2;
+        const float x12 = x6 * x6;
+        const float s = (e.cs12 * x12 + e.cs6 * x6) * inv2 - e.sc;
+        fx -= dx * s;
+        fy -= dy * s;
+        fz -= dz * s;
+        if (REC) {
+            const float r = sqrtf(d2);
+            const float uu = e.cu12 * x12 + e.cu6 * x6 - e.uc + e.sccut * (r - e.cut);
+            u += 0.5f * uu;
+            w += d2 * s * (1.0f / 6.0f);
+            l += -2.0f * s + (e.cm12 * x12 + e.cm6 * x6) * inv2;
+        }
+    }
+}
+
+// Neighbours of particle i handled by lane `sub` of TP: chunks of four
+// indices (one int4 load), four independent position gathers per chunk.
+// pair_potential.py:223-231 with the full-list calculator :164-178.
+template <int TP, bool NT1, bool REC, bool NC>
+__device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *pos, const PairEntry *tab, int nt,
+                                               int i, int sub, float4 pi, float &fx, float &fy, float &fz, float &u,
+                                               float &w, float &l) {
+    const int ti = NT1 ? 0 : ptype_of(pi);
+    const int cnt = min(a.nbc[i], a.max_nbs);
+    const int nch = (cnt + 3) >> 2;
+    const PairEntry *trow = tab + ti * nt;
+    const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
+    const float ilx = 1.0f / Lx, ily = 1.0f / Ly, ilz = 1.0f / Lz;
+    const int4 *base = reinterpret_cast<const int4 *>(a.nbl) + i;
+    const size_t cstride = (size_t)a.stride;  // int4 units between chunks
+    for (int ch = sub; ch < nch; ch += TP) {
+        const int4 jj = load<NC>(base + ch * cstride);
+        const int k0 = ch * 4;
+        const bool v1 = k0 + 1 < cnt, v2 = k0 + 2 < cnt, v3 = k0 + 3 < cnt;
+        const int j0 = jj.x, j1 = v1 ? jj.y : i, j2 = v2 ? jj.z : i, j3 = v3 ? jj.w : i;
+        const float4 p0 = load<NC>(pos + j0);
+        const float4 p1 = load<NC>(pos + j1);
+        const float4 p2 = load<NC>(pos + j2);
+        const float4 p3 = load<NC>(pos + j3);
+        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p0)], pi, p0, true, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
+                           w, l);
+        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p1)], pi, p1, v1, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
+                           w, l);
+        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p2)], pi, p2, v2, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
+                           w, l);
+        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p3)], pi, p3, v3, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
+                           w, l);
+    }
+}
+
+// Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
+// only (MODE_EVAL).  Each block accumulates float64 partial sums over all the
+// particles it handles and writes them to partials[blockIdx.x].  Sets the
+// rebuild flag when a particle has moved more than skin/2 since the build.
+template <int TP, bool NT1, int INTEG, int MODE, bool NC, bool PERSIST>
+__device__ void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red) {
+    DevCtrl *ctrl = a.ctrl;
+    const float4 *pos = cur_pos(a, cur);
+    float4 *pos_next = cur_pos(a, cur ^ 1);
+    const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
+    const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
+    const int ppar = (step & 1) ^ 1;
+    const bool shift_pending = ctrl->pending[ppar] != 0;
+    float shx = 0.f, shy = 0.f, shz = 0.f;
+    if (shift_pending) {
+        shx = ctrl->shift[ppar][0];
+        shy = ctrl->shift[ppar][1];
+        shz = ctrl->shift[ppar][2];
+    }
+    const float xi = ctrl->xi;
+    const size_t n = a.n;
+    const int per_block = blockDim.x / TP;
+    const int rounds_total = (a.n + per_block - 1) / per_block;
+    double red[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) red[q] = 0.0;
+    bool moved = false;
+    for (int round = blockIdx.x; round < rounds_total; round += gridDim.x) {
+        const int i = round * per_block + threadIdx.x / TP;
+        const int sub = threadIdx.x % TP;
+        const bool active = i < a.n;
+        float fx = 0.f, fy = 0.f, fz = 0.f, u = 0.f, w = 0.f, l = 0.f;
+        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (active) {
+            pi = pos[i];
+            if (rec)
+                neighbour_loop<TP, NT1, true, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
+            else
+                neighbour_loop<TP, NT1, false, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
+        }
+        if (TP > 1) {
+#pragma unroll
+            for (int o = TP / 2; o > 0; o >>= 1) {
+                fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                if (rec) {
+                    u += __shfl_xor_sync(0xffffffffu, u, o);
+                    w += __shfl_xor_sync(0xffffffffu, w, o);
+                    l += __shfl_xor_sync(0xffffffffu, l, o);
+                }
+            }
+        }
+        if (!(active && sub == 0)) continue;
+        // ConfigurationSaver: frame taken before this step's integration
+        if (a.conf) {
+            const int si = conf_save_index(step);
+            if (si >= 0 && si < a.conf_per_block) {
+                const int4 im = a.img[i];
+                const size_t uidx = (size_t)a.orig[i];
+                float *fr = a.conf + (size_t)si * 2 * n * 3;
+                fr[3 * uidx] = pi.x;
+                fr[3 * uidx + 1] = pi.y;
+                fr[3 * uidx + 2] = pi.z;
+                fr += n * 3;
+                fr[3 * uidx] = (float)im.x;
+                fr[3 * uidx + 1] = (float)im.y;
+                fr[3 * uidx + 2] = (float)im.z;
+            }
+        }
+        float4 v = a.vel[i];
+        if (shift_pending) {
+            v.x -= shx;
+            v.y -= shy;
+            v.z -= shz;
+        }
+        const float fsq = fx * fx + fy * fy + fz * fz;
+        if (rec) {
+            a.pscal[i] = u;
+            a.pscal[n + i] = w;
+            a.pscal[2 * n + i] = l;
+        }
+        red[1] += u;
+        red[2] += w;
+        red[3] += l;
+        red[4] += fsq;
+        if (MODE == MODE_EVAL) {
+            a.frc[i] = make_float4(fx, fy, fz, 0.f);
+            if (shift_pending) a.vel[i] = v;
+            continue;
+        }
+        const float m = v.w;
+        float kin = 0.f;
+        float r[3] = {pi.x, pi.y, pi.z};
+        float vv[3] = {v.x, v.y, v.z};
+        const float ff[3] = {fx, fy, fz};
+        if (INTEG == GDB_INTEGRATOR_NVE) {  // integrators/NVE.py:78-97
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                float v_mean = vv[k];
+                vv[k] += ff[k] / m * a.dt;
+                v_mean += vv[k];
+                v_mean *= 0.5f;
+                kin += 0.5f * m * v_mean * v_mean;
+                r[k] += vv[k] * a.dt;
+            }
+        } else {  // integrators/NVT.py:196-215
+            const float factor = 0.5f * xi * a.dt;
+            const float plus = 1.0f / (1.0f + factor);
+            const float minus = 1.0f - factor;
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                vv[k] = plus * (minus * vv[k] + ff[k] / m * a.dt);
+                kin += 0.5f * m * vv[k] * vv[k];
+                r[k] += vv[k] * a.dt;
+            }
+        }
+        // periodic boundaries with image counters (orthorhombic.py:75-86)
+        const float L[3] = {a.Lx, a.Ly, a.Lz};
+        int dimg[3] = {0, 0, 0};
+        bool wrapped = false;
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            if (r[k] * 2.0f > L[k]) {
+                r[k] -= L[k];
+                dimg[k] += 1;
+                wrapped = true;
+            }
+            if (r[k] * 2.0f < -L[k]) {
+                r[k] += L[k];
+                dimg[k] -= 1;
+                wrapped = true;
+            }
+        }
+        if (wrapped) {
+            int4 im = a.img[i];
+            im.x += dimg[0];
+            im.y += dimg[1];
+            im.z += dimg[2];
+            a.img[i] = im;
+        }
+        if (!(fabsf(r[0]) <= L[0] && fabsf(r[1]) <= L[1] && fabsf(r[2]) <= L[2]))
+            atomicOr(&ctrl->status, GDB_STATUS_NAN);
+        const float4 pn = make_float4(r[0], r[1], r[2], pi.w);
+        pos_next[i] = pn;
+        a.vel[i] = make_float4(vv[0], vv[1], vv[2], m);
+        a.pscal[3 * n + i] = kin;
+        a.pscal[4 * n + i] = fsq;
+        // skin check for the next step (nblist.py:57-86)
+        moved |= dist_sq_exact<false>(pn, a.rref[i], a.Lx, a.Ly, a.Lz) > a.skin2q;
+        red[0] += kin;
+        if (reset) {
+            red[5] += (double)m * vv[0];
+            red[6] += (double)m * vv[1];
+            red[7] += (double)m * vv[2];
+            red[8] += m;
+        }
+    }
+    if (MODE == MODE_STEP) {
+        // inside the persistent kernel other blocks may still be reading
+        // ctrl->rebuild for this step: stage the flag, the barrier promotes it
+        if (__syncthreads_or(moved) && threadIdx.x == 0) {
+            if (PERSIST)
+                ctrl->rebuild_next = 1;
+            else
+                ctrl->rebuild = 1;
+        }
+    }
+    block_sum<NQ>(red, s_red);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) a.partials[(size_t)blockIdx.x * NQ + q] = red[q];
+    }
+}
+
+// Fixed-order float64 sum of the partials of `nblocks` blocks and the
+// bookkeeping of a finished step (NVT.py:226-237, scalar_saver.py:274-288,
+// momentum_reset.py:379-393).  Run by one whole block.
+template <int MODE>
+__device__ void finalize_step(const SimArgs &a, int step, int nblocks, double *s_red) {
+    DevCtrl *ctrl = a.ctrl;
+    const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
+    const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
+    const int par = step & 1, ppar = par ^ 1;
+    double tot[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) tot[q] = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+#pragma unroll
+        for (int q = 0; q < NQ; q++) tot[q] += __ldcg(a.partials + (size_t)b * NQ + q);
+    }
+    block_sum<NQ>(tot, s_red);
+    if (threadIdx.x == 0) {
+        if (MODE == MODE_STEP) {
+            const double time = ctrl->time_zero + (double)step * (double)a.dt;
+            if (a.omega2 > 0.f) {
+                const double T = target_temperature(a, time);
+                const double dev = 2.0 * tot[0] / ((double)a.dof * T) - 1.0;
+                ctrl->xi = (float)((double)ctrl->xi + (double)(a.dt * a.omega2) * dev);
+            }
+            ctrl->sumK = (float)tot[0];
+            if (rec && step / a.every < a.nrows) {
+                double *row = a.rows + (size_t)(step / a.every) * GDB_NUM_SCALARS;
+                row[GDB_SCALAR_U] = tot[1];
+                row[GDB_SCALAR_W] = tot[2];
+                row[GDB_SCALAR_LAPU] = tot[3];
+                row[GDB_SCALAR_K] = tot[0];
+                row[GDB_SCALAR_FSQ] = tot[4];
+            }
+            if (reset) {
+                ctrl->shift[par][0] = (float)(tot[5] / tot[8]);
+                ctrl->shift[par][1] = (float)(tot[6] / tot[8]);
+                ctrl->shift[par][2] = (float)(tot[7] / tot[8]);
+                ctrl->pending[par] = 1;
+            }
+            ctrl->step = step + 1;
+        } else {
+            ctrl->evalU = tot[1];
+            ctrl->evalW = tot[2];
+        }
+        ctrl->pending[ppar] = 0;
+    }
+}
+
+}  // namespace gdb

@@ -69,9 +69,10 @@ def get_default_compute_plan(configuration):
 
 
 def _lanes(tp):
-    """Library lanes per particle for a gamdpy ``tp``: largest of 1, 2, 4, 8 <= tp."""
+    """Library lanes per particle for a gamdpy ``tp``: largest power of two
+    <= tp, at most 32."""
     t = 1
-    while t * 2 <= min(int(tp), 8):
+    while t * 2 <= min(int(tp), 32):
         t *= 2
     return t
 
@@ -151,7 +152,9 @@ class Simulation:
         conf._device = self._sim
         self._sim.set_box(conf.simbox.lengths)
         pp.configure_device(self._sim, conf, self.compute_plan)
-        self._sim.set_plan(_lanes(self.compute_plan.get("tp", 0)) if self.compute_plan.get("tp") else 0)
+        # gamdpy's tp heuristic targets its own launch shape; the library picks
+        # lanes per particle for B200 unless the plan sets "lanes"
+        self._sim.set_plan(int(self.compute_plan.get("lanes", 0)))
         self.integrator.configure_device(self._sim, conf)
         scalar_every, reset_every, conf_per_block = 0, 0, 0
         self._scalar_saver = self._conf_saver = None
@@ -267,10 +270,11 @@ class Simulation:
         """Steps per second over the timed blocks, as benchmarks/benchmark_LJ.py:90."""
         return self.last_num_blocks * self.steps_per_block / (np.sum(self.timing_numba_blocks) / 1000)
 
-    def autotune(self, tps_candidates=(1, 2, 4, 8), skins=None, steps=None, verbose=False):
+    def autotune(self, tps_candidates=(1, 2, 4, 8, 16, 32), skins=None, steps=None, verbose=False):
         """Pick lanes per particle (and optionally skin) by timing short runs,
         as Simulation.autotune (Simulation.py:636-821) does for pb/tp/skin.
-        Keeps the fastest plan; the configuration is restored afterwards."""
+        Keeps the fastest plan (``compute_plan['lanes']``, ``['skin']``); the
+        configuration is restored afterwards."""
         steps = steps or min(self.steps_per_block, 256)
         conf = self.configuration
         saved = (conf["r"].copy(), conf["v"].copy(), conf.r_im.copy())
@@ -281,7 +285,7 @@ class Simulation:
         for skin in skins:
             for tp in tps_candidates:
                 self.compute_plan["skin"] = skin
-                self.compute_plan["tp"] = tp
+                self.compute_plan["lanes"] = tp
                 self._sim.set_nblist(pp.nblist.kind, float(np.float32(skin)), pp.max_num_nbs)
                 self._sim.set_plan(tp)
                 conf.copy_to_device()
@@ -292,7 +296,7 @@ class Simulation:
                 if best is None or ms < best[0]:
                     best = (ms, tp, skin)
         _, tp, skin = best
-        self.compute_plan["tp"], self.compute_plan["skin"] = tp, skin
+        self.compute_plan["lanes"], self.compute_plan["skin"] = tp, skin
         self._sim.set_nblist(pp.nblist.kind, float(np.float32(skin)), pp.max_num_nbs)
         self._sim.set_plan(tp)
         conf["r"], conf["v"] = saved[0], saved[1]

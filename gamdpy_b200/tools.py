@@ -3,7 +3,7 @@ without time stepping."""
 import numpy as np
 
 from . import _lib
-from .simulation import _lanes, get_default_compute_plan
+from .simulation import get_default_compute_plan
 
 
 class Evaluator:
@@ -24,8 +24,7 @@ class Evaluator:
         self._sim = _lib.Sim(configuration.N, table.shape[0], device)
         self._sim.set_box(configuration.simbox.lengths)
         pp.configure_device(self._sim, configuration, self.compute_plan)
-        tp = self.compute_plan.get("tp", 0)
-        self._sim.set_plan(_lanes(tp) if tp else 0)
+        self._sim.set_plan(int(self.compute_plan.get("lanes", 0)))
 
     def evaluate(self, configuration=None):
         conf = configuration if configuration is not None else self.configuration

@@ -36,6 +36,7 @@ extern "C" {
 #define GDB_ERR_NBLIST 4   /* neighbour-list overflow (count >= max_nbs) */
 #define GDB_ERR_NUMERIC 5  /* non-finite position seen by a kernel */
 #define GDB_ERR_UNSUPPORTED 6
+#define GDB_ERR_TIMEOUT 7  /* a bounded wait inside a kernel gave up (status bit BARRIER_TIMEOUT) */
 
 /* status-word bits (gdb_status_word), set by kernels, cleared by gdb_clear_status */
 #define GDB_STATUS_NBLIST_OVERFLOW 0x1u
@@ -108,8 +109,9 @@ int gdb_set_pair_potential(gdb_sim *h, int kind, int cutmode, int ntypes, const 
  * pair_potential.py:84-97; compute_plan['nblist'], ['skin']). */
 int gdb_set_nblist(gdb_sim *h, int kind, float skin, int max_nbs);
 
-/* Threads per particle (compute_plan['tp'], simulation/get_default_compute_plan.py:55-63)
- * and particles per thread block (compute_plan['pb']).  0 = choose. */
+/* Threads per particle (compute_plan['tp'], simulation/get_default_compute_plan.py:55-63):
+ * 1, 2, 4, 8, 16 or 32 lanes share one particle's neighbours; 0 = choose.
+ * pb (particles per block) is accepted for compatibility.  0 = choose. */
 int gdb_set_plan(gdb_sim *h, int tp, int pb);
 
 /* Integrators: NVE.get_params (integrators/NVE.py:29-31);
@@ -152,6 +154,15 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms);
  * duration.  Advances the state; intended for benchmarks (the reference
  * times whole timeblocks with CUDA events, simulation/Simulation.py:404-448). */
 int gdb_time_step_kernel(gdb_sim *h, int reps, float *ms_per_launch);
+
+/* Phase trace of the persistent step kernel (tracing aid; no counterpart in
+ * the reference, which times whole timeblocks only): with capacity > 0,
+ * every grid barrier appends (tag << 56 | globaltimer ns); tags: 1 step,
+ * 2 final evaluation, 3 rebuild phase, 4 rebuild done, 5 kernel start.
+ * gdb_get_trace copies up to `capacity` entries, sets *count and restarts
+ * the trace.  capacity 0 switches tracing off. */
+int gdb_set_trace(gdb_sim *h, int capacity);
+int gdb_get_trace(gdb_sim *h, unsigned long long *out, int capacity, int *count);
 
 /* Mean and maximum neighbour count of the current list (per particle). */
 int gdb_nblist_stats(gdb_sim *h, double *mean_count, int *max_count);

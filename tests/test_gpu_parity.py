@@ -36,7 +36,8 @@ def table_of(d):
     return O.param_table([d["sigma"], d["epsilon"], d["cut"]])
 
 
-@pytest.mark.parametrize("name,tp", [("lj256_sf", 0), ("lj256_sp", 0), ("lj256_sf", 1), ("lj256_sf", 4)])
+@pytest.mark.parametrize("name,tp", [("lj256_sf", 0), ("lj256_sp", 0), ("lj256_sf", 1), ("lj256_sf", 4),
+                                     ("lj256_sf", 16)])
 def test_nsq_list_and_forces_vs_gamdpy(name, tp):
     d = golden(name)
     cm = _lib.CUT_SHIFTED_FORCE if str(d["cutoff"]) == "SF" else _lib.CUT_SHIFTED_POTENTIAL
@@ -52,7 +53,7 @@ def test_nsq_list_and_forces_vs_gamdpy(name, tp):
         assert rel_rms(sc[k], d[k]) < FORCE_TOL, k
 
 
-@pytest.mark.parametrize("tp", [0, 1, 2, 8])
+@pytest.mark.parametrize("tp", [0, 1, 2, 8, 32])
 def test_cell_list_and_forces_vs_gamdpy(tp):
     d = golden("ka1372_cells")
     sim = make_sim(d["r"], d["box"], d["ptype"], table_of(d), nblist=_lib.NBLIST_CELLS, skin=float(d["skin"]),
