@@ -52,6 +52,7 @@ struct PairTable {
 struct DevCtrl {
     int rebuild;       // 1 = neighbour list must be rebuilt before the next force evaluation
     int rebuild_next;  // set during a persistent step, promoted to `rebuild` at the barrier
+    int cell_wrap;     // a coordinate sat exactly on +L/2 (binned to cell 0 by the modulo)
     int maxcount;      // largest neighbour count of the last build
     int nrebuild;      // number of builds (gamdpy nbflag[2])
     unsigned status;   // GDB_STATUS_* bits

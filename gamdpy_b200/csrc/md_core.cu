@@ -36,7 +36,7 @@
 
 #include "../../include/gamdb200.h"
 #include "gdb_internal.cuh"
-#include "md_phases.cuh"
+#include "md_kernels.cuh"
 
 using namespace gdb;
 
@@ -180,117 +180,6 @@ __global__ void __launch_bounds__(GDB_BLOCK) k_finish_cells(SimArgs a, int cur) 
 }
 __global__ void k_rebuild_done(DevCtrl *ctrl) {
     if (ctrl->rebuild) rebuild_done(ctrl);
-}
-
-template <bool NT1>
-__device__ __forceinline__ void load_table(const PairTable &tab, PairEntry *s_tab) {
-    if (NT1) {
-        if (threadIdx.x == 0) s_tab[0] = tab.e[0];
-    } else {
-        for (int t = threadIdx.x; t < tab.nt * tab.nt; t += blockDim.x) s_tab[t] = tab.e[t];
-    }
-    __syncthreads();
-}
-
-// one step (or the force-only evaluation); the last block to finish does
-// the float64 bookkeeping
-// register budget: 64 per thread (4 blocks/SM) for one lane per particle,
-// 80 (3 blocks/SM) when lanes share a particle (measured best on B200)
-#define GDB_STEP_MINBLOCKS(TP) ((TP) == 1 ? 4 : 3)
-
-template <int TP, bool NT1, int INTEG, int MODE>
-__global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_step(SimArgs a, PairTable tab, int cur) {
-    __shared__ PairEntry s_tab[NT1 ? 1 : GDB_MAX_TYPES * GDB_MAX_TYPES];
-    __shared__ double s_red[NQ * 32];
-    __shared__ bool s_last;
-    load_table<NT1>(tab, s_tab);
-    DevCtrl *ctrl = a.ctrl;
-    const int step = ctrl->step;
-    phase_step<TP, NT1, INTEG, MODE, true, false>(a, s_tab, tab.nt, cur, step, s_red);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!s_last) return;
-    finalize_step<MODE>(a, step, gridDim.x, s_red);
-    if (threadIdx.x == 0) ctrl->ticket = 0;
-}
-
-// Rebuild inside the persistent kernel: the same phases with grid barriers.
-template <bool FMA>
-__device__ bool rebuild_persistent(const SimArgs &a, int cur) {
-    DevCtrl *c = a.ctrl;
-    auto none = [] {};
-    if (a.nb_kind == GDB_NBLIST_NSQ) {
-        phase_nbl_nsq<FMA, false>(a, cur);
-        const bool ok = grid_barrier(c, [&] {
-            if (threadIdx.x == 0) rebuild_done(c);
-        });
-        trace_mark(c, TR_REBUILD_DONE);
-        return ok;
-    }
-    phase_cell_assign<false>(a, cur);
-    if (!grid_barrier(c, none)) return false;
-    trace_mark(c, TR_REBUILD_PHASE);
-    phase_scan_partial(a);
-    if (!grid_barrier(c, [&] { block_scan_chunks(a); })) return false;
-    phase_scan_final(a);
-    if (!grid_barrier(c, none)) return false;
-    phase_scatter(a);
-    if (!grid_barrier(c, none)) return false;
-    trace_mark(c, TR_REBUILD_PHASE);
-    phase_sort_cells(a);
-    if (!grid_barrier(c, none)) return false;
-    phase_gather(a, cur);
-    if (!grid_barrier(c, none)) return false;
-    trace_mark(c, TR_REBUILD_PHASE);
-    phase_nbl_cells<FMA>(a);
-    if (!grid_barrier(c, none)) return false;
-    trace_mark(c, TR_REBUILD_PHASE);
-    phase_finish_cells(a, cur);
-    const bool ok = grid_barrier(c, [&] {
-        if (threadIdx.x == 0) rebuild_done(c);
-    });
-    trace_mark(c, TR_REBUILD_DONE);
-    return ok;
-}
-
-// Persistent cooperative kernel: `nsteps` steps starting from pos[cur0], then
-// (if do_eval) the force-only evaluation of the final state -- one timeblock
-// of simulation/Simulation.py:306-328 in one launch.
-template <int TP, bool NT1, int INTEG>
-__global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
-    __shared__ PairEntry s_tab[NT1 ? 1 : GDB_MAX_TYPES * GDB_MAX_TYPES];
-    __shared__ double s_red[NQ * 32];
-    load_table<NT1>(tab, s_tab);
-    DevCtrl *ctrl = a.ctrl;
-    int cur = cur0;
-    trace_mark(ctrl, TR_START);
-    for (int s = 0; s < nsteps + do_eval; s++) {
-        if (*(volatile int *)&ctrl->rebuild) {
-            const bool ok = a.fma ? rebuild_persistent<true>(a, cur) : rebuild_persistent<false>(a, cur);
-            if (!ok) return;
-        }
-        const int step = *(volatile int *)&ctrl->step;
-        bool ok;
-        if (s < nsteps) {
-            phase_step<TP, NT1, INTEG, MODE_STEP, false, true>(a, s_tab, tab.nt, cur, step, s_red);
-            ok = grid_barrier(ctrl, [&] {
-                finalize_step<MODE_STEP>(a, step, gridDim.x, s_red);
-                if (threadIdx.x == 0 && ctrl->rebuild_next) {
-                    ctrl->rebuild = 1;
-                    ctrl->rebuild_next = 0;
-                }
-            });
-            cur ^= 1;
-            trace_mark(ctrl, TR_STEP);
-        } else {
-            phase_step<TP, NT1, INTEG, MODE_EVAL, false, true>(a, s_tab, tab.nt, cur, step, s_red);
-            ok = grid_barrier(ctrl, [&] { finalize_step<MODE_EVAL>(a, step, gridDim.x, s_red); });
-            trace_mark(ctrl, TR_EVAL);
-        }
-        if (!ok) return;
-    }
 }
 
 __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
@@ -562,59 +451,20 @@ static int enqueue_rebuild(gdb_sim *h) {
     return GDB_OK;
 }
 
-template <int TP, bool NT1>
-static void launch_step_tp(gdb_sim *h, const SimArgs &a, int mode, int grid) {
-    const int cur = h->cur;
-    if (mode == MODE_EVAL)
-        k_step<TP, NT1, 0, MODE_EVAL><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table, cur);
-    else if (h->integ == GDB_INTEGRATOR_NVT)
-        k_step<TP, NT1, GDB_INTEGRATOR_NVT, MODE_STEP><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table, cur);
-    else
-        k_step<TP, NT1, GDB_INTEGRATOR_NVE, MODE_STEP><<<grid, GDB_BLOCK, 0, h->st>>>(a, h->table, cur);
-}
-
-template <bool NT1>
-static void launch_step_nt(gdb_sim *h, const SimArgs &a, int mode, int grid) {
-    switch (h->tp) {
-        case 1: launch_step_tp<1, NT1>(h, a, mode, grid); break;
-        case 2: launch_step_tp<2, NT1>(h, a, mode, grid); break;
-        case 4: launch_step_tp<4, NT1>(h, a, mode, grid); break;
-        case 8: launch_step_tp<8, NT1>(h, a, mode, grid); break;
-        case 16: launch_step_tp<16, NT1>(h, a, mode, grid); break;
-        default: launch_step_tp<32, NT1>(h, a, mode, grid); break;
-    }
-}
-
 static int enqueue_step(gdb_sim *h, int mode) {
     const int grid = grid_for((long long)h->n * h->tp);
     int rc = ensure_partials(h, grid);
     if (rc) return rc;
     const SimArgs a = make_args(h);
     if (h->ntypes == 1)
-        launch_step_nt<true>(h, a, mode, grid);
+        launch_step_nt1(a, h->table, h->st, h->tp, h->integ, mode, grid, h->cur);
+    else if (h->ntypes == 2)
+        launch_step_nt2(a, h->table, h->st, h->tp, h->integ, mode, grid, h->cur);
     else
-        launch_step_nt<false>(h, a, mode, grid);
+        launch_step_ntg(a, h->table, h->st, h->tp, h->integ, mode, grid, h->cur);
     CKL();
     if (mode == MODE_STEP) h->cur ^= 1;
     return GDB_OK;
-}
-
-// The k_run instantiation for the handle's lanes, type count and integrator.
-template <int TP, bool NT1>
-static const void *run_kernel_tp(int integ) {
-    return integ == GDB_INTEGRATOR_NVT ? (const void *)k_run<TP, NT1, GDB_INTEGRATOR_NVT>
-                                       : (const void *)k_run<TP, NT1, GDB_INTEGRATOR_NVE>;
-}
-template <bool NT1>
-static const void *run_kernel_nt(int tp, int integ) {
-    switch (tp) {
-        case 1: return run_kernel_tp<1, NT1>(integ);
-        case 2: return run_kernel_tp<2, NT1>(integ);
-        case 4: return run_kernel_tp<4, NT1>(integ);
-        case 8: return run_kernel_tp<8, NT1>(integ);
-        case 16: return run_kernel_tp<16, NT1>(integ);
-        default: return run_kernel_tp<32, NT1>(integ);
-    }
 }
 
 // Grid of the persistent kernel: every block resident (cooperative launch).
@@ -629,7 +479,9 @@ static int run_grid(gdb_sim *h, const void *fn, int *grid) {
 
 // One launch of k_run: `steps` steps from pos[cur], then the final evaluation.
 static int launch_run(gdb_sim *h, int steps, int do_eval) {
-    const void *fn = h->ntypes == 1 ? run_kernel_nt<true>(h->tp, h->integ) : run_kernel_nt<false>(h->tp, h->integ);
+    const void *fn = h->ntypes == 1   ? run_kernel_nt1(h->tp, h->integ)
+                     : h->ntypes == 2 ? run_kernel_nt2(h->tp, h->integ)
+                                      : run_kernel_ntg(h->tp, h->integ);
     int grid = 0;
     int rc = run_grid(h, fn, &grid);
     if (rc) return rc;

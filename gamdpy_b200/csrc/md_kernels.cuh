@@ -1,0 +1,171 @@
+// md_kernels.cuh -- the fused step kernel (k_step, one step per launch) and
+// the persistent kernel (k_run, a timeblock per launch), instantiated per
+// type-count path in md_inst_nt1.cu / md_inst_nt2.cu / md_inst_ntg.cu so the
+// instantiations compile in parallel.
+#pragma once
+
+#include "md_phases.cuh"
+
+namespace gdb {
+
+__device__ __forceinline__ void load_table(const PairTable &tab, PairEntry *s_tab) {
+    for (int t = threadIdx.x; t < tab.nt * tab.nt; t += blockDim.x) s_tab[t] = tab.e[t];
+    __syncthreads();
+}
+
+// one step (or the force-only evaluation); the last block to finish does
+// the float64 bookkeeping
+// register budget: 64 per thread (4 blocks/SM) for one lane per particle,
+// 80 (3 blocks/SM) when lanes share a particle (measured best on B200); the
+// persistent kernel also holds the list-build phase
+#define GDB_STEP_MINBLOCKS(TP) ((TP) == 1 ? 4 : 3)
+#ifndef GDB_RUN_MINBLOCKS_TP1
+#define GDB_RUN_MINBLOCKS_TP1 4
+#endif
+#define GDB_RUN_MINBLOCKS(TP) ((TP) == 1 ? GDB_RUN_MINBLOCKS_TP1 : 3)
+
+template <int TP, int NT, int INTEG, int MODE>
+__global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_step(SimArgs a, PairTable tab, int cur) {
+    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    __shared__ bool s_last;
+    load_table(tab, s_tab);
+    DevCtrl *ctrl = a.ctrl;
+    const int step = ctrl->step;
+    phase_step<TP, NT, INTEG, MODE, true, false>(a, s_tab, tab.nt, cur, step, s_red);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    finalize_step<MODE>(a, step, gridDim.x, s_red);
+    if (threadIdx.x == 0) ctrl->ticket = 0;
+}
+
+// Rebuild inside the persistent kernel: the same phases with grid barriers.
+template <bool FMA>
+__device__ inline bool rebuild_persistent(const SimArgs &a, int cur) {
+    DevCtrl *c = a.ctrl;
+    auto none = [] {};
+    if (a.nb_kind == GDB_NBLIST_NSQ) {
+        phase_nbl_nsq<FMA, false>(a, cur);
+        const bool ok = grid_barrier(c, [&] {
+            if (threadIdx.x == 0) rebuild_done(c);
+        });
+        trace_mark(c, TR_REBUILD_DONE);
+        return ok;
+    }
+    phase_cell_assign<false>(a, cur);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_scan_partial(a);
+    if (!grid_barrier(c, [&] { block_scan_chunks(a); })) return false;
+    phase_scan_final(a);
+    if (!grid_barrier(c, none)) return false;
+    phase_scatter(a);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_sort_cells(a);
+    if (!grid_barrier(c, none)) return false;
+    phase_gather(a, cur);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_nbl_cells<FMA>(a);
+    if (!grid_barrier(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_finish_cells(a, cur);
+    const bool ok = grid_barrier(c, [&] {
+        if (threadIdx.x == 0) rebuild_done(c);
+    });
+    trace_mark(c, TR_REBUILD_DONE);
+    return ok;
+}
+
+// Persistent cooperative kernel: `nsteps` steps starting from pos[cur0], then
+// (if do_eval) the force-only evaluation of the final state -- one timeblock
+// of simulation/Simulation.py:306-328 in one launch.
+template <int TP, int NT, int INTEG>
+__global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
+    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    load_table(tab, s_tab);
+    DevCtrl *ctrl = a.ctrl;
+    int cur = cur0;
+    trace_mark(ctrl, TR_START);
+    for (int s = 0; s < nsteps + do_eval; s++) {
+        if (*(volatile int *)&ctrl->rebuild) {
+            const bool ok = a.fma ? rebuild_persistent<true>(a, cur) : rebuild_persistent<false>(a, cur);
+            if (!ok) return;
+        }
+        const int step = *(volatile int *)&ctrl->step;
+        bool ok;
+        if (s < nsteps) {
+            phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, tab.nt, cur, step, s_red);
+            ok = grid_barrier(ctrl, [&] {
+                finalize_step<MODE_STEP>(a, step, gridDim.x, s_red);
+                if (threadIdx.x == 0 && ctrl->rebuild_next) {
+                    ctrl->rebuild = 1;
+                    ctrl->rebuild_next = 0;
+                }
+            });
+            cur ^= 1;
+            trace_mark(ctrl, TR_STEP);
+        } else {
+            phase_step<TP, NT, INTEG, MODE_EVAL, false, true>(a, s_tab, tab.nt, cur, step, s_red);
+            ok = grid_barrier(ctrl, [&] { finalize_step<MODE_EVAL>(a, step, gridDim.x, s_red); });
+            trace_mark(ctrl, TR_EVAL);
+        }
+        if (!ok) return;
+    }
+}
+
+
+// Entry points each instantiation unit exports to the host code.
+#define GDB_DECLARE_NT(NTNAME)                                                                          \
+    void launch_step_##NTNAME(const SimArgs &a, const PairTable &tab, cudaStream_t st, int tp, int integ, \
+                              int mode, int grid, int cur);                                            \
+    const void *run_kernel_##NTNAME(int tp, int integ);
+
+GDB_DECLARE_NT(nt1)
+GDB_DECLARE_NT(nt2)
+GDB_DECLARE_NT(ntg)
+
+#define GDB_DEFINE_NT(NTNAME, NT)                                                                            \
+    template <int TP>                                                                                        \
+    static void step_tp_##NTNAME(const SimArgs &a, const PairTable &tab, cudaStream_t st, int integ, int mode, \
+                                 int grid, int cur) {                                                        \
+        if (mode == MODE_EVAL)                                                                               \
+            k_step<TP, NT, 0, MODE_EVAL><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);                           \
+        else if (integ == GDB_INTEGRATOR_NVT)                                                                \
+            k_step<TP, NT, GDB_INTEGRATOR_NVT, MODE_STEP><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);          \
+        else                                                                                                 \
+            k_step<TP, NT, GDB_INTEGRATOR_NVE, MODE_STEP><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);          \
+    }                                                                                                        \
+    void launch_step_##NTNAME(const SimArgs &a, const PairTable &tab, cudaStream_t st, int tp, int integ,    \
+                              int mode, int grid, int cur) {                                                 \
+        switch (tp) {                                                                                        \
+            case 1: step_tp_##NTNAME<1>(a, tab, st, integ, mode, grid, cur); break;                          \
+            case 2: step_tp_##NTNAME<2>(a, tab, st, integ, mode, grid, cur); break;                          \
+            case 4: step_tp_##NTNAME<4>(a, tab, st, integ, mode, grid, cur); break;                          \
+            case 8: step_tp_##NTNAME<8>(a, tab, st, integ, mode, grid, cur); break;                          \
+            case 16: step_tp_##NTNAME<16>(a, tab, st, integ, mode, grid, cur); break;                        \
+            default: step_tp_##NTNAME<32>(a, tab, st, integ, mode, grid, cur); break;                       \
+        }                                                                                                    \
+    }                                                                                                        \
+    template <int TP>                                                                                        \
+    static const void *run_tp_##NTNAME(int integ) {                                                          \
+        return integ == GDB_INTEGRATOR_NVT ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVT>                 \
+                                           : (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVE>;                \
+    }                                                                                                        \
+    const void *run_kernel_##NTNAME(int tp, int integ) {                                                     \
+        switch (tp) {                                                                                        \
+            case 1: return run_tp_##NTNAME<1>(integ);                                                        \
+            case 2: return run_tp_##NTNAME<2>(integ);                                                        \
+            case 4: return run_tp_##NTNAME<4>(integ);                                                        \
+            case 8: return run_tp_##NTNAME<8>(integ);                                                        \
+            case 16: return run_tp_##NTNAME<16>(integ);                                                      \
+            default: return run_tp_##NTNAME<32>(integ);                                                      \
+        }                                                                                                    \
+    }
+
+}  // namespace gdb

@@ -14,6 +14,7 @@
 // where kernel boundaries order the accesses.
 #pragma once
 
+#include "../../include/gamdb200.h"
 #include "gdb_internal.cuh"
 
 namespace gdb {
@@ -126,7 +127,7 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
 // N^2 build (interactions/nblist.py:88-143): one warp per particle, lanes
 // stride over j, ballot + popc append hits in ascending j (deterministic).
 template <bool FMA, bool NC>
-__device__ void phase_nbl_nsq(const SimArgs &a, int cur) {
+__device__ inline void phase_nbl_nsq(const SimArgs &a, int cur) {
     const float4 *pos = cur_pos(a, cur);
     const int lane = threadIdx.x & 31;
     const int warps = (gridDim.x * blockDim.x) >> 5;
@@ -163,11 +164,14 @@ __device__ __forceinline__ int cell_coord(float x, float L, int nc, DevCtrl *ctr
     const long long c = (long long)floor(v);
     long long m = c % nc;
     if (m < 0) m += nc;
+    // outside [0, nc) only for a coordinate on the box face (or beyond it):
+    // the build then uses the general minimum-image test
+    if (c != m) ctrl->cell_wrap = 1;
     return (int)m;
 }
 
 template <bool NC>
-__device__ void phase_cell_assign(const SimArgs &a, int cur) {
+__device__ inline void phase_cell_assign(const SimArgs &a, int cur) {
     const float4 *pos = cur_pos(a, cur);
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
         const float4 p = load<NC>(pos + i);
@@ -224,7 +228,7 @@ __device__ __forceinline__ void chunk_scan(const int *in, int len, int base, int
     __syncthreads();
 }
 
-__device__ void phase_scan_partial(const SimArgs &a) {
+__device__ inline void phase_scan_partial(const SimArgs &a) {
     __shared__ int sm[32];
     __shared__ int tot;
     for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x) {
@@ -235,7 +239,7 @@ __device__ void phase_scan_partial(const SimArgs &a) {
 }
 
 // exclusive scan of the chunk sums, by one block
-__device__ void block_scan_chunks(const SimArgs &a) {
+__device__ inline void block_scan_chunks(const SimArgs &a) {
     __shared__ int sm[32];
     __shared__ int tot;
     int carry = 0;
@@ -246,21 +250,21 @@ __device__ void block_scan_chunks(const SimArgs &a) {
     }
 }
 
-__device__ void phase_scan_final(const SimArgs &a) {
+__device__ inline void phase_scan_final(const SimArgs &a) {
     __shared__ int sm[32];
     for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x)
         chunk_scan(a.cell_count, a.ncell, c * SCAN_CHUNK, a.cell_start, a.bsum[c], nullptr, sm);
     if (blockIdx.x == 0 && threadIdx.x == 0) a.cell_start[a.ncell] = a.n;
 }
 
-__device__ void phase_scatter(const SimArgs &a) {
+__device__ inline void phase_scatter(const SimArgs &a) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
         a.perm[a.cell_start[a.pcell[i]] + a.prank[i]] = i;
 }
 
 // Order every cell's particles by user index: the atomics of the assignment
 // rank them arbitrarily; this makes the layout and every sum deterministic.
-__device__ void phase_sort_cells(const SimArgs &a) {
+__device__ inline void phase_sort_cells(const SimArgs &a) {
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += gridDim.x * blockDim.x) {
         const int lo = a.cell_start[c], hi = a.cell_start[c + 1];
         for (int x = lo + 1; x < hi; x++) {
@@ -276,7 +280,7 @@ __device__ void phase_sort_cells(const SimArgs &a) {
     }
 }
 
-__device__ void phase_gather(const SimArgs &a, int cur) {
+__device__ inline void phase_gather(const SimArgs &a, int cur) {
     const float4 *pos = cur_pos(a, cur);
     const size_t n = a.n;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
@@ -293,28 +297,57 @@ __device__ void phase_gather(const SimArgs &a, int cur) {
     }
 }
 
+// Exact squared distance with a known periodic shift per component: the
+// reference computes d = rj - ri, then d += -L / +L / 0 from 2d vs L
+// (orthorhombic.py:59-73).  When the shift is known in advance the result is
+// __fadd_rn(__fsub_rn(rj, ri), shift), bit for bit.
+template <bool FMA>
+__device__ __forceinline__ float dist_sq_shifted(float4 pj, float4 pi, float sx, float sy, float sz) {
+    const float dx = __fadd_rn(__fsub_rn(pj.x, pi.x), sx);
+    const float dy = __fadd_rn(__fsub_rn(pj.y, pi.y), sy);
+    const float dz = __fadd_rn(__fsub_rn(pj.z, pi.z), sz);
+    float s = __fmul_rn(dx, dx);
+    if (FMA) {
+        s = __fmaf_rn(dy, dy, s);
+        s = __fmaf_rn(dz, dz, s);
+    } else {
+        s = __fadd_rn(s, __fmul_rn(dy, dy));
+        s = __fadd_rn(s, __fmul_rn(dz, dz));
+    }
+    return s;
+}
+
 // Cell-list build (nblist_linked_lists.py:133-183 semantics: all particles of
 // the 5x5x5 stencil with dist_sq < (max_cut+skin)^2, j != i).  One warp per
 // cell: the cell's particles share the stencil.  Slots are sorted by cell
 // with x fastest, so the five x-cells of one (dy, dz) row are one contiguous
 // slot range (two at the x wrap); the warp lists the <= 50 ranges with their
-// prefix sums in shared memory and walks the packed candidate sequence 32 at a
-// time, testing each candidate against up to NBW particles of the cell held
+// prefix sums in shared memory and walks the packed candidate sequence 64 at
+// a time, testing each candidate against up to NBW particles of the cell held
 // in registers.  Ballot + popc append in candidate order: deterministic.
-// Grids with fewer than five cells in a dimension visit each cell once.
-constexpr int NBW = 8;        // particles of a cell handled per pass
+//
+// SHIFTED (every dimension >= 7 cells, no coordinate on a box face): a pair
+// in cells at most two apart is closer than 3 cell edges < L/2 without a
+// wrap and farther than L/2 with one, so the minimum-image decision of the
+// reference is fixed per range and the distance needs no comparisons.
+// Otherwise (small grids) every candidate takes the reference's full test,
+// and grids with fewer than five cells in a dimension visit each cell once.
+constexpr int NBW = 4;         // particles of a cell handled per pass
 constexpr int NB_SEG_MAX = 64; // 25 rows x at most 2 ranges
 
 __device__ __forceinline__ int wrapi(int x, int n) { return ((x % n) + n) % n; }
 
-template <bool FMA>
-__device__ void phase_nbl_cells(const SimArgs &a) {
+template <bool FMA, bool SHIFTED>
+__device__ inline void phase_nbl_cells_t(const SimArgs &a) {
     __shared__ int s_lo[GDB_BLOCK / 32][NB_SEG_MAX];
     __shared__ int s_pre[GDB_BLOCK / 32][NB_SEG_MAX + 1];
+    __shared__ float3 s_sh[GDB_BLOCK / 32][SHIFTED ? NB_SEG_MAX : 1];
     const float4 *pos = a.pos_tmp;
     const int ncx = a.ncx, ncy = a.ncy, ncz = a.ncz;
+    const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int *lo_s = s_lo[wib], *pre_s = s_pre[wib];
+    float3 *sh_s = s_sh[wib];
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     const int ry = ncy < 5 ? ncy : 5, rz = ncz < 5 ? ncz : 5;
     const int nrows = ry * rz;
@@ -324,10 +357,16 @@ __device__ void phase_nbl_cells(const SimArgs &a) {
         const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
         // lane r < nrows builds the x-range(s) of stencil row r
         int len0 = 0, len1 = 0, lo0 = 0, lo1 = 0;
+        float sy = 0.f, sz = 0.f, sx0 = 0.f, sx1 = 0.f;
         if (lane < nrows) {
             const int za = lane / ry, yb = lane % ry;
-            const int z = ncz < 5 ? za : wrapi(cz - 2 + za, ncz);
-            const int y = ncy < 5 ? yb : wrapi(cy - 2 + yb, ncy);
+            const int zu = cz - 2 + za, yu = cy - 2 + yb;  // unwrapped (SHIFTED: grid >= 7 cells)
+            const int z = ncz < 5 ? za : wrapi(zu, ncz);
+            const int y = ncy < 5 ? yb : wrapi(yu, ncy);
+            if (SHIFTED) {  // cells past the low face hold coordinates near +L/2: shift -L
+                sz = zu < 0 ? -Lz : (zu >= ncz ? Lz : 0.f);
+                sy = yu < 0 ? -Ly : (yu >= ncy ? Ly : 0.f);
+            }
             const int rowbase = (z * ncy + y) * ncx;
             int l0, h0, l1 = 0, h1 = 0;
             if (ncx <= 5) {
@@ -343,11 +382,13 @@ __device__ void phase_nbl_cells(const SimArgs &a) {
                     h0 = rowbase + ncx;
                     l1 = rowbase;
                     h1 = rowbase + x1 + 1;
+                    sx0 = -Lx;
                 } else {
                     l0 = rowbase + x0;
                     h0 = rowbase + ncx;
                     l1 = rowbase;
                     h1 = rowbase + x1 - ncx + 1;
+                    sx1 = Lx;
                 }
             }
             lo0 = a.cell_start[l0];
@@ -371,6 +412,10 @@ __device__ void phase_nbl_cells(const SimArgs &a) {
             pre_s[2 * lane] = excl;
             lo_s[2 * lane + 1] = lo1;
             pre_s[2 * lane + 1] = excl + len0;
+            if (SHIFTED) {
+                sh_s[2 * lane] = make_float3(sx0, sy, sz);
+                sh_s[2 * lane + 1] = make_float3(sx1, sy, sz);
+            }
         }
         const int T = __shfl_sync(0xffffffffu, incl, 31);
         if (lane == 0) pre_s[2 * nrows] = T;
@@ -385,34 +430,46 @@ __device__ void phase_nbl_cells(const SimArgs &a) {
                 pi[p] = p < gn ? pos[g0 + p] : make_float4(0.f, 0.f, 0.f, 0.f);
                 cnt[p] = 0;
             }
-            for (int v0 = 0; v0 < T; v0 += 32) {
-                const int v = v0 + lane;
-                const bool valid = v < T;
-                int j = 0;
-                float4 pj = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (valid) {
-                    // last segment whose prefix <= v
-                    int lo = 0, hi = nseg - 1;
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (pre_s[mid] <= v)
-                            lo = mid;
-                        else
-                            hi = mid - 1;
-                    }
-                    j = lo_s[lo] + (v - pre_s[lo]);
-                    pj = pos[j];
+            // each lane walks the segments forward as its candidate index grows
+            // (64 candidates per iteration: two independent position loads)
+            int seg = 0;
+            for (int v0 = 0; v0 < T; v0 += 64) {
+                const int va = v0 + lane, vb = va + 32;
+                const bool oka = va < T, okb = vb < T;
+                int ja = 0, jb = 0;
+                float4 pa = make_float4(0.f, 0.f, 0.f, 0.f), pb = pa;
+                float3 sha = make_float3(0.f, 0.f, 0.f), shb = sha;
+                if (oka) {
+                    while (seg + 1 < nseg && pre_s[seg + 1] <= va) seg++;
+                    ja = lo_s[seg] + (va - pre_s[seg]);
+                    pa = pos[ja];
+                    if (SHIFTED) sha = sh_s[seg];
+                }
+                if (okb) {
+                    while (seg + 1 < nseg && pre_s[seg + 1] <= vb) seg++;
+                    jb = lo_s[seg] + (vb - pre_s[seg]);
+                    pb = pos[jb];
+                    if (SHIFTED) shb = sh_s[seg];
                 }
 #pragma unroll
-                for (int p = 0; p < NBW; p++) {
-                    if (p >= gn) break;
-                    const bool hit = valid && j != g0 + p && dist_sq_exact<FMA>(pj, pi[p], a.Lx, a.Ly, a.Lz) < a.cps2;
-                    const unsigned m = __ballot_sync(0xffffffffu, hit);
-                    if (hit) {
-                        const int k = cnt[p] + __popc(m & ((1u << lane) - 1u));
-                        if (k < a.max_nbs) a.nbl[nbl_index(g0 + p, k, a.stride)] = j;
+                for (int half = 0; half < 2; half++) {
+                    const bool ok = half ? okb : oka;
+                    const int j = half ? jb : ja;
+                    const float4 pj = half ? pb : pa;
+                    const float3 sh = half ? shb : sha;
+#pragma unroll
+                    for (int p = 0; p < NBW; p++) {
+                        if (p >= gn) break;
+                        const float d2 = SHIFTED ? dist_sq_shifted<FMA>(pj, pi[p], sh.x, sh.y, sh.z)
+                                                 : dist_sq_exact<FMA>(pj, pi[p], Lx, Ly, Lz);
+                        const bool hit = ok && j != g0 + p && d2 < a.cps2;
+                        const unsigned m = __ballot_sync(0xffffffffu, hit);
+                        if (hit) {
+                            const int k = cnt[p] + __popc(m & ((1u << lane) - 1u));
+                            if (k < a.max_nbs) a.nbl[nbl_index(g0 + p, k, a.stride)] = j;
+                        }
+                        cnt[p] += __popc(m);
                     }
-                    cnt[p] += __popc(m);
                 }
             }
 #pragma unroll
@@ -427,8 +484,17 @@ __device__ void phase_nbl_cells(const SimArgs &a) {
     }
 }
 
+template <bool FMA>
+__device__ inline void phase_nbl_cells(const SimArgs &a) {
+    const bool shifted = a.ncx >= 7 && a.ncy >= 7 && a.ncz >= 7 && !*(volatile int *)&a.ctrl->cell_wrap;
+    if (shifted)
+        phase_nbl_cells_t<FMA, true>(a);
+    else
+        phase_nbl_cells_t<FMA, false>(a);
+}
+
 // Move the reordered state into place, record r_ref, clear the cell counters.
-__device__ void phase_finish_cells(const SimArgs &a, int cur) {
+__device__ inline void phase_finish_cells(const SimArgs &a, int cur) {
     float4 *pos = cur_pos(a, cur);
     const size_t n = a.n;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
@@ -447,6 +513,7 @@ __device__ void phase_finish_cells(const SimArgs &a, int cur) {
 __device__ __forceinline__ void rebuild_done(DevCtrl *c) {
     c->rebuild = 0;
     c->nrebuild += 1;
+    c->cell_wrap = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -469,10 +536,41 @@ __device__ __forceinline__ int conf_save_index(int step) {
     return 32 - __clz(step);
 }
 
+// Pair parameters a particle of type ti needs for its neighbours.  NT is the
+// number of particle types when it is 1 or 2: the five force parameters of
+// each neighbour type (c, cs12, cs6, sc, cut^2) sit in registers and a
+// neighbour's type selects them; NT = 0 reads a general table in shared
+// memory.  Energy and virial terms (saved steps only) always come from the
+// shared-memory row.
+template <int NT>
+struct PairRow {
+    const PairEntry *row;
+    float c0, a0, b0, s0, k0, c1, a1, b1, s1, k1;
+    __device__ __forceinline__ PairRow(const PairEntry *tab, int nt, int ti) : row(tab + ti * nt) {
+        if (NT >= 1) {
+            c0 = row[0].c, a0 = row[0].cs12, b0 = row[0].cs6, s0 = row[0].sc, k0 = row[0].cut2;
+        }
+        if (NT == 2) {
+            c1 = row[1].c, a1 = row[1].cs12, b1 = row[1].cs6, s1 = row[1].sc, k1 = row[1].cut2;
+        }
+    }
+    __device__ __forceinline__ void force(int tj, float &c, float &cs12, float &cs6, float &sc, float &cut2) const {
+        if (NT == 1) {
+            c = c0, cs12 = a0, cs6 = b0, sc = s0, cut2 = k0;
+        } else if (NT == 2) {
+            const bool t = tj != 0;
+            c = t ? c1 : c0, cs12 = t ? a1 : a0, cs6 = t ? b1 : b0, sc = t ? s1 : s0, cut2 = t ? k1 : k0;
+        } else {
+            const PairEntry &e = row[tj];
+            c = e.c, cs12 = e.cs12, cs6 = e.cs6, sc = e.sc, cut2 = e.cut2;
+        }
+    }
+};
+
 // Minimum image for list pairs (|d| < L): d - L*rint(d/L) equals the
 // reference's 2d-vs-L selection for every pair closer than L/2.
-template <bool REC, int CUT>
-__device__ __forceinline__ void pair_force(const PairEntry &e, float4 pi, float4 pj, bool valid, float Lx, float Ly,
+template <bool REC, int NT>
+__device__ __forceinline__ void pair_force(const PairRow<NT> &pr, float4 pi, float4 pj, bool valid, float Lx, float Ly,
                                            float Lz, float ilx, float ily, float ilz, float &fx, float &fy, float &fz,
                                            float &u, float &w, float &l) {
     float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
@@ -480,16 +578,20 @@ __device__ __forceinline__ void pair_force(const PairEntry &e, float4 pi, float4
     dy -= Ly * rintf(dy * ily);
     dz -= Lz * rintf(dz * ilz);
     const float d2 = dx * dx + dy * dy + dz * dz;
-    if (valid && d2 < e.cut2) {
+    const int tj = NT == 1 ? 0 : ptype_of(pj);
+    float c, cs12, cs6, sc, cut2;
+    pr.force(tj, c, cs12, cs6, sc, cut2);
+    if (valid && d2 < cut2) {
         const float inv2 = __fdividef(1.0f, d2);
-        const float x2 = e.c * inv2;
+        const float x2 = c * inv2;
         const float x6 = x2 * x2 * x2;
         const float x12 = x6 * x6;
-        const float s = (e.cs12 * x12 + e.cs6 * x6) * inv2 - e.sc;
+        const float s = (cs12 * x12 + cs6 * x6) * inv2 - sc;
         fx -= dx * s;
         fy -= dy * s;
         fz -= dz * s;
         if (REC) {
+            const PairEntry &e = pr.row[tj];
             const float r = sqrtf(d2);
             const float uu = e.cu12 * x12 + e.cu6 * x6 - e.uc + e.sccut * (r - e.cut);
             u += 0.5f * uu;
@@ -502,14 +604,13 @@ __device__ __forceinline__ void pair_force(const PairEntry &e, float4 pi, float4
 // Neighbours of particle i handled by lane `sub` of TP: chunks of four
 // indices (one int4 load), four independent position gathers per chunk.
 // pair_potential.py:223-231 with the full-list calculator :164-178.
-template <int TP, bool NT1, bool REC, bool NC>
+template <int TP, int NT, bool REC, bool NC>
 __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *pos, const PairEntry *tab, int nt,
                                                int i, int sub, float4 pi, float &fx, float &fy, float &fz, float &u,
                                                float &w, float &l) {
-    const int ti = NT1 ? 0 : ptype_of(pi);
+    const PairRow<NT> pr(tab, nt, NT == 1 ? 0 : ptype_of(pi));
     const int cnt = min(a.nbc[i], a.max_nbs);
     const int nch = (cnt + 3) >> 2;
-    const PairEntry *trow = tab + ti * nt;
     const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
     const float ilx = 1.0f / Lx, ily = 1.0f / Ly, ilz = 1.0f / Lz;
     const int4 *base = reinterpret_cast<const int4 *>(a.nbl) + i;
@@ -523,14 +624,10 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
         const float4 p1 = load<NC>(pos + j1);
         const float4 p2 = load<NC>(pos + j2);
         const float4 p3 = load<NC>(pos + j3);
-        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p0)], pi, p0, true, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
-                           w, l);
-        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p1)], pi, p1, v1, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
-                           w, l);
-        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p2)], pi, p2, v2, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
-                           w, l);
-        pair_force<REC, 0>(NT1 ? tab[0] : trow[ptype_of(p3)], pi, p3, v3, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u,
-                           w, l);
+        pair_force<REC, NT>(pr, pi, p0, true, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
+        pair_force<REC, NT>(pr, pi, p1, v1, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
+        pair_force<REC, NT>(pr, pi, p2, v2, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
+        pair_force<REC, NT>(pr, pi, p3, v3, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
     }
 }
 
@@ -538,8 +635,8 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
 // only (MODE_EVAL).  Each block accumulates float64 partial sums over all the
 // particles it handles and writes them to partials[blockIdx.x].  Sets the
 // rebuild flag when a particle has moved more than skin/2 since the build.
-template <int TP, bool NT1, int INTEG, int MODE, bool NC, bool PERSIST>
-__device__ void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red) {
+template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
+__device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red) {
     DevCtrl *ctrl = a.ctrl;
     const float4 *pos = cur_pos(a, cur);
     float4 *pos_next = cur_pos(a, cur ^ 1);
@@ -570,9 +667,9 @@ __device__ void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int c
         if (active) {
             pi = pos[i];
             if (rec)
-                neighbour_loop<TP, NT1, true, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
+                neighbour_loop<TP, NT, true, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
             else
-                neighbour_loop<TP, NT1, false, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
+                neighbour_loop<TP, NT, false, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
         }
         if (TP > 1) {
 #pragma unroll
@@ -713,7 +810,7 @@ __device__ void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int c
 // bookkeeping of a finished step (NVT.py:226-237, scalar_saver.py:274-288,
 // momentum_reset.py:379-393).  Run by one whole block.
 template <int MODE>
-__device__ void finalize_step(const SimArgs &a, int step, int nblocks, double *s_red) {
+__device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, double *s_red) {
     DevCtrl *ctrl = a.ctrl;
     const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
     const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;

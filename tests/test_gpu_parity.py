@@ -88,6 +88,28 @@ def test_lists_vs_oracle_larger(oracle, n, nblist):
     assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
 
 
+@pytest.mark.parametrize("n,face", [(1372, False), (1372, True), (600, False), (900, True), (20000, True)])
+def test_cell_build_paths_vs_oracle(oracle, n, face):
+    """Both build paths: >= 7 cells per dimension uses per-range periodic
+    shifts, smaller grids (and a particle exactly on the +L/2 face, which the
+    reference's modulo bins into cell 0) use the full minimum-image test."""
+    conf = workloads.ka_configuration(n, seed=11, jitter=0.25)
+    r = conf["r"].copy()
+    L = conf.simbox.lengths
+    if face:
+        r[3, 0] = np.float32(L[0]) / np.float32(2.0)
+        r[17, 1] = -np.float32(L[1]) / np.float32(2.0)
+        r[29, 2] = np.float32(L[2]) / np.float32(2.0)
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    sim = make_sim(r, L, conf.ptype, table, nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.eval_forces()
+    got = sim.nblist(300)
+    ref, _ = oracle.nblist_nsq(r, L, float(np.float32(2.5) + np.float32(0.3)), 300, fma=1)
+    c1, f1 = sorted_rows(got)
+    c2, f2 = sorted_rows(ref)
+    assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
+
+
 def run_api_trajectory(d):
     """Golden trajectory through the public API (Simulation + runtime actions)."""
     n = len(d["r0"])
