@@ -160,13 +160,18 @@ def ncu_traffic_per_atom_step():
 
 def trace_summary(tags, ns):
     """Per-phase times from the persistent kernel's barrier trace (tags:
-    1 step, 2 evaluation, 3 rebuild phase, 4 rebuild done, 5 start)."""
-    step_us, rebuild_us, phase_us = [], [], []
+    1 step, 2 evaluation, 3 rebuild phase, 4 rebuild done, 5 start, 6 end of
+    block 0's step phase)."""
+    step_us, rebuild_us, phase_us, sphase_us, bar_us = [], [], [], [], []
     start = None
     for k in range(1, len(tags)):
         dt = (ns[k] - ns[k - 1]) / 1e3
-        if tags[k] == 1 and tags[k - 1] in (1, 4):
-            step_us.append(dt)
+        if tags[k] == 6 and k >= 1 and tags[k - 1] in (1, 4, 5):
+            sphase_us.append(dt)
+        if tags[k] == 1 and tags[k - 1] == 6:
+            bar_us.append(dt)
+            if k >= 2 and tags[k - 2] in (1, 4):
+                step_us.append((ns[k] - ns[k - 2]) / 1e3)
         if tags[k] == 3 and tags[k - 1] in (1, 5) and start is None:
             start = ns[k - 1]
         if tags[k] in (3, 4):
@@ -176,6 +181,7 @@ def trace_summary(tags, ns):
             start = None
     med = lambda x: float(np.median(x)) if x else None
     return {"entries": int(len(tags)), "steps": len(step_us), "step_us_median": med(step_us),
+            "step_phase_us_median": med(sphase_us), "step_barrier_us_median": med(bar_us),
             "step_us_mean": float(np.mean(step_us)) if step_us else None, "rebuilds": len(rebuild_us),
             "rebuild_us_median": med(rebuild_us),
             "rebuild_phase_us": [round(x, 1) for x in phase_us[:5]]}

@@ -65,8 +65,9 @@ struct DevCtrl {
     float sumK;        // last kinetic-energy sum (float copy, NVT.thermostat_state[1] analogue)
     double time_zero;  // simulated time at the start of the timeblock
     double evalU, evalW;  // sums of the last force-only evaluation
-    unsigned bar_count;   // grid barrier of the persistent kernel
+    unsigned bar_count;   // grid barrier of the persistent kernel: top-level arrivals
     unsigned bar_gen;
+    unsigned bar_group[64];  // arrivals per group of 16 blocks (grids up to 1024 blocks)
     int abort;            // set when a barrier wait timed out
     unsigned long long *trace;  // optional phase trace: (tag << 56) | globaltimer ns
     int trace_cap;
@@ -75,7 +76,7 @@ struct DevCtrl {
 
 // Phase trace (block 0, thread 0 of the persistent kernel): one entry per
 // barrier with a tag naming the phase that just finished.
-enum TraceTag { TR_STEP = 1, TR_EVAL = 2, TR_REBUILD_PHASE = 3, TR_REBUILD_DONE = 4, TR_START = 5 };
+enum TraceTag { TR_STEP = 1, TR_EVAL = 2, TR_REBUILD_PHASE = 3, TR_REBUILD_DONE = 4, TR_START = 5, TR_STEP_PHASE = 6 };
 
 __device__ __forceinline__ void trace_mark(DevCtrl *c, int tag) {
     if (c->trace && blockIdx.x == 0 && threadIdx.x == 0) {

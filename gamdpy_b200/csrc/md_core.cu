@@ -186,6 +186,7 @@ __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
     ctrl->step = 0;
     ctrl->time_zero = time_zero;
     ctrl->bar_count = 0;
+    for (int g = 0; g < 64; g++) ctrl->bar_group[g] = 0;
     ctrl->abort = 0;
     ctrl->ticket = 0;
     if (ctrl->rebuild_next) {
@@ -473,7 +474,7 @@ static int run_grid(gdb_sim *h, const void *fn, int *grid) {
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GDB_BLOCK, 0));
     if (occ < 1) return set_err(h, GDB_ERR_CUDA, "persistent kernel cannot be resident");
     const int needed = grid_for((long long)h->n * h->tp);
-    *grid = std::min(needed, occ * h->num_sms);
+    *grid = std::min(std::min(needed, occ * h->num_sms), 64 * BAR_GROUP);
     return GDB_OK;
 }
 

@@ -101,6 +101,7 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArg
         bool ok;
         if (s < nsteps) {
             phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, tab.nt, cur, step, s_red);
+            trace_mark(ctrl, TR_STEP_PHASE);
             ok = grid_barrier(ctrl, [&] {
                 finalize_step<MODE_STEP>(a, step, gridDim.x, s_red);
                 if (threadIdx.x == 0 && ctrl->rebuild_next) {

@@ -77,43 +77,68 @@ __device__ __forceinline__ T load(const T *p) {
 // ---------------------------------------------------------------------------
 constexpr long long BARRIER_TIMEOUT_CYCLES = 2000000000LL;
 
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned atom_add_acq_rel_gpu(unsigned *p, unsigned v) {
+    unsigned old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Arrival is hierarchical: an acq_rel add on the counter of the block's group
+// of 16 (after a CTA barrier, so the block's writes are ordered before it);
+// the last of a group adds to the top counter, and the last there has seen
+// every block's writes.  It runs `last`, resets the counters and publishes the
+// next generation with a release store; waiters poll it with acquire loads.
+constexpr int BAR_GROUP = 16;
+
 template <typename F>
 __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
     __shared__ int s_last, s_ok;
     __syncthreads();
     if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned gen = *(volatile unsigned *)&c->bar_gen;
-        const unsigned t = atomicAdd(&c->bar_count, 1u);
-        s_last = (t == gridDim.x - 1);
+        const unsigned gen = ld_acquire_gpu(&c->bar_gen);
+        const unsigned grp = blockIdx.x / BAR_GROUP;
+        const unsigned gsize = min((unsigned)BAR_GROUP, gridDim.x - grp * BAR_GROUP);
+        const unsigned ngroups = (gridDim.x + BAR_GROUP - 1) / BAR_GROUP;
+        bool top = false;
+        if (atom_add_acq_rel_gpu(&c->bar_group[grp], 1u) == gsize - 1) {
+            c->bar_group[grp] = 0;  // no block of this group arrives again before the release
+            top = atom_add_acq_rel_gpu(&c->bar_count, 1u) == ngroups - 1;
+        }
+        s_last = top;
         s_ok = 1;
         if (!s_last) {
             const long long t0 = clock64();
-            while (*(volatile unsigned *)&c->bar_gen == gen) {
+            int polls = 0;
+            while (ld_acquire_gpu(&c->bar_gen) == gen) {
                 if (*(volatile int *)&c->abort) {
                     s_ok = 0;
                     break;
                 }
-                if (clock64() - t0 > BARRIER_TIMEOUT_CYCLES) {
+                if ((++polls & 63) == 0 && clock64() - t0 > BARRIER_TIMEOUT_CYCLES) {
                     atomicOr(&c->status, GDB_STATUS_BARRIER_TIMEOUT);
                     c->abort = 1;
                     s_ok = 0;
                     break;
                 }
-                __nanosleep(64);
+                if (polls > 64) __nanosleep(32);
             }
-            __threadfence();
         }
     }
     __syncthreads();
     if (s_last) {
-        __threadfence();
         last();
         __syncthreads();
         if (threadIdx.x == 0) {
             c->bar_count = 0;
-            __threadfence();
-            atomicAdd(&c->bar_gen, 1u);
+            st_release_gpu(&c->bar_gen, *(volatile unsigned *)&c->bar_gen + 1u);
         }
         __syncthreads();
     }
@@ -664,6 +689,13 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
         const bool active = i < a.n;
         float fx = 0.f, fy = 0.f, fz = 0.f, u = 0.f, w = 0.f, l = 0.f;
         float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+        // the integrating lane's own state, loaded before the neighbour loop so
+        // its latency overlaps the gathers
+        float4 v = make_float4(0.f, 0.f, 0.f, 1.f), rr = v;
+        if (active && sub == 0) {
+            v = a.vel[i];
+            if (MODE == MODE_STEP) rr = a.rref[i];
+        }
         if (active) {
             pi = pos[i];
             if (rec)
@@ -701,7 +733,6 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
                 fr[3 * uidx + 2] = (float)im.z;
             }
         }
-        float4 v = a.vel[i];
         if (shift_pending) {
             v.x -= shx;
             v.y -= shy;
@@ -780,7 +811,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
         a.pscal[3 * n + i] = kin;
         a.pscal[4 * n + i] = fsq;
         // skin check for the next step (nblist.py:57-86)
-        moved |= dist_sq_exact<false>(pn, a.rref[i], a.Lx, a.Ly, a.Lz) > a.skin2q;
+        moved |= dist_sq_exact<false>(pn, rr, a.Lx, a.Ly, a.Lz) > a.skin2q;
         red[0] += kin;
         if (reset) {
             red[5] += (double)m * vv[0];
