@@ -48,6 +48,11 @@ def parse():
                    help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
     p.add_argument("--tp", type=int, default=0, help="lanes per particle (0 = library default)")
     p.add_argument("--trace", action="store_true", help="with --profile: phase trace of the persistent kernel")
+    p.add_argument("--workload", default="ka", choices=["ka", "batch"],
+                   help="ka: one KA system of --n particles; batch: --replicas KA replicas of uneven N, "
+                        "density and temperature advanced together, against the same replicas run one by one")
+    p.add_argument("--replicas", type=int, default=128)
+    p.add_argument("--autotune", action="store_true", help="batch: pick particles per CTA by timing")
     return p.parse_args()
 
 
@@ -176,7 +181,9 @@ def trace_summary(tags, ns):
             start = ns[k - 1]
         if tags[k] in (3, 4):
             phase_us.append(dt)
-        if tags[k] == 4 and start is not None:
+        if tags[k] == 4:
+            if start is None:  # builds without intermediate marks
+                start = ns[k - 1]
             rebuild_us.append((ns[k] - start) / 1e3)
             start = None
     med = lambda x: float(np.median(x)) if x else None
@@ -229,10 +236,99 @@ def run_reference_arm(args):
     barrier(pg)
 
 
+def run_batch(args):
+    """Batched replicas: ``--replicas`` KA systems (N log-uniform 256-32768,
+    rho in [1.1, 1.3], T in [0.4, 1.0], NVT dt 0.005, cells skin 0.3) advanced
+    together by SimulationBatch, against the same systems advanced one after
+    another through Simulation (each its own launches)."""
+    rank, world, local, pg = dist_setup(args)
+    import gamdpy_b200 as gp
+    from gamdpy_b200 import workloads
+
+    points = workloads.ka_replica_sweep(args.replicas, seed=2024 + rank)
+    block = min(args.block, max(1, args.steps))
+    nblocks = max(1, args.steps // block)
+    steps = nblocks * block
+    plan = {"pb": 64, "tp": 1, "lanes": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
+            "nblist": "linked lists"}
+    sims = []
+    for k, (n, rho, temp) in enumerate(points):
+        conf = workloads.ka_configuration(n, rho=rho, temperature=temp, seed=k)
+        integ = gp.integrators.NVT(temperature=temp, tau=0.2, dt=0.005)
+        sims.append(gp.Simulation(conf, workloads.ka_pair_potential(max_num_nbs=300), integ,
+                                  [gp.ScalarSaver(max(1, block // 8))], num_timeblocks=nblocks,
+                                  steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local))
+    total_n = sum(p[0] for p in points)
+    batch = gp.SimulationBatch(sims)
+    tuned = batch.autotune(steps=min(block, 200)) if args.autotune else batch.particles_per_cta
+    # warm-up of both paths
+    for s in sims:
+        s.configuration.copy_to_device()
+        s._sim.run(0.0, max(3, min(args.warmup, block)))
+    batch.integrate_self(0.0, max(3, min(args.warmup, block)))
+    barrier(pg)
+    # sequential: every replica's timeblocks, one replica after another
+    for s in sims:
+        s.configuration.copy_to_device()
+    ms_seq = 0.0
+    for s in sims:
+        for b in range(nblocks):
+            ms_seq += s._sim.run(float(b * block * 0.005), block)
+    # batched: one launch per timeblock for all replicas
+    for s in sims:
+        s.configuration.copy_to_device()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms_bat = 0.0
+    for b in range(nblocks):
+        ms_bat += batch.integrate_self(float(b * block * 0.005), block)
+    clock_info = clocks.stop()
+    paths = batch.paths()
+    t_bat = allreduce_max(pg, ms_bat / 1e3, local)
+    t_seq = allreduce_max(pg, ms_seq / 1e3, local)
+    # end to end through the public API: SimulationBatch.run_timeblocks
+    # (upload once, per timeblock the state of every replica back to the host)
+    e2e_blocks = max(1, min(nblocks, 2))
+    t0 = time.perf_counter()
+    for _ in batch.run_timeblocks(e2e_blocks):
+        pass
+    e2e_s = allreduce_max(pg, time.perf_counter() - t0, local)
+    h2d = total_n * (12 + 12 + 4 + 4 + 12)
+    d2h = total_n * (12 + 12 + 12 + 12 + 4 * 5)
+    mats = total_n * steps * world / t_bat / 1e6
+    line = {
+        "metric": "MATS batched KA replicas (N 256-32768, rho 1.1-1.3, T 0.4-1.0), 1 B200", "value": mats,
+        "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": max(3, min(args.warmup, block)),
+        "ms_per_step": t_bat * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded KA lattices)",
+        "config": {"workload": f"{args.replicas} KA-LJ NVT replicas, cells skin=0.3, total N={total_n}",
+                   "replicas": args.replicas, "total_n": total_n, "timeblock_steps": block,
+                   "particles_per_cta": tuned, "cluster_systems": int(sum(1 for p in paths if p == 2)),
+                   "grid_systems": int(sum(1 for p in paths if p != 2)),
+                   "l2": "working set of all replicas > 126 MB L2, no flush"},
+        "sequential": {"value": total_n * steps * world / t_seq / 1e6, "unit": UNIT,
+                       "ms_per_step": t_seq * 1e3 / steps,
+                       "note": "the same replicas, one Simulation after another (device time summed)"},
+        "speedup_vs_sequential": t_seq / t_bat,
+        "e2e": {"value": total_n * e2e_blocks * block * world / e2e_s / 1e6, "unit": UNIT,
+                "h2d_bytes_per_step": h2d / (e2e_blocks * block), "d2h_bytes_per_step": d2h / (e2e_blocks * block),
+                "timeblock_steps": block},
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.workload == "batch":
+        run_batch(args)
         return
     rank, world, local, pg = dist_setup(args)
     import gamdpy_b200 as gp

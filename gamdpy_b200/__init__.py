@@ -19,6 +19,7 @@ from .potential_functions import (LJ_12_6, LJ_12_6_sigma_epsilon, apply_shifted_
                                   apply_shifted_potential_cutoff)
 from .runtime_actions import ConfigurationSaver, MomentumReset, RuntimeAction, ScalarSaver
 from .simulation import Simulation, get_default_compute_plan, get_default_sim
+from .batch import SimulationBatch
 from .simulation_boxes import Orthorhombic
 from .tools import Evaluator
 

@@ -73,12 +73,17 @@ SIGNATURES = {
     "gdb_get_nbflag": ([_P, _P], _i),
     "gdb_status_word": ([_P], ctypes.c_uint32),
     "gdb_clear_status": ([_P], _i),
+    "gdb_get_last_path": ([_P], _i),
     "gdb_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
     "gdb_rdf_update": ([_P, _i, _d, _P], _i),
     "gdb_sq_update": ([_P, _i, _P, _P, _P, _P], _i),
     "gdb_rdf_compute": ([_i, _P, _P, _P, _i, _i, _d, _P], _i),
     "gdb_sq_compute": ([_i, _P, _P, _P, _i, _P, _P, _P], _i),
     "gdb_sq_compute_noalloc": ([_i, _P, _P, _P, _i, _P, _i, _P, _P, _P], _i),
+    "gdb_batch_create": ([_P, _i, _i, _P], _i),
+    "gdb_batch_run": ([_P, _d, _i, _P], _i),
+    "gdb_batch_destroy": ([_P], _i),
+    "gdb_batch_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
 }
 
 _lib = None
@@ -275,6 +280,10 @@ class Sim:
         self.call("gdb_get_nbflag", ptr(out))
         return out
 
+    def last_path(self):
+        """0 graph launches, 1 persistent grid kernel, 2 thread-block cluster."""
+        return int(lib().gdb_get_last_path(self.h))
+
     def status(self):
         return int(lib().gdb_status_word(self.h))
 
@@ -316,3 +325,34 @@ def sq_compute(r, box, n_vectors, ff=None):
     check(lib().gdb_sq_compute(int(n), ptr(r), ptr(ffa), ptr(L), int(len(nv)), ptr(nv), ptr(re), ptr(im)), None,
           "gdb_sq_compute")
     return re + 1j * im
+
+
+class BatchHandle:
+    """Owner of one gdb_batch handle: several Sim handles advanced together."""
+
+    def __init__(self, sims, particles_per_cta=0):
+        self.sims = list(sims)
+        arr = (ctypes.c_void_p * len(self.sims))(*[s.h.value for s in self.sims])
+        self.h = ctypes.c_void_p()
+        rc = lib().gdb_batch_create(arr, len(self.sims), int(particles_per_cta), ctypes.byref(self.h))
+        if rc != GDB_OK:
+            buf = ctypes.create_string_buffer(512)
+            lib().gdb_batch_get_last_error(None, buf, 512)
+            raise GdbError(rc, f"gdb_batch_create: {buf.value.decode(errors='replace')}")
+
+    def run(self, time_zero, steps):
+        ms = ctypes.c_float(0.0)
+        rc = lib().gdb_batch_run(self.h, float(time_zero), int(steps), ctypes.byref(ms))
+        if rc != GDB_OK:
+            buf = ctypes.create_string_buffer(512)
+            lib().gdb_batch_get_last_error(self.h, buf, 512)
+            raise GdbError(rc, f"gdb_batch_run: {buf.value.decode(errors='replace')}")
+        return ms.value
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().gdb_batch_destroy(self.h)
+                self.h = ctypes.c_void_p()
+        except Exception:
+            pass

@@ -12,7 +12,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgamdb200.so")
-SOURCES = ["md_core.cu", "md_inst_nt1.cu", "md_inst_nt2.cu", "md_inst_ntg.cu", "analysis.cu"]
+SOURCES = ["md_core.cu", "md_inst_nt1.cu", "md_inst_nt2.cu", "md_inst_ntg.cu", "md_cluster.cu", "analysis.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
@@ -28,7 +28,7 @@ def _stale(target, deps):
 
 def build(verbose=False, force=False):
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [
-        os.path.join(CSRC, h) for h in ("gdb_internal.cuh", "md_phases.cuh", "md_kernels.cuh")
+        os.path.join(CSRC, h) for h in ("gdb_internal.cuh", "md_phases.cuh", "md_kernels.cuh", "md_cluster.cuh")
     ] + [os.path.join(HERE, "..", "include", "gamdb200.h")]
     if not force and not _stale(LIB, deps):
         return LIB

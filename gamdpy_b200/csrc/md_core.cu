@@ -37,6 +37,8 @@
 #include "../../include/gamdb200.h"
 #include "gdb_internal.cuh"
 #include "md_kernels.cuh"
+#include "md_cluster.cuh"
+
 
 using namespace gdb;
 
@@ -96,6 +98,10 @@ struct gdb_sim {
     int cur = 0;
     int num_sms = 148;
     bool persistent = true;
+    bool cluster_ok = true;  // small systems run resident in one thread-block cluster
+    int last_path = -1;      // 0 graph, 1 persistent grid, 2 cluster
+    int grid_cap = 0;        // upper bound on the persistent grid (0: the whole GPU)
+    ClusterJob *d_job = nullptr, *h_job = nullptr;
     bool uploaded = false;
     // graphs: [parity] for chunks of GRAPH_STEPS steps
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
@@ -475,6 +481,7 @@ static int run_grid(gdb_sim *h, const void *fn, int *grid) {
     if (occ < 1) return set_err(h, GDB_ERR_CUDA, "persistent kernel cannot be resident");
     const int needed = grid_for((long long)h->n * h->tp);
     *grid = std::min(std::min(needed, occ * h->num_sms), 64 * BAR_GROUP);
+    if (h->grid_cap > 0) *grid = std::min(*grid, h->grid_cap);
     return GDB_OK;
 }
 
@@ -525,6 +532,51 @@ static int status_to_rc(gdb_sim *h) {
     return GDB_OK;
 }
 
+// One timeblock resident in a thread-block cluster (md_cluster.cu).  Returns
+// GDB_ERR_UNSUPPORTED (and disables the path for this handle) when the
+// cluster launch is not possible on this device.
+static int run_cluster(gdb_sim *h, int steps) {
+    int C, tp;
+    cluster_shape(h->n, 0, &C, &tp);
+    SimArgs a = make_args(h);
+    // the cell grid of the global cell build, whatever list kind was chosen
+    // (both kinds give the same sets)
+    const float min_cell = (h->max_cut + h->skin) / 2.0f;
+    int nc[3];
+    for (int k = 0; k < 3; k++) {
+        nc[k] = (int)(h->box[k] / min_cell);
+        if (nc[k] < 1) nc[k] = 1;
+    }
+    a.ncx = nc[0];
+    a.ncy = nc[1];
+    a.ncz = nc[2];
+    const int ncell = nc[0] * nc[1] * nc[2];
+    int cap;
+    size_t smem;
+    if (!cluster_plan(h->n, C, ncell, h->max_nbs, &cap, &smem)) {
+        h->cluster_ok = false;
+        return GDB_ERR_UNSUPPORTED;
+    }
+    if (!h->d_job) {
+        CK(cudaMalloc(&h->d_job, sizeof(ClusterJob)));
+        CK(cudaMallocHost(&h->h_job, sizeof(ClusterJob)));
+    }
+    CK(cudaStreamSynchronize(h->st));  // the pinned job buffer is rewritten below
+    h->h_job->a = a;
+    h->h_job->tab = h->table;
+    h->h_job->cur = h->cur;
+    h->h_job->step0 = 0;
+    h->h_job->cap = cap;
+    CK(cudaMemcpyAsync(h->d_job, h->h_job, sizeof(ClusterJob), cudaMemcpyHostToDevice, h->st));
+    cudaError_t e = launch_clusters(h->d_job, 1, C, tp, h->ntypes, h->integ, smem, steps, 1, h->st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        h->cluster_ok = false;
+        return set_err(h, GDB_ERR_UNSUPPORTED, "cluster launch not possible: %s", cudaGetErrorString(e));
+    }
+    return GDB_OK;
+}
+
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
@@ -555,6 +607,8 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (fm && fm[0] == '0') h->fma = 0;
     const char *ps = getenv("GDB_PERSISTENT");
     if (ps && ps[0] == '0') h->persistent = false;
+    const char *cs = getenv("GDB_CLUSTER");
+    if (cs && cs[0] == '0') h->cluster_ok = false;
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
@@ -614,6 +668,8 @@ int gdb_sim_destroy(gdb_sim *h) {
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
+    if (h->h_job) cudaFreeHost(h->h_job);
+    if (h->d_job) cudaFree(h->d_job);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
     if (h->st) cudaStreamDestroy(h->st);
@@ -890,9 +946,36 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
     CK(cudaEventRecord(h->ev0, h->st));
     k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
     CKL();
+    if (h->cluster_ok && h->n <= CL_MAX_N) {
+        rc = run_cluster(h, steps);
+        if (rc == GDB_OK) {
+            CK(cudaEventRecord(h->ev1, h->st));
+            if ((rc = read_ctrl(h))) return rc;
+            if (!(h->h_ctrl->status & GDB_STATUS_CLUSTER_CAPACITY)) {
+                h->cur ^= (steps & 1);
+                h->last_path = 2;
+                if (ms) CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
+                return status_to_rc(h);
+            }
+            // a list outgrew shared memory: nothing was written back; rerun
+            // this timeblock (and the following ones) on the global path
+            h->cluster_ok = false;
+            const unsigned clear = h->h_ctrl->status & ~GDB_STATUS_CLUSTER_CAPACITY;
+            CK(cudaMemcpyAsync(&h->ctrl->status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice, h->st));
+            int one = 1;
+            CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
+            CK(cudaEventRecord(h->ev0, h->st));
+            k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
+            CKL();
+        } else if (rc != GDB_ERR_UNSUPPORTED) {
+            return rc;
+        }
+    }
     if (h->persistent) {
         if ((rc = launch_run(h, steps, 1))) return rc;
+        h->last_path = 1;
     } else {
+        h->last_path = 0;
         const int G = 16;
         int s = 0;
         if (h->use_graphs && steps >= G) {
@@ -1051,6 +1134,252 @@ int gdb_clear_status(gdb_sim *h) {
     CK(cudaStreamSynchronize(h->st));
     return GDB_OK;
 }
+
+int gdb_get_last_path(gdb_sim *h) { return h ? h->last_path : -1; }
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// batched replicas: many independent systems advanced together
+// ---------------------------------------------------------------------------
+struct gdb_batch {
+    struct Group {
+        int C = 0, tp = 0;
+        size_t smem = 0;
+        std::vector<int> idx, cap;
+        ClusterJob *d_jobs = nullptr, *h_jobs = nullptr;
+        cudaStream_t st = nullptr;
+        cudaEvent_t done = nullptr;
+    };
+    std::vector<gdb_sim *> sims;
+    std::vector<Group> groups;
+    std::vector<int> big;  // systems too large for a cluster: persistent grid kernel, capped grid
+    int dev = 0, ntypes = 1, integ = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    char err[512] = "";
+};
+
+static int bset(gdb_batch *b, int code, const char *fmt, ...) {
+    char *dst = b ? b->err : g_lib_error;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(dst, 512, fmt, ap);
+    va_end(ap);
+    return code;
+}
+
+#define BCK(call)                                                                                     \
+    do {                                                                                              \
+        cudaError_t e_ = (call);                                                                      \
+        if (e_ != cudaSuccess)                                                                        \
+            return bset(b, GDB_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, \
+                        __LINE__);                                                                    \
+    } while (0)
+
+static void batch_free(gdb_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->dev);
+    if (b->st) cudaStreamSynchronize(b->st);
+    for (auto &g : b->groups) {
+        if (g.st) cudaStreamSynchronize(g.st);
+        if (g.d_jobs) cudaFree(g.d_jobs);
+        if (g.h_jobs) cudaFreeHost(g.h_jobs);
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.st) cudaStreamDestroy(g.st);
+    }
+    for (gdb_sim *h : b->sims) h->grid_cap = 0;
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+static void cluster_grid_of(const gdb_sim *h, int nc[3]) {
+    const float min_cell = (h->max_cut + h->skin) / 2.0f;
+    for (int k = 0; k < 3; k++) {
+        nc[k] = (int)(h->box[k] / min_cell);
+        if (nc[k] < 1) nc[k] = 1;
+    }
+}
+
+extern "C" {
+
+int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb_batch **out) {
+    gdb_batch *b = nullptr;
+    if (!sims || count < 1 || !out) return bset(b, GDB_ERR_ARG, "gdb_batch_create: bad arguments");
+    b = new gdb_batch();
+    b->sims.assign(sims, sims + count);
+    b->dev = sims[0]->dev;
+    b->ntypes = sims[0]->ntypes;
+    b->integ = sims[0]->integ;
+    for (int k = 0; k < count; k++) {
+        gdb_sim *h = sims[k];
+        if (!h || h->dev != b->dev || h->ntypes != b->ntypes || h->integ != b->integ) {
+            batch_free(b);
+            return bset(nullptr, GDB_ERR_ARG,
+                        "gdb_batch_create: every system needs the same device, type count and integrator");
+        }
+        int rc = check_ready(h);
+        if (rc) {
+            snprintf(g_lib_error, sizeof(g_lib_error), "gdb_batch_create: system %d: %.400s", k, h->err);
+            batch_free(b);
+            return rc;
+        }
+    }
+    cudaError_t e;
+    if ((e = cudaSetDevice(b->dev)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking)) ||
+        (e = cudaEventCreate(&b->ev0)) || (e = cudaEventCreate(&b->ev1))) {
+        batch_free(b);
+        return bset(nullptr, GDB_ERR_CUDA, "gdb_batch_create: %s", cudaGetErrorString(e));
+    }
+    // group the cluster-sized systems by cluster shape (one launch each)
+    for (int k = 0; k < count; k++) {
+        gdb_sim *h = sims[k];
+        int nc[3];
+        cluster_grid_of(h, nc);
+        int C, tp;
+        cluster_shape(h->n, particles_per_cta, &C, &tp);
+        int cap;
+        size_t smem;
+        if (!h->cluster_ok || h->n > CL_MAX_N || !cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &smem)) {
+            b->big.push_back(k);
+            continue;
+        }
+        gdb_batch::Group *g = nullptr;
+        for (auto &x : b->groups)
+            if (x.C == C && x.tp == tp) g = &x;
+        if (!g) {
+            b->groups.emplace_back();
+            g = &b->groups.back();
+            g->C = C;
+            g->tp = tp;
+        }
+        g->idx.push_back(k);
+        g->cap.push_back(cap);
+        g->smem = std::max(g->smem, smem);
+    }
+    for (auto &g : b->groups) {
+        const size_t bytes = g.idx.size() * sizeof(ClusterJob);
+        if ((e = cudaMalloc(&g.d_jobs, bytes)) || (e = cudaMallocHost(&g.h_jobs, bytes)) ||
+            (e = cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking)) ||
+            (e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming))) {
+            batch_free(b);
+            return bset(nullptr, GDB_ERR_CUDA, "gdb_batch_create: %s", cudaGetErrorString(e));
+        }
+    }
+    // large systems share the GPU with the clusters: cap their persistent grids
+    if (!b->big.empty()) {
+        const int share = std::max(16, 3 * 148 / (int)(b->big.size() + (b->groups.empty() ? 0 : 1)));
+        for (int k : b->big) sims[k]->grid_cap = share;
+    }
+    *out = b;
+    return GDB_OK;
+}
+
+int gdb_batch_destroy(gdb_batch *b) {
+    batch_free(b);
+    return GDB_OK;
+}
+
+int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
+    if (!b || steps < 0) return bset(b, GDB_ERR_ARG, "gdb_batch_run: bad arguments");
+    BCK(cudaSetDevice(b->dev));
+    // per-system preparation on each system's own stream
+    for (gdb_sim *h : b->sims) {
+        int rc = check_ready(h);
+        if (rc) return bset(b, rc, "gdb_batch_run: %s", h->err);
+        const int rows = h->scalar_every > 0 ? steps / h->scalar_every : 0;
+        if (rows > h->rows_cap) {
+            if (h->rows) cudaFree(h->rows);
+            h->rows = nullptr;
+            BCK(cudaMalloc(&h->rows, (size_t)rows * GDB_NUM_SCALARS * sizeof(double)));
+            h->rows_cap = rows;
+            free_graphs(h);
+        }
+        if (rows > 0) BCK(cudaMemsetAsync(h->rows, 0, (size_t)rows * GDB_NUM_SCALARS * sizeof(double), h->st));
+        if ((rc = ensure_partials(h, grid_for((long long)h->n * h->tp)))) return bset(b, rc, "%s", h->err);
+        BCK(cudaMemsetAsync(&h->ctrl->maxcount, 0, sizeof(int), h->st));
+        k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
+        BCK(cudaGetLastError());
+        BCK(cudaEventRecord(h->ev0, h->st));
+        BCK(cudaStreamWaitEvent(b->st, h->ev0, 0));
+    }
+    BCK(cudaEventRecord(b->ev0, b->st));
+    // one cluster launch per shape group
+    for (auto &g : b->groups) {
+        BCK(cudaStreamWaitEvent(g.st, b->ev0, 0));
+        BCK(cudaStreamSynchronize(g.st));  // pinned job buffer is rewritten below
+        for (size_t q = 0; q < g.idx.size(); q++) {
+            gdb_sim *h = b->sims[g.idx[q]];
+            SimArgs a = make_args(h);
+            int nc[3];
+            cluster_grid_of(h, nc);
+            a.ncx = nc[0];
+            a.ncy = nc[1];
+            a.ncz = nc[2];
+            g.h_jobs[q].a = a;
+            g.h_jobs[q].tab = h->table;
+            g.h_jobs[q].cur = h->cur;
+            g.h_jobs[q].step0 = 0;
+            g.h_jobs[q].cap = g.cap[q];
+        }
+        BCK(cudaMemcpyAsync(g.d_jobs, g.h_jobs, g.idx.size() * sizeof(ClusterJob), cudaMemcpyHostToDevice, g.st));
+        BCK(launch_clusters(g.d_jobs, (int)g.idx.size(), g.C, g.tp, b->ntypes, b->integ, g.smem, steps, 1, g.st));
+        BCK(cudaEventRecord(g.done, g.st));
+        BCK(cudaStreamWaitEvent(b->st, g.done, 0));
+    }
+    // large systems: persistent kernels on their own streams, concurrently
+    for (int k : b->big) {
+        gdb_sim *h = b->sims[k];
+        BCK(cudaStreamWaitEvent(h->st, b->ev0, 0));
+        int rc = launch_run(h, steps, 1);
+        if (rc) return bset(b, rc, "gdb_batch_run: %s", h->err);
+        h->last_path = 1;
+        BCK(cudaEventRecord(h->ev1, h->st));
+        BCK(cudaStreamWaitEvent(b->st, h->ev1, 0));
+    }
+    BCK(cudaEventRecord(b->ev1, b->st));
+    BCK(cudaEventSynchronize(b->ev1));
+    if (ms) BCK(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    for (auto &g : b->groups)
+        for (int k : g.idx) {
+            gdb_sim *h = b->sims[k];
+            h->cur ^= (steps & 1);
+            h->last_path = 2;
+        }
+    // status; a cluster whose lists outgrew shared memory reruns alone
+    int first_rc = GDB_OK;
+    for (size_t k = 0; k < b->sims.size(); k++) {
+        gdb_sim *h = b->sims[k];
+        int rc = read_ctrl(h);
+        if (rc) return bset(b, rc, "gdb_batch_run: %s", h->err);
+        if (h->h_ctrl->status & GDB_STATUS_CLUSTER_CAPACITY) {
+            h->cur ^= (steps & 1);  // nothing was written back
+            h->cluster_ok = false;
+            const unsigned clear = h->h_ctrl->status & ~GDB_STATUS_CLUSTER_CAPACITY;
+            BCK(cudaMemcpy(&h->ctrl->status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice));
+            int one = 1;
+            BCK(cudaMemcpy(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice));
+            rc = gdb_sim_run(h, time_zero, steps, nullptr);
+        } else {
+            rc = status_to_rc(h);
+        }
+        if (rc && first_rc == GDB_OK) {
+            first_rc = rc;
+            bset(b, rc, "system %d: %s", (int)k, h->err);
+        }
+    }
+    return first_rc;
+}
+
+int gdb_batch_get_last_error(gdb_batch *b, char *buf, int n) {
+    if (!buf || n < 1) return GDB_ERR_ARG;
+    snprintf(buf, (size_t)n, "%s", b ? b->err : g_lib_error);
+    return GDB_OK;
+}
+
+
 
 int gdb_get_last_error(gdb_sim *h, char *buf, int n) {
     if (!buf || n < 1) return GDB_ERR_ARG;

@@ -214,18 +214,26 @@ class Simulation:
                 ra.initialize_before_timeblock()
             ms = self.integrate_self(np.float32(block * self.steps_per_block * self.dt), self.steps_per_block)
             block_times.append(ms)
-            self.configuration.copy_to_host()
-            if isinstance(self.integrator, NVT):
-                self.integrator.sync_from_device()
-            for interaction in self.interactions:
-                interaction.check_datastructure_validity()
-            if self._scalar_saver is not None:
-                rows = self._sim.scalar_rows(self._scalar_saver.scalar_saves_per_block)
-                self._scalar_saver.update_from_rows(block, rows, self.memory, self.configuration.get_volume())
-            if self._conf_saver is not None:
-                frames = self._sim.saved_configurations(self._conf_saver.conf_per_block)
-                self._conf_saver.update_from_frames(block, frames, self.memory)
+            self._after_block(block)
             yield block
+        self._finish_blocks(block_times)
+
+    def _after_block(self, block):
+        """Host side of one finished timeblock: state back to the host, list
+        validity check, runtime-action output (Simulation.py:418-447)."""
+        self.configuration.copy_to_host()
+        if isinstance(self.integrator, NVT):
+            self.integrator.sync_from_device()
+        for interaction in self.interactions:
+            interaction.check_datastructure_validity()
+        if self._scalar_saver is not None:
+            rows = self._sim.scalar_rows(self._scalar_saver.scalar_saves_per_block)
+            self._scalar_saver.update_from_rows(block, rows, self.memory, self.configuration.get_volume())
+        if self._conf_saver is not None:
+            frames = self._sim.saved_configurations(self._conf_saver.conf_per_block)
+            self._conf_saver.update_from_frames(block, frames, self.memory)
+
+    def _finish_blocks(self, block_times):
         if self.timing:
             self.timing_numba_blocks = np.array(block_times)
             self.timing_numba = float(np.sum(block_times))

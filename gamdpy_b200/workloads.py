@@ -57,3 +57,16 @@ def lj_configuration(cells, rho, temperature, seed=0, compute_flags=None):
 def lj_pair_potential(cut=2.5, shifted_force=True, max_num_nbs=300):
     wrap = apply_shifted_force_cutoff if shifted_force else apply_shifted_potential_cutoff
     return PairPotential(wrap(LJ_12_6_sigma_epsilon), params=[1.0, 1.0, cut], max_num_nbs=max_num_nbs)
+
+
+def ka_replica_sweep(count=128, seed=0, n_min=256, n_max=32768):
+    """State points of the batched-replica workload: ``count`` KA systems with
+    N log-uniform in [n_min, n_max] (rounded to a multiple of 4, FCC sites
+    trimmed to N), density uniform in [1.1, 1.3] and temperature uniform in
+    [0.4, 1.0], all drawn from ``seed``.  Returns a list of (N, rho, T)."""
+    rng = np.random.default_rng(seed)
+    ns = np.exp(rng.uniform(np.log(n_min), np.log(n_max), count))
+    ns = np.clip((np.round(ns / 4) * 4).astype(int), n_min, n_max)
+    rhos = rng.uniform(1.1, 1.3, count)
+    temps = rng.uniform(0.4, 1.0, count)
+    return [(int(n), float(r), float(t)) for n, r, t in zip(ns, rhos, temps)]

@@ -43,6 +43,7 @@ extern "C" {
 #define GDB_STATUS_BARRIER_TIMEOUT 0x2u
 #define GDB_STATUS_NAN 0x4u
 #define GDB_STATUS_BAD_ARG 0x8u
+#define GDB_STATUS_CLUSTER_CAPACITY 0x10u /* a list outgrew the cluster path's shared memory (rerun on the global path) */
 
 /* potentials: gamdpy/interactions/potential_functions/ */
 #define GDB_POT_LJ_SIGMA_EPSILON 0 /* LJ_12_6_sigma_epsilon.py:6-36, params (sigma, epsilon, cut) */
@@ -179,6 +180,11 @@ int gdb_get_nblist(gdb_sim *h, int32_t *out, int max_nbs);
  * else 0, number of rebuilds}. */
 int gdb_get_nbflag(gdb_sim *h, int32_t out[3]);
 
+/* Which implementation ran the last gdb_sim_run: 0 CUDA-graph launch
+ * sequence, 1 persistent cooperative kernel, 2 thread-block cluster
+ * (N <= 4096), -1 none yet.  Diagnostic; no counterpart in the reference. */
+int gdb_get_last_path(gdb_sim *h);
+
 /* Status bits set by kernels since the last clear; gdb_clear_status resets. */
 uint32_t gdb_status_word(gdb_sim *h);
 int gdb_clear_status(gdb_sim *h);
@@ -206,6 +212,24 @@ int gdb_rdf_compute(int n, const float *r, const int32_t *ptype, const float box
                     double r_max, uint64_t *out);
 int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], int nq, const int32_t *n_vectors,
                    double *rho_re, double *rho_im);
+
+/* Batched replicas (no counterpart in the reference, whose users loop over
+ * state points one Simulation at a time, e.g. examples/isomorph.py:27-82):
+ * advance many independent, fully configured and uploaded systems together.
+ * Systems of up to 4096 particles run one thread-block cluster each, grouped
+ * into one launch per cluster shape; larger systems run their persistent
+ * kernels concurrently on their own streams with a share of the GPU.  All
+ * systems need the same device, number of types and integrator; sizes,
+ * boxes, parameters and temperatures may differ.  gdb_batch_run is one
+ * timeblock for every system (as gdb_sim_run) and returns the first error;
+ * per-system results are read from each handle as usual. */
+typedef struct gdb_batch gdb_batch;
+/* particles_per_cta: cluster shaping target (about that many particles per
+ * CTA, up to 16 CTAs per system); 0 = 128.  Tuned by Batch.autotune. */
+int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb_batch **out);
+int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms);
+int gdb_batch_destroy(gdb_batch *b);
+int gdb_batch_get_last_error(gdb_batch *b, char *buf, int n);
 
 /* S(q) without any device allocation.  No counterpart in the reference: it
  * serves callers that cannot let the library call cudaMalloc -- programs whose
