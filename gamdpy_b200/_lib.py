@@ -281,7 +281,9 @@ class Sim:
         return out
 
     def last_path(self):
-        """0 graph launches, 1 persistent grid kernel, 2 thread-block cluster."""
+        """0 graph launches, 1 persistent grid kernel, 2 thread-block cluster with the
+        state in shared memory, 3 thread-block cluster with the state in global
+        memory (batched systems)."""
         return int(lib().gdb_get_last_path(self.h))
 
     def status(self):

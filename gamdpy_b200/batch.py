@@ -3,10 +3,12 @@
 gamdpy runs one Simulation per process and launches one kernel grid per
 system; ensembles of small systems (state-point sweeps, replicas for
 averaging) leave most of a B200 idle that way.  ``SimulationBatch`` gives
-each system of up to 4096 particles one thread-block cluster (positions in
-distributed shared memory, velocities in registers, the whole timeblock in one
-launch) and runs every such system of the batch in the same launch; larger
-systems run their persistent grid kernels concurrently on their own streams.
+every system one thread-block cluster for a whole timeblock: up to 4096
+particles with positions and lists in the cluster's shared memory
+(velocities in registers), larger systems with their state in global memory
+and hardware cluster barriers between the phases.  Systems of one cluster
+shape share one launch; systems above 131072 particles run one after another
+on the persistent grid kernel.
 Per system the result is that of ``Simulation.run_timeblocks``: the same
 output datasets, runtime actions and state on the host after each block.
 """
@@ -52,7 +54,8 @@ class SimulationBatch:
 
     def paths(self):
         """Execution path each system took in the last block (1 persistent
-        grid kernel, 2 thread-block cluster)."""
+        grid kernel, 2 cluster with the state in shared memory, 3 cluster with
+        the state in global memory)."""
         return [s._sim.last_path() for s in self.simulations]
 
     def integrate_self(self, time_zero, steps):

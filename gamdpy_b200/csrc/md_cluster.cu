@@ -98,8 +98,56 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     int maxcount = 0, nbuild = 0;
     const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
     const float ilx = 1.0f / Lx, ily = 1.0f / Ly, ilz = 1.0f / Lz;
+    // cluster-wide maximum of a per-thread value (called by every thread)
+    auto cluster_max = [&](int v) -> int {
+        v = __reduce_max_sync(0xffffffffu, v);
+        if (tid == 0) s_flag[0] = 0;
+        __syncthreads();
+        if (lane == 0) atomicMax(&s_flag[0], v);
+        __syncthreads();
+        if (tid == 0) spart[NQ + 1] = (double)s_flag[0];
+        cl.sync();
+        if (tid < C) s_gather[tid][0] = cl.map_shared_rank(spart, tid)[NQ + 1];
+        __syncthreads();
+        if (tid == 0) {
+            int m = 0;
+            for (int r = 0; r < C; r++) m = max(m, (int)s_gather[r][0]);
+            s_flag[1] = m;
+        }
+        __syncthreads();
+        const int m = s_flag[1];
+        cl.sync();
+        return m;
+    };
     cl.sync();
     trace_mark(ctrl, TR_START);
+    // Shared memory holds the lists only while this launch runs.  Without a
+    // rebuild due, the current lists come from global memory, where the last
+    // build (on either path) left them.
+    if (!rebuild) {
+        int lmax = 0;
+        for (int q = warp; q < np; q += CL_THREADS / 32) {
+            int cnt = a.nbc[p0 + q];
+            const int lim = min(min(cnt, cap), a.max_nbs);
+            bool bad = false;
+            for (int k = lane; k < lim; k += 32) {
+                const int j = a.nbl[nbl_index(p0 + q, k, a.stride)];
+                bad |= (unsigned)j >= (unsigned)n;
+                snbl[cl_nbl_index(q, k, P)] = (unsigned short)j;
+            }
+            if (__any_sync(0xffffffffu, bad)) {  // not a list of this system: no pairs, error status
+                cnt = 0;
+                if (lane == 0) atomicOr(&ctrl->status, GDB_STATUS_BAD_INDEX);
+            }
+            if (lane == 0) snbc[q] = cnt;
+            lmax = max(lmax, cnt);
+        }
+        const int mx = cluster_max(lmax);
+        if (mx > cap && mx < a.max_nbs) {
+            if (rank == 0 && tid == 0) atomicOr(&ctrl->status, GDB_STATUS_CLUSTER_CAPACITY);
+            return;  // uniform across the cluster: nothing was written back
+        }
+    }
 
     for (int s = 0; s < nsteps + do_eval; s++) {
         const int step = job.step0 + s;
@@ -264,25 +312,9 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                     lmax = max(lmax, count);
                 }
             }
-            lmax = __reduce_max_sync(0xffffffffu, lmax);
-            if (tid == 0) s_flag[0] = 0;
-            __syncthreads();
-            if (lane == 0) atomicMax(&s_flag[0], lmax);
-            __syncthreads();
             if (owner) rr = spos[i];
-            if (tid == 0) spart[NQ + 1] = (double)s_flag[0];
-            cl.sync();
             // cluster-wide longest list; beyond the shared capacity: abort
-            if (tid < C) s_gather[tid][0] = cl.map_shared_rank(spart, tid)[NQ + 1];
-            __syncthreads();
-            if (tid == 0) {
-                int mx = 0;
-                for (int r = 0; r < C; r++) mx = max(mx, (int)s_gather[r][0]);
-                s_flag[1] = mx;
-            }
-            __syncthreads();
-            const int mx = s_flag[1];
-            cl.sync();
+            const int mx = cluster_max(lmax);
             trace_mark(ctrl, TR_REBUILD_DONE);
             maxcount = max(maxcount, mx);
             nbuild++;
@@ -581,7 +613,11 @@ bool cluster_plan(int n, int C, int ncell, int max_nbs, int *cap, size_t *smem) 
 cudaError_t launch_clusters(const ClusterJob *d_jobs, int count, int C, int tp, int ntypes, int integ, size_t smem,
                             int nsteps, int do_eval, cudaStream_t st) {
     const void *fn = cluster_kernel(tp, ntypes, integ);
-    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (smem > CL_SMEM_LIMIT) return cudaErrorInvalidValue;
+    // one value for every launch of the function: launches of one kernel with
+    // different shared-memory sizes may be in flight on several streams, and
+    // the function attribute is shared by all of them
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CL_SMEM_LIMIT);
     if (e != cudaSuccess) return e;
     if (C > 8) {
         e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);

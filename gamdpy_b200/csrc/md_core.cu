@@ -527,8 +527,17 @@ static int status_to_rc(gdb_sim *h) {
     }
     if (h->h_ctrl->status & GDB_STATUS_NAN)
         return set_err(h, GDB_ERR_NUMERIC, "non-finite or runaway particle position");
-    if (h->h_ctrl->status & GDB_STATUS_BARRIER_TIMEOUT)
+    if (h->h_ctrl->status & GDB_STATUS_BAD_INDEX)
+        return set_err(h, GDB_ERR_NUMERIC, "cell sort produced a slot outside the particle range");
+    if (h->h_ctrl->status & GDB_STATUS_BARRIER_TIMEOUT) {
+        // an abandoned rebuild leaves counted cells behind: clear them and
+        // rebuild before the next step
+        if (h->cell_count) cudaMemsetAsync(h->cell_count, 0, (size_t)h->cell_cap * sizeof(int), h->st);
+        int one = 1;
+        cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st);
+        cudaStreamSynchronize(h->st);
         return set_err(h, GDB_ERR_TIMEOUT, "grid barrier of the persistent step kernel timed out");
+    }
     return GDB_OK;
 }
 
@@ -1142,19 +1151,37 @@ int gdb_get_last_path(gdb_sim *h) { return h ? h->last_path : -1; }
 // ---------------------------------------------------------------------------
 // batched replicas: many independent systems advanced together
 // ---------------------------------------------------------------------------
+// Every system of a batch runs in one thread-block cluster: up to 4096
+// particles with the whole state in shared memory (k_cluster_run), larger
+// ones with the state in global memory and the phases of the persistent
+// kernel between cluster barriers (k_run_clusters).  Systems of one cluster
+// shape share a launch, largest first; the launches run concurrently on
+// their own streams.  Systems above CLG_MAX_N particles (a cluster is too
+// small for them) run one after another on the persistent grid kernel once
+// the clusters are done, so no cooperative grid shares the GPU.
+constexpr int CLG_MAX_N = 1 << 17;
+
+static const void *run_clusters_kernel(int ntypes, int tp, int integ) {
+    return ntypes == 1   ? run_clusters_kernel_nt1(tp, integ)
+           : ntypes == 2 ? run_clusters_kernel_nt2(tp, integ)
+                         : run_clusters_kernel_ntg(tp, integ);
+}
+
 struct gdb_batch {
     struct Group {
+        int kind = 0;  // 0 shared-memory clusters, 1 global-memory clusters
         int C = 0, tp = 0;
         size_t smem = 0;
         std::vector<int> idx, cap;
-        ClusterJob *d_jobs = nullptr, *h_jobs = nullptr;
+        void *d_jobs = nullptr, *h_jobs = nullptr;
         cudaStream_t st = nullptr;
         cudaEvent_t done = nullptr;
     };
     std::vector<gdb_sim *> sims;
     std::vector<Group> groups;
-    std::vector<int> big;  // systems too large for a cluster: persistent grid kernel, capped grid
+    std::vector<int> solo;  // too large for a cluster
     int dev = 0, ntypes = 1, integ = 0;
+    int clg_C = 16, clg_tp = 1;
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     char err[512] = "";
@@ -1188,7 +1215,6 @@ static void batch_free(gdb_batch *b) {
         if (g.done) cudaEventDestroy(g.done);
         if (g.st) cudaStreamDestroy(g.st);
     }
-    for (gdb_sim *h : b->sims) h->grid_cap = 0;
     if (b->ev0) cudaEventDestroy(b->ev0);
     if (b->ev1) cudaEventDestroy(b->ev1);
     if (b->st) cudaStreamDestroy(b->st);
@@ -1201,6 +1227,39 @@ static void cluster_grid_of(const gdb_sim *h, int nc[3]) {
         nc[k] = (int)(h->box[k] / min_cell);
         if (nc[k] < 1) nc[k] = 1;
     }
+}
+
+static gdb_batch::Group *batch_group(gdb_batch *b, int kind, int C, int tp) {
+    for (auto &x : b->groups)
+        if (x.kind == kind && x.C == C && x.tp == tp) return &x;
+    b->groups.emplace_back();
+    gdb_batch::Group *g = &b->groups.back();
+    g->kind = kind;
+    g->C = C;
+    g->tp = tp;
+    return g;
+}
+
+static cudaError_t launch_run_clusters(const void *fn, const ClusterRunJob *d_jobs, int count, int C, int nsteps,
+                                       int do_eval, cudaStream_t st) {
+    if (C > 8) {
+        cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        if (e != cudaSuccess) return e;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(count * C);
+    cfg.blockDim = dim3(GDB_BLOCK);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = C;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    void *args[] = {(void *)&d_jobs, (void *)&nsteps, (void *)&do_eval};
+    return cudaLaunchKernelExC(&cfg, fn, args);
 }
 
 extern "C" {
@@ -1220,6 +1279,11 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
             return bset(nullptr, GDB_ERR_ARG,
                         "gdb_batch_create: every system needs the same device, type count and integrator");
         }
+        for (int q = 0; q < k; q++)
+            if (sims[q] == h) {
+                batch_free(b);
+                return bset(nullptr, GDB_ERR_ARG, "gdb_batch_create: system %d appears twice", k);
+            }
         int rc = check_ready(h);
         if (rc) {
             snprintf(g_lib_error, sizeof(g_lib_error), "gdb_batch_create: system %d: %.400s", k, h->err);
@@ -1233,45 +1297,39 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
         batch_free(b);
         return bset(nullptr, GDB_ERR_CUDA, "gdb_batch_create: %s", cudaGetErrorString(e));
     }
-    // group the cluster-sized systems by cluster shape (one launch each)
-    for (int k = 0; k < count; k++) {
+    // largest first inside every launch: the long clusters start first
+    std::vector<int> order(count);
+    for (int k = 0; k < count; k++) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return sims[x]->n > sims[y]->n; });
+    for (int k : order) {
         gdb_sim *h = sims[k];
         int nc[3];
         cluster_grid_of(h, nc);
-        int C, tp;
-        cluster_shape(h->n, particles_per_cta, &C, &tp);
-        int cap;
+        int C, tp, cap;
         size_t smem;
-        if (!h->cluster_ok || h->n > CL_MAX_N || !cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &smem)) {
-            b->big.push_back(k);
-            continue;
+        cluster_shape(h->n, particles_per_cta, &C, &tp);
+        if (h->cluster_ok && h->n <= CL_MAX_N &&
+            cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &smem)) {
+            gdb_batch::Group *g = batch_group(b, 0, C, tp);
+            g->idx.push_back(k);
+            g->cap.push_back(cap);
+            g->smem = std::max(g->smem, smem);
+        } else if (h->n <= CLG_MAX_N) {
+            gdb_batch::Group *g = batch_group(b, 1, b->clg_C, b->clg_tp);
+            g->idx.push_back(k);
+            g->cap.push_back(0);
+        } else {
+            b->solo.push_back(k);
         }
-        gdb_batch::Group *g = nullptr;
-        for (auto &x : b->groups)
-            if (x.C == C && x.tp == tp) g = &x;
-        if (!g) {
-            b->groups.emplace_back();
-            g = &b->groups.back();
-            g->C = C;
-            g->tp = tp;
-        }
-        g->idx.push_back(k);
-        g->cap.push_back(cap);
-        g->smem = std::max(g->smem, smem);
     }
     for (auto &g : b->groups) {
-        const size_t bytes = g.idx.size() * sizeof(ClusterJob);
+        const size_t bytes = g.idx.size() * (g.kind == 0 ? sizeof(ClusterJob) : sizeof(ClusterRunJob));
         if ((e = cudaMalloc(&g.d_jobs, bytes)) || (e = cudaMallocHost(&g.h_jobs, bytes)) ||
             (e = cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking)) ||
             (e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming))) {
             batch_free(b);
             return bset(nullptr, GDB_ERR_CUDA, "gdb_batch_create: %s", cudaGetErrorString(e));
         }
-    }
-    // large systems share the GPU with the clusters: cap their persistent grids
-    if (!b->big.empty()) {
-        const int share = std::max(16, 3 * 148 / (int)(b->big.size() + (b->groups.empty() ? 0 : 1)));
-        for (int k : b->big) sims[k]->grid_cap = share;
     }
     *out = b;
     return GDB_OK;
@@ -1298,7 +1356,8 @@ int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
             free_graphs(h);
         }
         if (rows > 0) BCK(cudaMemsetAsync(h->rows, 0, (size_t)rows * GDB_NUM_SCALARS * sizeof(double), h->st));
-        if ((rc = ensure_partials(h, grid_for((long long)h->n * h->tp)))) return bset(b, rc, "%s", h->err);
+        if ((rc = ensure_partials(h, std::max(grid_for((long long)h->n * h->tp), b->clg_C))))
+            return bset(b, rc, "%s", h->err);
         BCK(cudaMemsetAsync(&h->ctrl->maxcount, 0, sizeof(int), h->st));
         k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
         BCK(cudaGetLastError());
@@ -1306,33 +1365,51 @@ int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
         BCK(cudaStreamWaitEvent(b->st, h->ev0, 0));
     }
     BCK(cudaEventRecord(b->ev0, b->st));
-    // one cluster launch per shape group
+    // one launch per cluster shape, concurrently
     for (auto &g : b->groups) {
         BCK(cudaStreamWaitEvent(g.st, b->ev0, 0));
-        BCK(cudaStreamSynchronize(g.st));  // pinned job buffer is rewritten below
+        BCK(cudaStreamSynchronize(g.st));  // the pinned job buffer is rewritten below
         for (size_t q = 0; q < g.idx.size(); q++) {
             gdb_sim *h = b->sims[g.idx[q]];
             SimArgs a = make_args(h);
-            int nc[3];
-            cluster_grid_of(h, nc);
-            a.ncx = nc[0];
-            a.ncy = nc[1];
-            a.ncz = nc[2];
-            g.h_jobs[q].a = a;
-            g.h_jobs[q].tab = h->table;
-            g.h_jobs[q].cur = h->cur;
-            g.h_jobs[q].step0 = 0;
-            g.h_jobs[q].cap = g.cap[q];
+            if (g.kind == 0) {
+                int nc[3];
+                cluster_grid_of(h, nc);
+                a.ncx = nc[0];
+                a.ncy = nc[1];
+                a.ncz = nc[2];
+                ClusterJob &j = static_cast<ClusterJob *>(g.h_jobs)[q];
+                j.a = a;
+                j.tab = h->table;
+                j.cur = h->cur;
+                j.step0 = 0;
+                j.cap = g.cap[q];
+            } else {
+                ClusterRunJob &j = static_cast<ClusterRunJob *>(g.h_jobs)[q];
+                j.a = a;
+                j.tab = h->table;
+                j.cur = h->cur;
+            }
         }
-        BCK(cudaMemcpyAsync(g.d_jobs, g.h_jobs, g.idx.size() * sizeof(ClusterJob), cudaMemcpyHostToDevice, g.st));
-        BCK(launch_clusters(g.d_jobs, (int)g.idx.size(), g.C, g.tp, b->ntypes, b->integ, g.smem, steps, 1, g.st));
+        const int cnt = (int)g.idx.size();
+        if (g.kind == 0) {
+            BCK(cudaMemcpyAsync(g.d_jobs, g.h_jobs, cnt * sizeof(ClusterJob), cudaMemcpyHostToDevice, g.st));
+            BCK(launch_clusters(static_cast<const ClusterJob *>(g.d_jobs), cnt, g.C, g.tp, b->ntypes, b->integ, g.smem,
+                                steps, 1, g.st));
+        } else {
+            BCK(cudaMemcpyAsync(g.d_jobs, g.h_jobs, cnt * sizeof(ClusterRunJob), cudaMemcpyHostToDevice, g.st));
+            BCK(launch_run_clusters(run_clusters_kernel(b->ntypes, g.tp, b->integ),
+                                    static_cast<const ClusterRunJob *>(g.d_jobs), cnt, g.C, steps, 1, g.st));
+        }
         BCK(cudaEventRecord(g.done, g.st));
         BCK(cudaStreamWaitEvent(b->st, g.done, 0));
     }
-    // large systems: persistent kernels on their own streams, concurrently
-    for (int k : b->big) {
+    // systems too large for a cluster: the persistent grid kernel, one at a
+    // time, after the clusters
+    for (int k : b->solo) {
         gdb_sim *h = b->sims[k];
-        BCK(cudaStreamWaitEvent(h->st, b->ev0, 0));
+        BCK(cudaEventRecord(b->ev1, b->st));
+        BCK(cudaStreamWaitEvent(h->st, b->ev1, 0));
         int rc = launch_run(h, steps, 1);
         if (rc) return bset(b, rc, "gdb_batch_run: %s", h->err);
         h->last_path = 1;
@@ -1346,9 +1423,10 @@ int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
         for (int k : g.idx) {
             gdb_sim *h = b->sims[k];
             h->cur ^= (steps & 1);
-            h->last_path = 2;
+            h->last_path = g.kind == 0 ? 2 : 3;
         }
-    // status; a cluster whose lists outgrew shared memory reruns alone
+    // status; a shared-memory cluster whose lists outgrew shared memory
+    // reruns alone on the global-memory path
     int first_rc = GDB_OK;
     for (size_t k = 0; k < b->sims.size(); k++) {
         gdb_sim *h = b->sims[k];

@@ -42,68 +42,94 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_step(SimA
     if (threadIdx.x == 0) ctrl->ticket = 0;
 }
 
-// Rebuild inside the persistent kernel: the same phases with grid barriers.
-template <bool FMA>
-__device__ inline bool rebuild_persistent(const SimArgs &a, int cur) {
+// Synchronisation of the blocks that share one system, between phases.
+// `last` runs on one whole block after every block has arrived and before
+// any leaves; the call returns false when the wait was abandoned.
+struct GridSync {  // bounded software barrier over a cooperative grid
+    template <typename F>
+    __device__ __forceinline__ bool operator()(DevCtrl *c, F last) const {
+        return grid_barrier(c, last);
+    }
+};
+
+// Hardware barrier of a thread-block cluster; release/acquire at cluster scope
+// orders the global-memory writes of every CTA of the cluster before the
+// reads after it.  Rank 0 runs `last` between two barriers.
+__device__ __forceinline__ void cluster_barrier() {
+    asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
+}
+struct ClusterSync {
+    int rank;
+    template <typename F>
+    __device__ __forceinline__ bool operator()(DevCtrl *, F last) const {
+        cluster_barrier();
+        if (rank == 0) last();
+        cluster_barrier();
+        return true;
+    }
+};
+
+// Neighbour-list rebuild by the blocks of span g: the phases of the
+// standalone chain with a synchronisation between them.
+template <bool FMA, class Sync>
+__device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const Sync &sync) {
     DevCtrl *c = a.ctrl;
     auto none = [] {};
     if (a.nb_kind == GDB_NBLIST_NSQ) {
-        phase_nbl_nsq<FMA, false>(a, cur);
-        const bool ok = grid_barrier(c, [&] {
+        phase_nbl_nsq<FMA, false>(a, cur, g);
+        const bool ok = sync(c, [&] {
             if (threadIdx.x == 0) rebuild_done(c);
         });
         trace_mark(c, TR_REBUILD_DONE);
         return ok;
     }
-    phase_cell_assign<false>(a, cur);
-    if (!grid_barrier(c, none)) return false;
+    phase_cell_assign<false>(a, cur, g);
+    if (!sync(c, none)) return false;
     trace_mark(c, TR_REBUILD_PHASE);
-    phase_scan_partial(a);
-    if (!grid_barrier(c, [&] { block_scan_chunks(a); })) return false;
-    phase_scan_final(a);
-    if (!grid_barrier(c, none)) return false;
-    phase_scatter(a);
-    if (!grid_barrier(c, none)) return false;
+    phase_scan_partial(a, g);
+    if (!sync(c, [&] { block_scan_chunks(a); })) return false;
+    phase_scan_final(a, g);
+    if (!sync(c, none)) return false;
+    phase_scatter(a, g);
+    if (!sync(c, none)) return false;
     trace_mark(c, TR_REBUILD_PHASE);
-    phase_sort_cells(a);
-    if (!grid_barrier(c, none)) return false;
-    phase_gather(a, cur);
-    if (!grid_barrier(c, none)) return false;
+    phase_sort_cells(a, g);
+    if (!sync(c, none)) return false;
+    phase_gather(a, cur, g);
+    if (!sync(c, none)) return false;
     trace_mark(c, TR_REBUILD_PHASE);
-    phase_nbl_cells<FMA>(a);
-    if (!grid_barrier(c, none)) return false;
+    phase_nbl_cells<FMA>(a, g);
+    if (!sync(c, none)) return false;
     trace_mark(c, TR_REBUILD_PHASE);
-    phase_finish_cells(a, cur);
-    const bool ok = grid_barrier(c, [&] {
+    phase_finish_cells(a, cur, g);
+    const bool ok = sync(c, [&] {
         if (threadIdx.x == 0) rebuild_done(c);
     });
     trace_mark(c, TR_REBUILD_DONE);
     return ok;
 }
 
-// Persistent cooperative kernel: `nsteps` steps starting from pos[cur0], then
-// (if do_eval) the force-only evaluation of the final state -- one timeblock
-// of simulation/Simulation.py:306-328 in one launch.
-template <int TP, int NT, int INTEG>
-__global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
-    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
-    __shared__ double s_red[NQ * 32];
-    load_table(tab, s_tab);
+// `nsteps` steps starting from pos[cur0], then (if do_eval) the force-only
+// evaluation of the final state -- one timeblock of
+// simulation/Simulation.py:306-328 -- by the blocks of span g.
+template <int TP, int NT, int INTEG, class Sync>
+__device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int nt, int cur0, int nsteps, int do_eval,
+                                 Span g, const Sync &sync, double *s_red) {
     DevCtrl *ctrl = a.ctrl;
     int cur = cur0;
     trace_mark(ctrl, TR_START);
     for (int s = 0; s < nsteps + do_eval; s++) {
         if (*(volatile int *)&ctrl->rebuild) {
-            const bool ok = a.fma ? rebuild_persistent<true>(a, cur) : rebuild_persistent<false>(a, cur);
+            const bool ok = a.fma ? rebuild_phases<true>(a, cur, g, sync) : rebuild_phases<false>(a, cur, g, sync);
             if (!ok) return;
         }
         const int step = *(volatile int *)&ctrl->step;
         bool ok;
         if (s < nsteps) {
-            phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, tab.nt, cur, step, s_red);
+            phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g);
             trace_mark(ctrl, TR_STEP_PHASE);
-            ok = grid_barrier(ctrl, [&] {
-                finalize_step<MODE_STEP>(a, step, gridDim.x, s_red);
+            ok = sync(ctrl, [&] {
+                finalize_step<MODE_STEP>(a, step, g.nb, s_red);
                 if (threadIdx.x == 0 && ctrl->rebuild_next) {
                     ctrl->rebuild = 1;
                     ctrl->rebuild_next = 0;
@@ -112,20 +138,56 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArg
             cur ^= 1;
             trace_mark(ctrl, TR_STEP);
         } else {
-            phase_step<TP, NT, INTEG, MODE_EVAL, false, true>(a, s_tab, tab.nt, cur, step, s_red);
-            ok = grid_barrier(ctrl, [&] { finalize_step<MODE_EVAL>(a, step, gridDim.x, s_red); });
+            phase_step<TP, NT, INTEG, MODE_EVAL, false, true>(a, s_tab, nt, cur, step, s_red, g);
+            ok = sync(ctrl, [&] { finalize_step<MODE_EVAL>(a, step, g.nb, s_red); });
             trace_mark(ctrl, TR_EVAL);
         }
         if (!ok) return;
     }
 }
 
+// Persistent cooperative kernel: one timeblock of one system per launch.
+template <int TP, int NT, int INTEG>
+__global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
+    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    load_table(tab, s_tab);
+    // a block that starts after others abandoned a barrier does no work
+    if (*(volatile int *)&a.ctrl->abort) return;
+    run_steps<TP, NT, INTEG>(a, s_tab, tab.nt, cur0, nsteps, do_eval, grid_span(), GridSync{}, s_red);
+}
+
+// One system per thread-block cluster, state in global memory: a batch of
+// systems advances a timeblock in one launch, each cluster with hardware
+// barriers between its phases (no cooperative launch, no software barrier).
+struct ClusterRunJob {
+    SimArgs a;
+    PairTable tab;
+    int cur;  // position buffer holding the current state
+};
+
+template <int TP, int NT, int INTEG>
+__global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP))
+    k_run_clusters(const ClusterRunJob *__restrict__ jobs, int nsteps, int do_eval) {
+    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    __shared__ SimArgs s_a;
+    unsigned rank, nrank;
+    asm("mov.u32 %0, %%cluster_ctarank;" : "=r"(rank));
+    asm("mov.u32 %0, %%cluster_nctarank;" : "=r"(nrank));
+    const ClusterRunJob &job = jobs[blockIdx.x / nrank];
+    if (threadIdx.x == 0) s_a = job.a;
+    load_table(job.tab, s_tab);  // ends with __syncthreads
+    run_steps<TP, NT, INTEG>(s_a, s_tab, job.tab.nt, job.cur, nsteps, do_eval, Span{(int)rank, (int)nrank},
+                             ClusterSync{(int)rank}, s_red);
+}
 
 // Entry points each instantiation unit exports to the host code.
 #define GDB_DECLARE_NT(NTNAME)                                                                          \
     void launch_step_##NTNAME(const SimArgs &a, const PairTable &tab, cudaStream_t st, int tp, int integ, \
                               int mode, int grid, int cur);                                            \
-    const void *run_kernel_##NTNAME(int tp, int integ);
+    const void *run_kernel_##NTNAME(int tp, int integ);                                                  \
+    const void *run_clusters_kernel_##NTNAME(int tp, int integ);
 
 GDB_DECLARE_NT(nt1)
 GDB_DECLARE_NT(nt2)
@@ -166,6 +228,19 @@ GDB_DECLARE_NT(ntg)
             case 8: return run_tp_##NTNAME<8>(integ);                                                        \
             case 16: return run_tp_##NTNAME<16>(integ);                                                      \
             default: return run_tp_##NTNAME<32>(integ);                                                      \
+        }                                                                                                    \
+    } \
+    template <int TP>                                                                                        \
+    static const void *run_clusters_tp_##NTNAME(int integ) {                                                 \
+        return integ == GDB_INTEGRATOR_NVT ? (const void *)k_run_clusters<TP, NT, GDB_INTEGRATOR_NVT>        \
+                                           : (const void *)k_run_clusters<TP, NT, GDB_INTEGRATOR_NVE>;       \
+    }                                                                                                        \
+    const void *run_clusters_kernel_##NTNAME(int tp, int integ) {                                            \
+        switch (tp) {                                                                                        \
+            case 1: return run_clusters_tp_##NTNAME<1>(integ);                                               \
+            case 2: return run_clusters_tp_##NTNAME<2>(integ);                                               \
+            case 4: return run_clusters_tp_##NTNAME<4>(integ);                                               \
+            default: return run_clusters_tp_##NTNAME<8>(integ);                                              \
         }                                                                                                    \
     }
 

@@ -63,6 +63,14 @@ struct SimArgs {
 
 __device__ __forceinline__ float4 *cur_pos(const SimArgs &a, int cur) { return cur ? a.pos1 : a.pos0; }
 
+// The blocks that share one system's work: the whole grid (standalone and
+// persistent kernels) or the CTAs of one thread-block cluster (batched
+// systems).  b is this block's index among them, nb their number.
+struct Span {
+    int b, nb;
+};
+__device__ __forceinline__ Span grid_span() { return Span{(int)blockIdx.x, (int)gridDim.x}; }
+
 template <bool NC, typename T>
 __device__ __forceinline__ T load(const T *p) {
     if (NC) return __ldg(p);
@@ -102,7 +110,11 @@ template <typename F>
 __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
     __shared__ int s_last, s_ok;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && *(volatile int *)&c->abort) {
+        // another block gave up: arrive nowhere, leave with the others
+        s_last = 0;
+        s_ok = 0;
+    } else if (threadIdx.x == 0) {
         const unsigned gen = ld_acquire_gpu(&c->bar_gen);
         const unsigned grp = blockIdx.x / BAR_GROUP;
         const unsigned gsize = min((unsigned)BAR_GROUP, gridDim.x - grp * BAR_GROUP);
@@ -133,6 +145,7 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
         }
     }
     __syncthreads();
+    if (!s_ok) return false;
     if (s_last) {
         last();
         __syncthreads();
@@ -152,11 +165,11 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
 // N^2 build (interactions/nblist.py:88-143): one warp per particle, lanes
 // stride over j, ballot + popc append hits in ascending j (deterministic).
 template <bool FMA, bool NC>
-__device__ inline void phase_nbl_nsq(const SimArgs &a, int cur) {
+__device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_span()) {
     const float4 *pos = cur_pos(a, cur);
     const int lane = threadIdx.x & 31;
-    const int warps = (gridDim.x * blockDim.x) >> 5;
-    for (int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < a.n; i += warps) {
+    const int warps = (g.nb * (int)blockDim.x) >> 5;
+    for (int i = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; i < a.n; i += warps) {
         const float4 pi = load<NC>(pos + i);
         int count = 0;
         for (int j0 = 0; j0 < a.n; j0 += 32) {
@@ -196,9 +209,9 @@ __device__ __forceinline__ int cell_coord(float x, float L, int nc, DevCtrl *ctr
 }
 
 template <bool NC>
-__device__ inline void phase_cell_assign(const SimArgs &a, int cur) {
+__device__ inline void phase_cell_assign(const SimArgs &a, int cur, Span g = grid_span()) {
     const float4 *pos = cur_pos(a, cur);
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    for (int i = g.b * (int)blockDim.x + (int)threadIdx.x; i < a.n; i += g.nb * (int)blockDim.x) {
         const float4 p = load<NC>(pos + i);
         const int cx = cell_coord(p.x, a.Lx, a.ncx, a.ctrl);
         const int cy = cell_coord(p.y, a.Ly, a.ncy, a.ctrl);
@@ -253,10 +266,10 @@ __device__ __forceinline__ void chunk_scan(const int *in, int len, int base, int
     __syncthreads();
 }
 
-__device__ inline void phase_scan_partial(const SimArgs &a) {
+__device__ inline void phase_scan_partial(const SimArgs &a, Span g = grid_span()) {
     __shared__ int sm[32];
     __shared__ int tot;
-    for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x) {
+    for (int c = g.b; c < a.nchunks; c += g.nb) {
         chunk_scan(a.cell_count, a.ncell, c * SCAN_CHUNK, nullptr, 0, &tot, sm);
         if (threadIdx.x == 0) a.bsum[c] = tot;
         __syncthreads();
@@ -275,22 +288,27 @@ __device__ inline void block_scan_chunks(const SimArgs &a) {
     }
 }
 
-__device__ inline void phase_scan_final(const SimArgs &a) {
+__device__ inline void phase_scan_final(const SimArgs &a, Span g = grid_span()) {
     __shared__ int sm[32];
-    for (int c = blockIdx.x; c < a.nchunks; c += gridDim.x)
+    for (int c = g.b; c < a.nchunks; c += g.nb)
         chunk_scan(a.cell_count, a.ncell, c * SCAN_CHUNK, a.cell_start, a.bsum[c], nullptr, sm);
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.cell_start[a.ncell] = a.n;
+    if (g.b == 0 && threadIdx.x == 0) a.cell_start[a.ncell] = a.n;
 }
 
-__device__ inline void phase_scatter(const SimArgs &a) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
-        a.perm[a.cell_start[a.pcell[i]] + a.prank[i]] = i;
+__device__ inline void phase_scatter(const SimArgs &a, Span g = grid_span()) {
+    for (int i = g.b * (int)blockDim.x + (int)threadIdx.x; i < a.n; i += g.nb * (int)blockDim.x) {
+        const int slot = a.cell_start[a.pcell[i]] + a.prank[i];
+        if ((unsigned)slot < (unsigned)a.n)
+            a.perm[slot] = i;
+        else
+            atomicOr(&a.ctrl->status, GDB_STATUS_BAD_INDEX);
+    }
 }
 
 // Order every cell's particles by user index: the atomics of the assignment
 // rank them arbitrarily; this makes the layout and every sum deterministic.
-__device__ inline void phase_sort_cells(const SimArgs &a) {
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += gridDim.x * blockDim.x) {
+__device__ inline void phase_sort_cells(const SimArgs &a, Span g = grid_span()) {
+    for (int c = g.b * (int)blockDim.x + (int)threadIdx.x; c < a.ncell; c += g.nb * (int)blockDim.x) {
         const int lo = a.cell_start[c], hi = a.cell_start[c + 1];
         for (int x = lo + 1; x < hi; x++) {
             const int v = a.perm[x];
@@ -305,11 +323,15 @@ __device__ inline void phase_sort_cells(const SimArgs &a) {
     }
 }
 
-__device__ inline void phase_gather(const SimArgs &a, int cur) {
+__device__ inline void phase_gather(const SimArgs &a, int cur, Span g = grid_span()) {
     const float4 *pos = cur_pos(a, cur);
     const size_t n = a.n;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
-        const int i = a.perm[s];
+    for (int s = g.b * (int)blockDim.x + (int)threadIdx.x; s < a.n; s += g.nb * (int)blockDim.x) {
+        int i = a.perm[s];
+        if ((unsigned)i >= (unsigned)a.n) {
+            atomicOr(&a.ctrl->status, GDB_STATUS_BAD_INDEX);
+            i = s;
+        }
         a.pos_tmp[s] = pos[i];
         a.vel_tmp[s] = a.vel[i];
         a.img_tmp[s] = a.img[i];
@@ -363,7 +385,7 @@ constexpr int NB_SEG_MAX = 64; // 25 rows x at most 2 ranges
 __device__ __forceinline__ int wrapi(int x, int n) { return ((x % n) + n) % n; }
 
 template <bool FMA, bool SHIFTED>
-__device__ inline void phase_nbl_cells_t(const SimArgs &a) {
+__device__ inline void phase_nbl_cells_t(const SimArgs &a, Span g) {
     __shared__ int s_lo[GDB_BLOCK / 32][NB_SEG_MAX];
     __shared__ int s_pre[GDB_BLOCK / 32][NB_SEG_MAX + 1];
     __shared__ float3 s_sh[GDB_BLOCK / 32][SHIFTED ? NB_SEG_MAX : 1];
@@ -373,10 +395,10 @@ __device__ inline void phase_nbl_cells_t(const SimArgs &a) {
     const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
     int *lo_s = s_lo[wib], *pre_s = s_pre[wib];
     float3 *sh_s = s_sh[wib];
-    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const int nwarps = (g.nb * (int)blockDim.x) >> 5;
     const int ry = ncy < 5 ? ncy : 5, rz = ncz < 5 ? ncz : 5;
     const int nrows = ry * rz;
-    for (int c = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; c < a.ncell; c += nwarps) {
+    for (int c = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; c < a.ncell; c += nwarps) {
         const int cs = a.cell_start[c], ce = a.cell_start[c + 1];
         if (cs == ce) continue;
         const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
@@ -510,19 +532,19 @@ __device__ inline void phase_nbl_cells_t(const SimArgs &a) {
 }
 
 template <bool FMA>
-__device__ inline void phase_nbl_cells(const SimArgs &a) {
+__device__ inline void phase_nbl_cells(const SimArgs &a, Span g = grid_span()) {
     const bool shifted = a.ncx >= 7 && a.ncy >= 7 && a.ncz >= 7 && !*(volatile int *)&a.ctrl->cell_wrap;
     if (shifted)
-        phase_nbl_cells_t<FMA, true>(a);
+        phase_nbl_cells_t<FMA, true>(a, g);
     else
-        phase_nbl_cells_t<FMA, false>(a);
+        phase_nbl_cells_t<FMA, false>(a, g);
 }
 
 // Move the reordered state into place, record r_ref, clear the cell counters.
-__device__ inline void phase_finish_cells(const SimArgs &a, int cur) {
+__device__ inline void phase_finish_cells(const SimArgs &a, int cur, Span g = grid_span()) {
     float4 *pos = cur_pos(a, cur);
     const size_t n = a.n;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.n; s += gridDim.x * blockDim.x) {
+    for (int s = g.b * (int)blockDim.x + (int)threadIdx.x; s < a.n; s += g.nb * (int)blockDim.x) {
         const float4 p = a.pos_tmp[s];
         pos[s] = p;
         a.rref[s] = p;
@@ -532,7 +554,7 @@ __device__ inline void phase_finish_cells(const SimArgs &a, int cur) {
         a.pscal[3 * n + s] = a.pscal_tmp[3 * n + s];
         a.pscal[4 * n + s] = a.pscal_tmp[4 * n + s];
     }
-    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < a.ncell; c += gridDim.x * blockDim.x) a.cell_count[c] = 0;
+    for (int c = g.b * (int)blockDim.x + (int)threadIdx.x; c < a.ncell; c += g.nb * (int)blockDim.x) a.cell_count[c] = 0;
 }
 
 __device__ __forceinline__ void rebuild_done(DevCtrl *c) {
@@ -658,10 +680,11 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
 
 // Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
 // only (MODE_EVAL).  Each block accumulates float64 partial sums over all the
-// particles it handles and writes them to partials[blockIdx.x].  Sets the
+// particles it handles and writes them to partials[g.b].  Sets the
 // rebuild flag when a particle has moved more than skin/2 since the build.
 template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
-__device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red) {
+__device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
+                                  Span g = grid_span()) {
     DevCtrl *ctrl = a.ctrl;
     const float4 *pos = cur_pos(a, cur);
     float4 *pos_next = cur_pos(a, cur ^ 1);
@@ -683,7 +706,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
 #pragma unroll
     for (int q = 0; q < NQ; q++) red[q] = 0.0;
     bool moved = false;
-    for (int round = blockIdx.x; round < rounds_total; round += gridDim.x) {
+    for (int round = g.b; round < rounds_total; round += g.nb) {
         const int i = round * per_block + threadIdx.x / TP;
         const int sub = threadIdx.x % TP;
         const bool active = i < a.n;
@@ -833,7 +856,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
     block_sum<NQ>(red, s_red);
     if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < NQ; q++) a.partials[(size_t)blockIdx.x * NQ + q] = red[q];
+        for (int q = 0; q < NQ; q++) a.partials[(size_t)g.b * NQ + q] = red[q];
     }
 }
 

@@ -44,6 +44,7 @@ extern "C" {
 #define GDB_STATUS_NAN 0x4u
 #define GDB_STATUS_BAD_ARG 0x8u
 #define GDB_STATUS_CLUSTER_CAPACITY 0x10u /* a list outgrew the cluster path's shared memory (rerun on the global path) */
+#define GDB_STATUS_BAD_INDEX 0x20u /* a cell-sort slot outside [0, n): the access was skipped */
 
 /* potentials: gamdpy/interactions/potential_functions/ */
 #define GDB_POT_LJ_SIGMA_EPSILON 0 /* LJ_12_6_sigma_epsilon.py:6-36, params (sigma, epsilon, cut) */
