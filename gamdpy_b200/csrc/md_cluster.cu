@@ -203,6 +203,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                     }
                 }
                 __syncthreads();
+                trace_mark(ctrl, TR_REBUILD_PHASE);
                 // per particle: the x-contiguous ranges of the 25 stencil rows
                 // (two at the x wrap; whole rows for grids under 5 cells),
                 // walked as one packed candidate sequence, 32 per iteration
@@ -313,6 +314,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                 }
             }
             if (owner) rr = spos[i];
+            trace_mark(ctrl, TR_REBUILD_PHASE);
             // cluster-wide longest list; beyond the shared capacity: abort
             const int mx = cluster_max(lmax);
             trace_mark(ctrl, TR_REBUILD_DONE);

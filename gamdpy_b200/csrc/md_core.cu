@@ -178,7 +178,8 @@ __global__ void __launch_bounds__(GDB_BLOCK) k_gather(SimArgs a, int cur) {
 template <bool FMA>
 __global__ void __launch_bounds__(GDB_BLOCK) k_nbl_cells(SimArgs a) {
     if (!a.ctrl->rebuild) return;
-    phase_nbl_cells<FMA>(a);
+    __shared__ NbScratch<GDB_BLOCK / 32> scr;
+    phase_nbl_cells<FMA>(a, grid_span(), scr);
 }
 __global__ void __launch_bounds__(GDB_BLOCK) k_finish_cells(SimArgs a, int cur) {
     if (!a.ctrl->rebuild) return;
@@ -445,7 +446,9 @@ static int enqueue_rebuild(gdb_sim *h) {
         k_scatter<<<g, GDB_BLOCK, 0, h->st>>>(a);
         k_sort_cells<<<grid_for(a.ncell), GDB_BLOCK, 0, h->st>>>(a);
         k_gather<<<g, GDB_BLOCK, 0, h->st>>>(a, cur);
-        const int gw = grid_for((long long)a.ncell * 32);
+        // a warp per cell, or a thread per particle for large systems (the
+        // build picks by threads per particle)
+        const int gw = n >= 131072 ? grid_for(n) : grid_for((long long)a.ncell * 32);
         if (h->fma)
             k_nbl_cells<true><<<gw, GDB_BLOCK, 0, h->st>>>(a);
         else
@@ -1181,7 +1184,7 @@ struct gdb_batch {
     std::vector<Group> groups;
     std::vector<int> solo;  // too large for a cluster
     int dev = 0, ntypes = 1, integ = 0;
-    int clg_C = 16, clg_tp = 1;
+    int clg_tp = 1;
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     char err[512] = "";
@@ -1248,7 +1251,7 @@ static cudaError_t launch_run_clusters(const void *fn, const ClusterRunJob *d_jo
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(count * C);
-    cfg.blockDim = dim3(GDB_BLOCK);
+    cfg.blockDim = dim3(CLG_BLOCK);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = st;
     cudaLaunchAttribute attr[1];
@@ -1315,7 +1318,10 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
             g->cap.push_back(cap);
             g->smem = std::max(g->smem, smem);
         } else if (h->n <= CLG_MAX_N) {
-            gdb_batch::Group *g = batch_group(b, 1, b->clg_C, b->clg_tp);
+            // about 1024 particles per CTA (one lane each), 4 to 16 CTAs
+            int c = 4;
+            while (c < 16 && h->n > c * 1024) c *= 2;
+            gdb_batch::Group *g = batch_group(b, 1, c, b->clg_tp);
             g->idx.push_back(k);
             g->cap.push_back(0);
         } else {
@@ -1356,7 +1362,7 @@ int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
             free_graphs(h);
         }
         if (rows > 0) BCK(cudaMemsetAsync(h->rows, 0, (size_t)rows * GDB_NUM_SCALARS * sizeof(double), h->st));
-        if ((rc = ensure_partials(h, std::max(grid_for((long long)h->n * h->tp), b->clg_C))))
+        if ((rc = ensure_partials(h, std::max(grid_for((long long)h->n * h->tp), 16))))
             return bset(b, rc, "%s", h->err);
         BCK(cudaMemsetAsync(&h->ctrl->maxcount, 0, sizeof(int), h->st));
         k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);

@@ -71,8 +71,8 @@ struct ClusterSync {
 
 // Neighbour-list rebuild by the blocks of span g: the phases of the
 // standalone chain with a synchronisation between them.
-template <bool FMA, class Sync>
-__device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const Sync &sync) {
+template <bool FMA, int WPB, class Sync>
+__device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const Sync &sync, NbScratch<WPB> &scr) {
     DevCtrl *c = a.ctrl;
     auto none = [] {};
     if (a.nb_kind == GDB_NBLIST_NSQ) {
@@ -98,7 +98,7 @@ __device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const S
     phase_gather(a, cur, g);
     if (!sync(c, none)) return false;
     trace_mark(c, TR_REBUILD_PHASE);
-    phase_nbl_cells<FMA>(a, g);
+    phase_nbl_cells<FMA>(a, g, scr);
     if (!sync(c, none)) return false;
     trace_mark(c, TR_REBUILD_PHASE);
     phase_finish_cells(a, cur, g);
@@ -112,15 +112,17 @@ __device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const S
 // `nsteps` steps starting from pos[cur0], then (if do_eval) the force-only
 // evaluation of the final state -- one timeblock of
 // simulation/Simulation.py:306-328 -- by the blocks of span g.
-template <int TP, int NT, int INTEG, class Sync>
+template <int TP, int NT, int INTEG, int WPB, class Sync>
 __device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int nt, int cur0, int nsteps, int do_eval,
                                  Span g, const Sync &sync, double *s_red) {
+    __shared__ NbScratch<WPB> scr;
     DevCtrl *ctrl = a.ctrl;
     int cur = cur0;
     trace_mark(ctrl, TR_START);
     for (int s = 0; s < nsteps + do_eval; s++) {
         if (*(volatile int *)&ctrl->rebuild) {
-            const bool ok = a.fma ? rebuild_phases<true>(a, cur, g, sync) : rebuild_phases<false>(a, cur, g, sync);
+            const bool ok =
+                a.fma ? rebuild_phases<true>(a, cur, g, sync, scr) : rebuild_phases<false>(a, cur, g, sync, scr);
             if (!ok) return;
         }
         const int step = *(volatile int *)&ctrl->step;
@@ -154,7 +156,7 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArg
     load_table(tab, s_tab);
     // a block that starts after others abandoned a barrier does no work
     if (*(volatile int *)&a.ctrl->abort) return;
-    run_steps<TP, NT, INTEG>(a, s_tab, tab.nt, cur0, nsteps, do_eval, grid_span(), GridSync{}, s_red);
+    run_steps<TP, NT, INTEG, GDB_BLOCK / 32>(a, s_tab, tab.nt, cur0, nsteps, do_eval, grid_span(), GridSync{}, s_red);
 }
 
 // One system per thread-block cluster, state in global memory: a batch of
@@ -166,8 +168,10 @@ struct ClusterRunJob {
     int cur;  // position buffer holding the current state
 };
 
+constexpr int CLG_BLOCK = 1024;  // one CTA per SM: a cluster of C CTAs spans C SMs
+
 template <int TP, int NT, int INTEG>
-__global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP))
+__global__ void __launch_bounds__(CLG_BLOCK, 1)
     k_run_clusters(const ClusterRunJob *__restrict__ jobs, int nsteps, int do_eval) {
     __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
     __shared__ double s_red[NQ * 32];
@@ -178,8 +182,8 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP))
     const ClusterRunJob &job = jobs[blockIdx.x / nrank];
     if (threadIdx.x == 0) s_a = job.a;
     load_table(job.tab, s_tab);  // ends with __syncthreads
-    run_steps<TP, NT, INTEG>(s_a, s_tab, job.tab.nt, job.cur, nsteps, do_eval, Span{(int)rank, (int)nrank},
-                             ClusterSync{(int)rank}, s_red);
+    run_steps<TP, NT, INTEG, CLG_BLOCK / 32>(s_a, s_tab, job.tab.nt, job.cur, nsteps, do_eval,
+                                             Span{(int)rank, (int)nrank}, ClusterSync{(int)rank}, s_red);
 }
 
 // Entry points each instantiation unit exports to the host code.

@@ -110,6 +110,27 @@ def test_cell_build_paths_vs_oracle(oracle, n, face):
     assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
 
 
+@pytest.mark.parametrize("n", [200000])
+def test_thread_per_particle_build_vs_oracle(oracle, n, monkeypatch):
+    """Large systems build a thread per particle (standalone chain and
+    persistent kernel); the sets must still equal the oracle's cell build."""
+    conf = workloads.ka_configuration(n, seed=13, jitter=0.2)
+    L = conf.simbox.lengths
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    ref, _ = oracle.nblist_cells(conf["r"], L, 2.5, 0.3, 300, fma=1)
+    c2, f2 = sorted_rows(ref)
+    sim = make_sim(conf["r"], L, conf.ptype, table, nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.eval_forces()  # standalone kernels
+    c1, f1 = sorted_rows(sim.nblist(300))
+    assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
+    sim.upload(conf["r"], np.zeros((n, 3), np.float32), np.ones(n, np.float32), conf.ptype)
+    sim.run(0.0, 0)  # persistent kernel: rebuild + evaluation
+    c1, f1 = sorted_rows(sim.nblist(300))
+    assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
+    res = oracle.forces(conf["r"], conf.ptype, L, table, ref, fma=1)
+    assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
+
+
 def run_api_trajectory(d):
     """Golden trajectory through the public API (Simulation + runtime actions)."""
     n = len(d["r0"])
