@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgamdb200.so")
-SOURCES = ["md_core.cu", "md_inst_nt1.cu", "md_inst_nt2.cu", "md_inst_ntg.cu", "md_cluster.cu", "analysis.cu"]
+SOURCES = ["md_core.cu", "md_inst_nt1.cu", "md_inst_nt2.cu", "md_inst_ntg.cu", "md_cluster.cu", "analysis.cu",
+           "adjoint.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",

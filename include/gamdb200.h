@@ -249,6 +249,38 @@ int gdb_sq_compute_noalloc(int n, const float *r_dev, const float *ff_dev, const
                            const int32_t *n_vectors_dev, int n_max, double *rho_re_dev, double *rho_im_dev,
                            void *stream);
 
+/* ---- adjoint: gradients of trajectory averages w.r.t. pair parameters ----
+ * No counterpart in the reference (gamdpy has no differentiation).  The
+ * forward is the NVE leapfrog of integrators/NVE.py:78-97 with the
+ * shifted-force Lennard-Jones of LJ_12_6_sigma_epsilon.py:26-36 and
+ * apply_shifted_force_cutoff.py:30-37, pairs over all j (the NbList2 set),
+ * float32 state with float64 sums.  Observables (time averages over the
+ * `steps` steps n = 0..steps-1): obs[0] = <U>, obs[1] = <W>, obs[2] = <K>
+ * (sums over particles; K from the mean of the half-step velocities, as NVE),
+ * obs[3 + b] = <g_AA(r_b)>, a Gaussian-kernel radial distribution of type-0
+ * pairs on every rdf_every-th step, bin centres r_lo + (b + 1/2)(r_hi - r_lo)/bins.
+ * The backward is the discrete adjoint of that forward: a reverse sweep with
+ * Hessian-vector products of the pair forces, recomputing each segment from
+ * checkpoints kept every checkpoint_every steps. */
+typedef struct gdb_adj gdb_adj;
+int gdb_adj_create(int n, int ntypes, int device, gdb_adj **out);
+int gdb_adj_destroy(gdb_adj *h);
+/* box lengths, types (n int32), masses (n float32), time step, steps,
+ * checkpoint interval; RDF bins (0 = none, at most 128), range, kernel width
+ * and sampling interval. */
+int gdb_adj_setup(gdb_adj *h, const float box[3], const int32_t *ptype, const float *mass, float dt, int steps,
+                  int checkpoint_every, int rdf_bins, float rdf_lo, float rdf_hi, float rdf_width, int rdf_every);
+/* params: ntypes*ntypes rows of (sigma, epsilon, cut) as double, symmetric;
+ * r0, v0: (n, 3) float32 host arrays.  obs: 3 + rdf_bins doubles. */
+int gdb_adj_forward(gdb_adj *h, const double *params, const float *r0, const float *v0, double *obs);
+/* grad_obs: dL/dobs (3 + rdf_bins doubles) -> grad_params, ntypes*ntypes rows
+ * of (dL/dsigma, dL/depsilon, 0); entry (a, b) holds the derivative with
+ * respect to the shared parameter of the unordered pair {a, b}. */
+int gdb_adj_backward(gdb_adj *h, const double *grad_obs, double *grad_params);
+/* State after the forward's last step (either pointer may be NULL). */
+int gdb_adj_final_state(gdb_adj *h, float *r, float *v);
+int gdb_adj_get_last_error(gdb_adj *h, char *buf, int n);
+
 #ifdef __cplusplus
 }
 #endif
