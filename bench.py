@@ -48,7 +48,7 @@ def parse():
                    help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
     p.add_argument("--tp", type=int, default=0, help="lanes per particle (0 = library default)")
     p.add_argument("--trace", action="store_true", help="with --profile: phase trace of the persistent kernel")
-    p.add_argument("--workload", default="ka", choices=["ka", "batch"],
+    p.add_argument("--workload", default="ka", choices=["ka", "batch", "adjoint"],
                    help="ka: one KA system of --n particles; batch: --replicas KA replicas of uneven N, "
                         "density and temperature advanced together, against the same replicas run one by one")
     p.add_argument("--replicas", type=int, default=128)
@@ -322,6 +322,99 @@ def run_batch(args):
         pg.destroy_process_group()
 
 
+def run_adjoint(args):
+    """Adjoint workload: KA N=4096, rho 1.2, T 0.6, an NVE trajectory of
+    --steps steps (2000 by default) with checkpoints every 50; loss = squared
+    deviations of <U>/N and P plus the L2 distance of the soft A-A g(r) from
+    targets made at eps_AB = 1.45, sigma_AB = 0.82; one gradient with respect
+    to the 6 pair parameters per timed iteration."""
+    import torch
+
+    from gamdpy_b200 import adjoint, workloads
+    rank, world, local, pg = dist_setup(args)
+    n = 4096
+    steps = args.steps
+    conf = workloads.ka_configuration(n, rho=1.2, temperature=0.6, seed=77 + rank)
+    rdf = {"bins": 40, "r_lo": 0.7, "r_hi": 2.7, "width": 0.05, "every": 10}
+    cut = workloads.KA_CUT.astype(np.float64)
+    eng = adjoint.AdjointNVE(conf, cut, dt=0.005, steps=steps, checkpoint_every=50, rdf=rdf, device=local)
+
+    def theta(eps_ab, sig_ab):
+        sig = workloads.KA_SIGMA.astype(np.float64).copy()
+        eps = workloads.KA_EPSILON.astype(np.float64).copy()
+        sig[0, 1] = sig[1, 0] = sig_ab
+        eps[0, 1] = eps[1, 0] = eps_ab
+        return adjoint.theta_from_tables(sig, eps)
+
+    target = torch.tensor(eng.forward(theta(1.45, 0.82)))
+    vol = float(np.prod(conf.simbox.lengths))
+    dr = (rdf["r_hi"] - rdf["r_lo"]) / rdf["bins"]
+
+    def gradient():
+        th = torch.tensor(theta(1.5, 0.8), requires_grad=True)
+        loss = adjoint.matching_loss(eng.observables(th), target, n, vol, dr)
+        loss.backward()
+        return float(loss), th.grad.detach().numpy().copy()
+
+    for _ in range(max(1, min(args.warmup, 3))):
+        gradient()
+    reps = max(1, min(args.steps // 1000, 3)) if args.steps >= 1000 else 3
+    t0 = time.perf_counter()
+    tf = 0.0
+    for _ in range(reps):
+        t1 = time.perf_counter()
+        eng.forward(theta(1.5, 0.8))
+        tf += time.perf_counter() - t1
+    t_fwd = tf / reps
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        loss, g = gradient()
+    t_grad = (time.perf_counter() - t0) / reps
+    # truncated adjoint (window of 100 steps) on the same trajectory, and the
+    # growth of the exact gradient with the horizon (chaos: ~exp(lambda t))
+    eng.set_window(100)
+    loss_w, g_w = gradient()
+    eng.set_window(0)
+    growth = {}
+    for t in (50, 100, 200, 400, 800):
+        e2 = adjoint.AdjointNVE(conf, cut, dt=0.005, steps=t, checkpoint_every=50, rdf=rdf, device=local)
+        tgt = torch.tensor(e2.forward(theta(1.45, 0.82)))
+        th = torch.tensor(theta(1.5, 0.8), requires_grad=True)
+        adjoint.matching_loss(e2.observables(th), tgt, n, vol, dr).backward()
+        growth[str(t)] = float(np.linalg.norm(th.grad.detach().numpy()))
+    # the plain path on the same system and trajectory length (forward only)
+    c2 = workloads.ka_configuration(n, rho=1.2, temperature=0.6, seed=77 + rank)
+    sim = __import__("gamdpy_b200").Simulation(
+        c2, workloads.ka_pair_potential(), __import__("gamdpy_b200").integrators.NVE(dt=0.005), [],
+        num_timeblocks=1, steps_per_timeblock=steps, storage="memory", steps_in_kernel_test=0, device=local,
+        compute_plan={"pb": 64, "tp": 1, "lanes": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
+                      "nblist": "linked lists"})
+    sim._sim.run(0.0, steps)
+    ms_plain = sim._sim.run(0.0, steps)
+    line = {
+        "metric": "adjoint gradients/s, KA N=4096 NVE trajectory, 6 pair parameters, 1 B200",
+        "value": 1.0 / t_grad, "unit": "gradients/s", "n_gpus": world, "steps": steps, "warmup": 1,
+        "ms_per_step": t_grad * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32 forward, f64 adjoint", "data": "synthetic (seeded KA lattice)",
+        "config": {"workload": f"KA-LJ NVE N={n} rho=1.2 T=0.6, {steps} steps, checkpoints every 50, "
+                               "loss = (<U>/N, P, soft g_AA(r)) vs targets at eps_AB=1.45 sigma_AB=0.82",
+                   "rdf": rdf},
+        "forward_ms": t_fwd * 1e3, "gradient_ms": t_grad * 1e3, "backward_over_forward": (t_grad - t_fwd) / t_fwd,
+        "plain_forward_ms": ms_plain, "loss": loss, "gradient": [float(x) for x in g],
+        "gradient_window100": [float(x) for x in g_w],
+        "exact_gradient_norm_vs_steps": growth,
+        "gradient_order": "eps_AA, eps_AB, eps_BB, sigma_AA, sigma_AB, sigma_BB",
+        "e2e": {"value": 1.0 / t_grad, "unit": "gradients/s", "h2d_bytes_per_step": n * 24 / steps,
+                "d2h_bytes_per_step": 8 * (3 + rdf["bins"]) / steps,
+                "note": "host initial state in, observables and gradient out, through AdjointNVE"},
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -329,6 +422,9 @@ def main():
         return
     if args.workload == "batch":
         run_batch(args)
+        return
+    if args.workload == "adjoint":
+        run_adjoint(args)
         return
     rank, world, local, pg = dist_setup(args)
     import gamdpy_b200 as gp

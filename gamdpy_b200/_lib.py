@@ -90,6 +90,7 @@ SIGNATURES = {
     "gdb_adj_forward": ([_P, _P, _P, _P, _P], _i),
     "gdb_adj_backward": ([_P, _P, _P], _i),
     "gdb_adj_final_state": ([_P, _P, _P], _i),
+    "gdb_adj_set_window": ([_P, _i], _i),
     "gdb_adj_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
 }
 

@@ -55,7 +55,7 @@ class AdjointNVE:
     cut: (nt, nt) cutoffs (fixed).  rdf: None or dict(bins, r_lo, r_hi,
     width, every) for the type-0 soft radial distribution."""
 
-    def __init__(self, configuration, cut, dt, steps, checkpoint_every=50, rdf=None, device=0):
+    def __init__(self, configuration, cut, dt, steps, checkpoint_every=50, rdf=None, window=0, device=0):
         conf = configuration
         self.n = conf.N
         self.nt = int(np.max(conf.ptype)) + 1
@@ -79,6 +79,14 @@ class AdjointNVE:
                     "gdb_adj_setup")
         self.forward_count = 0
         self._last_theta = None
+        self.set_window(window)
+
+    def set_window(self, window):
+        """0: the exact adjoint.  W > 0: the truncated adjoint that treats the
+        state at every multiple of W steps as a constant (a trajectory of a
+        chaotic system has an exact gradient growing like exp(lambda t))."""
+        self.window = int(window)
+        self._check(_lib.lib().gdb_adj_set_window(self.h, self.window), "gdb_adj_set_window")
 
     @property
     def n_obs(self):

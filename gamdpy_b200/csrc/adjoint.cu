@@ -378,6 +378,7 @@ struct gdb_adj {
     float dt = 0.f;
     int steps = 0, ckpt = 50;
     int nbins = 0, rdf_every = 0;
+    int window = 0;  // 0: exact adjoint; W > 0: cotangents cut every W steps
     float r_lo = 0.f, r_hi = 0.f, width = 0.f;
     bool setup = false, forward_done = false;
     Tables tab{};
@@ -676,6 +677,11 @@ int gdb_adj_backward(gdb_adj *h, const double *grad_obs, double *grad_params) {
         // reverse sweep of the segment
         for (int k = len - 1; k >= 0; k--) {
             const int s = s0 + k;
+            if (h->window > 0 && (s + 1) % h->window == 0) {
+                // last step of a window: nothing flows back across its end
+                ACK(cudaMemsetAsync(h->d_R, 0, (size_t)n * 3 * sizeof(double), h->st));
+                ACK(cudaMemsetAsync(h->d_V, 0, (size_t)n * 3 * sizeof(double), h->st));
+            }
             const float4 *pn = h->d_seg_pos + (size_t)k * n;
             const float4 *vn = h->d_seg_vel + (size_t)k * n, *vn1 = h->d_seg_vel + (size_t)(k + 1) * n;
             k_adj_vtot<<<(n + 255) / 256, 256, 0, h->st>>>(n, h->dt, gK, h->d_mass, h->d_R, h->d_V, vn, vn1, h->d_Vt);
@@ -704,6 +710,12 @@ int gdb_adj_backward(gdb_adj *h, const double *grad_obs, double *grad_params) {
             grad_params[3 * k + 1] = ge;
             grad_params[3 * k + 2] = 0.0;
         }
+    return GDB_OK;
+}
+
+int gdb_adj_set_window(gdb_adj *h, int window) {
+    if (!h || window < 0) return aset(h, GDB_ERR_ARG, "gdb_adj_set_window: bad arguments");
+    h->window = window;
     return GDB_OK;
 }
 

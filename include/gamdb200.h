@@ -277,6 +277,11 @@ int gdb_adj_forward(gdb_adj *h, const double *params, const float *r0, const flo
  * of (dL/dsigma, dL/depsilon, 0); entry (a, b) holds the derivative with
  * respect to the shared parameter of the unordered pair {a, b}. */
 int gdb_adj_backward(gdb_adj *h, const double *grad_obs, double *grad_params);
+/* Truncated adjoint: window W > 0 treats the state at every multiple of W
+ * steps as a constant, so each observable term is differentiated through at
+ * most W steps of the trajectory (the exact gradient of a chaotic trajectory
+ * grows like exp(lambda t)); 0 (the default) = the exact adjoint. */
+int gdb_adj_set_window(gdb_adj *h, int window);
 /* State after the forward's last step (either pointer may be NULL). */
 int gdb_adj_final_state(gdb_adj *h, float *r, float *v);
 int gdb_adj_get_last_error(gdb_adj *h, char *buf, int n);

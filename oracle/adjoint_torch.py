@@ -75,11 +75,12 @@ def _soft_rdf_sum(rr, eye, types, rdf):
     return torch.where(mask, k, torch.zeros_like(k)).sum(0)
 
 
-def observables(theta, r0, v0, types, mass, box, cut, dt, steps, rdf=None):
+def observables(theta, r0, v0, types, mass, box, cut, dt, steps, rdf=None, window=0):
     """Time averages [<U>, <W>, <K>, <g_b>...] of the float64 trajectory.
 
     theta: torch float64 (eps of the unordered pairs, then sigma); the rest
-    numpy.  Differentiable in theta."""
+    numpy.  Differentiable in theta.  window W > 0 detaches the state at every
+    multiple of W steps (the truncated adjoint's gradient)."""
     nt = int(np.max(types)) + 1
     sig_t, eps_t = _tables(theta, nt)
     cut_t = torch.as_tensor(np.broadcast_to(np.asarray(cut, np.float64), (nt, nt)).copy())
@@ -92,6 +93,8 @@ def observables(theta, r0, v0, types, mass, box, cut, dt, steps, rdf=None):
     accG = None
     nsamp = 0
     for n in range(steps):
+        if window > 0 and n % window == 0:
+            r, v = r.detach(), v.detach()
         d, r2, rr, s, u, eye = _pair_terms(r, ty, L, sig_t, eps_t, cut_t)
         f = (s[:, :, None] * d).sum(1)
         accU = accU + 0.5 * u.sum()

@@ -141,6 +141,30 @@ def test_checkpoint_spacing_and_reruns_do_not_change_gradients():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("window,ckpt", [(10, 10), (8, 10), (15, 7)])
+def test_truncated_adjoint_matches_detached_autograd(window, ckpt):
+    """Window W: the state at multiples of W is a constant; torch.autograd
+    through the float64 forward with the same detaches is the reference."""
+    import torch
+
+    from oracle import adjoint_torch as R
+    conf = small_ka(seed=12)
+    cut = workloads.KA_CUT.astype(np.float64)
+    vol = float(np.prod(conf.simbox.lengths))
+    dr = (RDF["r_hi"] - RDF["r_lo"]) / RDF["bins"]
+    args = (conf["r"], conf["v"], conf.ptype, conf["m"], conf.simbox.lengths, cut, 0.005, 40)
+    target = R.observables(torch.tensor(ka_theta(1.45, 0.82)), *args, rdf=RDF).detach()
+    eng = adjoint.AdjointNVE(conf, cut, dt=0.005, steps=40, checkpoint_every=ckpt, rdf=RDF, window=window)
+    th = torch.tensor(ka_theta(), requires_grad=True)
+    adjoint.matching_loss(eng.observables(th), target, conf.N, vol, dr).backward()
+    th_ref = torch.tensor(ka_theta(), requires_grad=True)
+    adjoint.matching_loss(R.observables(th_ref, *args, rdf=RDF, window=window), target, conf.N, vol,
+                          dr).backward()
+    g, g_ref = th.grad.numpy(), th_ref.grad.numpy()
+    assert np.linalg.norm(g - g_ref) <= GRAD_TOL * np.linalg.norm(g_ref), (g, g_ref)
+
+
+@pytest.mark.gpu
 def test_backward_after_another_forward_reruns_the_forward():
     import torch
     conf = small_ka(seed=9)
