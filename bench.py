@@ -48,7 +48,7 @@ def parse():
                    help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
     p.add_argument("--tp", type=int, default=0, help="lanes per particle (0 = library default)")
     p.add_argument("--trace", action="store_true", help="with --profile: phase trace of the persistent kernel")
-    p.add_argument("--workload", default="ka", choices=["ka", "batch", "adjoint"],
+    p.add_argument("--workload", default="ka", choices=["ka", "lj2048", "batch", "adjoint"],
                    help="ka: one KA system of --n particles; batch: --replicas KA replicas of uneven N, "
                         "density and temperature advanced together, against the same replicas run one by one")
     p.add_argument("--replicas", type=int, default=128)
@@ -322,6 +322,59 @@ def run_batch(args):
         pg.destroy_process_group()
 
 
+def run_lj_small(args):
+    """The reference's small plain case: single-component LJ (shifted force,
+    rc = 2.5), FCC 8x8x8 = 2048 particles at rho = 0.973, Maxwell-Boltzmann
+    velocities at T = 0.7 (seeded), NVE dt = 0.005, N^2 list with skin 0.5.
+    TPS and MATS over the timeblocks' device time."""
+    import gamdpy_b200 as gp
+    from gamdpy_b200 import workloads
+    rank, world, local, pg = dist_setup(args)
+    conf = workloads.lj_configuration([8, 8, 8], 0.973, 0.7, seed=rank)
+    n = conf.N
+    pp = workloads.lj_pair_potential(cut=2.5, shifted_force=True, max_num_nbs=300)
+    block = min(args.block, max(1, args.steps))
+    nblocks = max(1, args.steps // block)
+    steps = nblocks * block
+    plan = {"pb": 8, "tp": 16, "lanes": args.tp, "skin": 0.5, "UtilizeNIII": False, "gridsync": True,
+            "nblist": "N squared"}
+    sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.005), [gp.MomentumReset(100)], num_timeblocks=nblocks,
+                        steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
+    dev = sim._sim
+    dev.run(0.0, max(3, args.warmup))
+    barrier(pg)
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = sum(dev.run(float(b * block * 0.005), block) for b in range(nblocks))
+    clock_info = clocks.stop()
+    t_max = allreduce_max(pg, ms / 1e3, local)
+    e2e_blocks = max(1, min(nblocks, 4))
+    t0 = time.perf_counter()
+    conf.copy_to_device()
+    for b in range(e2e_blocks):
+        dev.run(float(b * block * 0.005), block)
+        conf.copy_to_host()
+    e2e_s = allreduce_max(pg, time.perf_counter() - t0, local)
+    tps = steps / t_max
+    line = {
+        "metric": "TPS (time steps/s), LJ N=2048 NVE N^2 list, 1 B200", "value": tps * world, "unit": "steps/s",
+        "n_gpus": world, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded FCC lattice)",
+        "config": {"workload": "LJ SF rc=2.5, FCC 8x8x8 N=2048 rho=0.973 T=0.7, NVE dt=0.005, N^2 list skin 0.5",
+                   "n": n, "mats": n * tps * world / 1e6, "timeblock_steps": block, "path": dev.last_path(),
+                   "l2": "working set < L2; the metric is step latency, so no flush"},
+        "e2e": {"value": e2e_blocks * block * world / e2e_s, "unit": "steps/s",
+                "h2d_bytes_per_step": n * 44 / (e2e_blocks * block), "d2h_bytes_per_step": n * 68 / block},
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def run_adjoint(args):
     """Adjoint workload: KA N=4096, rho 1.2, T 0.6, an NVE trajectory of
     --steps steps (2000 by default) with checkpoints every 50; loss = squared
@@ -425,6 +478,9 @@ def main():
         return
     if args.workload == "adjoint":
         run_adjoint(args)
+        return
+    if args.workload == "lj2048":
+        run_lj_small(args)
         return
     rank, world, local, pg = dist_setup(args)
     import gamdpy_b200 as gp

@@ -1,7 +1,7 @@
 // md_cluster.cu -- small systems (N <= 4096) resident in one thread-block
 // cluster, and many of them at once (batched replicas).
 //
-// One cluster of C CTAs (1024 threads each, one per SM) owns one system for a
+// One cluster of C CTAs (512 threads each, one per SM) owns one system for a
 // whole timeblock:
 //   * every CTA holds all N positions in shared memory; after each step a CTA
 //     sends the new positions of its own particles to every CTA of the
@@ -9,10 +9,12 @@
 //   * each CTA owns P = ceil(N / C) particles; their neighbour lists (uint16
 //     indices, chunks of four) live in its shared memory; velocities, images
 //     and the build reference positions stay in registers across steps;
-//   * steps are separated by hardware cluster barriers; the per-CTA float64
-//     partial sums are read by every CTA from the others' shared memory in a
-//     fixed order, so every CTA computes the same thermostat update, flags and
-//     sums without another round trip.
+//   * steps are separated by hardware cluster barriers -- one per step when
+//     two position copies fit (new positions go straight into every CTA's
+//     other copy), two otherwise; the per-CTA float64 partial sums (only
+//     those a step needs) are read by every CTA from the others' shared
+//     memory in a fixed order, so every CTA computes the same thermostat
+//     update, flags and sums without another round trip.
 // Global memory is read at the start of a timeblock and written at its end
 // (plus ScalarSaver rows and ConfigurationSaver frames).  Lists are built in
 // shared memory over the cell grid of the global cell build (counting sort of
@@ -40,9 +42,10 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
     __shared__ double s_red[NQ * 32];
     __shared__ int s_flag[4];
+    __shared__ double s_lmax;
+    __shared__ double s_gather[16][CL_NQ];
     __shared__ int s_seg_lo[CL_THREADS / 32][64];
     __shared__ int s_seg_pre[CL_THREADS / 32][64];
-    __shared__ double s_gather[16][CL_NQ];
     cg::cluster_group cl = cg::this_cluster();
     const int C = (int)cl.num_blocks();
     const int rank = (int)cl.block_rank();
@@ -55,18 +58,23 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     const int ncell = ncx * ncy * ncz;
     const bool use_cells = ncell > 0 && ncell <= CL_MAX_CELLS;
     const int cap = job.cap;
-    const ClusterSmem L = cluster_smem_layout(n, P, use_cells ? ncell : 0, cap);
+    const bool pp = job.pingpong != 0;
+    const bool sorted = use_cells && job.sorted != 0;
+    const ClusterSmem L = cluster_smem_layout(n, P, use_cells ? ncell : 0, cap, job.pingpong, job.sorted);
     int *scs = reinterpret_cast<int *>(smem + L.cstart);
     unsigned short *scell = reinterpret_cast<unsigned short *>(smem + L.cell);
     unsigned short *srank = reinterpret_cast<unsigned short *>(smem + L.crank);
     unsigned short *sperm = reinterpret_cast<unsigned short *>(smem + L.cperm);
-    float4 *spos = reinterpret_cast<float4 *>(smem + L.pos);
+    float4 *const sposA = reinterpret_cast<float4 *>(smem + L.pos);
+    float4 *const sposB = pp ? reinterpret_cast<float4 *>(smem + L.pos2) : sposA;
+    float4 *spos = sposA;  // the current positions
     float4 *snew = reinterpret_cast<float4 *>(smem + L.newp);
+    float4 *ssort = reinterpret_cast<float4 *>(smem + L.sorted);
     unsigned short *snbl = reinterpret_cast<unsigned short *>(smem + L.nbl);
     int *snbc = reinterpret_cast<int *>(smem + L.nbc);
     double *spart = reinterpret_cast<double *>(smem + L.part);
     double *stot = reinterpret_cast<double *>(smem + L.tot);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int p0 = rank * P;
     const int np = max(0, min(P, n - p0));
     const int lp = tid / TP, sub = tid % TP;
@@ -99,15 +107,15 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz;
     const float ilx = 1.0f / Lx, ily = 1.0f / Ly, ilz = 1.0f / Lz;
     // cluster-wide maximum of a per-thread value (called by every thread)
-    auto cluster_max = [&](int v) -> int {
-        v = __reduce_max_sync(0xffffffffu, v);
+    auto cluster_max = [&](int val) -> int {
+        val = __reduce_max_sync(0xffffffffu, val);
         if (tid == 0) s_flag[0] = 0;
         __syncthreads();
-        if (lane == 0) atomicMax(&s_flag[0], v);
+        if (lane == 0) atomicMax(&s_flag[0], val);
         __syncthreads();
-        if (tid == 0) spart[NQ + 1] = (double)s_flag[0];
+        if (tid == 0) s_lmax = (double)s_flag[0];
         cl.sync();
-        if (tid < C) s_gather[tid][0] = cl.map_shared_rank(spart, tid)[NQ + 1];
+        if (tid < C) s_gather[tid][0] = *cl.map_shared_rank(&s_lmax, tid);
         __syncthreads();
         if (tid == 0) {
             int m = 0;
@@ -126,7 +134,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     // build (on either path) left them.
     if (!rebuild) {
         int lmax = 0;
-        for (int q = warp; q < np; q += CL_THREADS / 32) {
+        for (int q = tid >> 5; q < np; q += CL_THREADS / 32) {
             int cnt = a.nbc[p0 + q];
             const int lim = min(min(cnt, cap), a.max_nbs);
             bool bad = false;
@@ -155,9 +163,10 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
         // ---- neighbour list from shared memory -----------------------------
         // Every CTA bins all N particles into the cell grid of the global
         // build (nblist_linked_lists.py:36-39, :127), orders each cell by
-        // index, and builds the lists of its own particles over the 5x5x5
-        // stencil (warp per particle, ballot append).  Grids with more than
-        // CL_MAX_CELLS cells build N^2.  Same exact distance: same sets.
+        // index, copies the positions into cell order and builds the lists of
+        // its own particles over the 5x5x5 stencil (a warp per particle,
+        // candidates in stencil-row order as the global builds).  Grids with
+        // more than CL_MAX_CELLS cells build N^2.
         if (rebuild) {
             int lmax = 0;
             if (use_cells) {
@@ -172,7 +181,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                 }
                 __syncthreads();
                 // exclusive scan of the counts (one warp, 32-wide chunks)
-                if (warp == 0) {
+                if (tid < 32) {
                     int carry = 0;
                     for (int base = 0; base <= ncell; base += 32) {
                         const int c = base + lane;
@@ -204,13 +213,22 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                 }
                 __syncthreads();
                 trace_mark(ctrl, TR_REBUILD_PHASE);
-                // per particle: the x-contiguous ranges of the 25 stencil rows
-                // (two at the x wrap; whole rows for grids under 5 cells),
-                // walked as one packed candidate sequence, 32 per iteration
+                // positions in cell order: the candidates of a stencil row
+                // are one contiguous run, read conflict-free by a warp
+                if (sorted) {
+                    for (int x = tid; x < n; x += CL_THREADS) ssort[x] = spos[sperm[x]];
+                    __syncthreads();
+                }
+                // per particle (a warp each): the x-contiguous ranges of the 25
+                // stencil rows (two at the x wrap; whole rows for grids under 5
+                // cells), walked as one packed candidate sequence, 32 at a time,
+                // ballot-appended in order
                 const int ry = ncy < 5 ? ncy : 5, rz = ncz < 5 ? ncz : 5;
                 const int nrows = ry * rz, nseg = 2 * nrows;
-                int *lo_s = s_seg_lo[warp], *pre_s = s_seg_pre[warp];
-                for (int q = warp; q < np; q += CL_THREADS / 32) {
+                const float cps2 = a.cps2;
+                const bool fma = a.fma != 0;
+                int *lo_s = s_seg_lo[tid >> 5], *pre_s = s_seg_pre[tid >> 5];
+                for (int q = tid >> 5; q < np; q += CL_THREADS / 32) {
                     const int ii = p0 + q;
                     const float4 pi = spos[ii];
                     const int c = scell[ii];
@@ -271,11 +289,13 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                         int j = 0;
                         if (vv < T) {
                             while (seg + 1 < nseg && pre_s[seg + 1] <= vv) seg++;
-                            j = sperm[lo_s[seg] + (vv - pre_s[seg])];
+                            const int x = lo_s[seg] + (vv - pre_s[seg]);
+                            j = sperm[x];
+                            const float4 pj = sorted ? ssort[x] : spos[j];
                             if (j != ii) {
-                                const float d2 = a.fma ? dist_sq_exact<true>(spos[j], pi, Lx, Ly, Lz)
-                                                       : dist_sq_exact<false>(spos[j], pi, Lx, Ly, Lz);
-                                hit = d2 < a.cps2;
+                                const float d2 = fma ? dist_sq_exact<true>(pj, pi, Lx, Ly, Lz)
+                                                     : dist_sq_exact<false>(pj, pi, Lx, Ly, Lz);
+                                hit = d2 < cps2;
                             }
                         }
                         const unsigned m = __ballot_sync(0xffffffffu, hit);
@@ -290,7 +310,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                     lmax = max(lmax, count);
                 }
             } else {
-                for (int q = warp; q < np; q += CL_THREADS / 32) {
+                for (int q = tid >> 5; q < np; q += CL_THREADS / 32) {
                     const int ii = p0 + q;
                     const float4 pi = spos[ii];
                     int count = 0;
@@ -389,6 +409,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
 #pragma unroll
         for (int q = 0; q < NQ; q++) red[q] = 0.0;
         bool moved = false;
+        float4 *const sother = (spos == sposA) ? sposB : sposA;  // next positions (ping-pong)
         if (owner) {
             const float fsq = fx * fx + fy * fy + fz * fz;
             const size_t N = n;
@@ -463,29 +484,55 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                 }
             }
         }
-        const int any_moved = __syncthreads_or(moved);
-        block_sum<NQ>(red, s_red);
+        // ---- block partials: only the sums this step needs ----------------
+        // every sum on saved and reset steps, the kinetic energy of the
+        // thermostat (NVT) otherwise, and always the rebuild flag
+        const bool full = rec || reset;
+        const bool needk = full || INTEG == GDB_INTEGRATOR_NVT;
+        double *slot = spart + (pp ? (s & 1) : 0) * CL_NQ;
+        const int any_moved = __syncthreads_or(moved);  // also orders snew before the copies below
+        if (full) {
+            block_sum<NQ>(red, s_red);
+        } else if (needk) {
+            double rk[1] = {red[0]};
+            block_sum<1>(rk, s_red);
+            red[0] = rk[0];
+        }
         if (tid == 0) {
+            if (full) {
 #pragma unroll
-            for (int q = 0; q < NQ; q++) spart[q] = red[q];
-            spart[NQ] = any_moved ? 1.0 : 0.0;
+                for (int q = 0; q < NQ; q++) slot[q] = red[q];
+            } else if (needk) {
+                slot[0] = red[0];
+            }
+            slot[NQ] = any_moved ? 1.0 : 0.0;
+        }
+        // with two position copies, the new positions go straight into every
+        // CTA's other copy, read only after the barrier below
+        if (pp && !eval) {
+            for (int k = tid; k < np * C; k += CL_THREADS) {
+                const int r = k / np, q = k - r * np;
+                cl.map_shared_rank(sother, r)[p0 + q] = snew[q];
+            }
         }
         trace_mark(ctrl, TR_STEP_PHASE);
-        cl.sync();  // every force phase done, every partial written
-        // ---- broadcast new positions, fixed-order totals ------------------
-        if (!eval) {
+        cl.sync();  // every force phase done, every partial written (and, ping-pong, every position)
+        if (!pp && !eval) {
             for (int k = tid; k < np * C; k += CL_THREADS) {
-                const int r = k / np, q = k % np;
+                const int r = k / np, q = k - r * np;
                 cl.map_shared_rank(spos, r)[p0 + q] = snew[q];
             }
         }
-        // one remote load per thread, then a fixed-order local sum
-        if (tid < C * (NQ + 1)) {
-            const int r = tid / (NQ + 1), q = tid % (NQ + 1);
-            s_gather[r][q] = cl.map_shared_rank(spart, r)[q];
+        // the needed partials of every CTA, one remote load per thread, then
+        // a fixed-order local sum
+        const int ng = full ? NQ + 1 : (needk ? 2 : 1);
+        if (tid < C * ng) {
+            const int r = tid / ng, g = tid - r * ng;
+            const int q = full ? g : (g == ng - 1 ? NQ : 0);
+            s_gather[r][q] = cl.map_shared_rank(slot, r)[q];
         }
         __syncthreads();
-        if (tid < NQ + 1) {
+        if (tid < NQ + 1 && (full || tid == NQ || (needk && tid == 0))) {
             double acc = 0.0;
             for (int r = 0; r < C; r++) acc += s_gather[r][tid];
             stot[tid] = acc;
@@ -512,12 +559,16 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                 v.z -= (float)(stot[7] / stot[8]);
             }
             rebuild = stot[NQ] > 0.0;
-            if (rank == 0 && tid == 0) ctrl->sumK = (float)stot[0];
+            if (rank == 0 && tid == 0 && needk) ctrl->sumK = (float)stot[0];
         } else if (rank == 0 && tid == 0) {
             ctrl->evalU = stot[1];
             ctrl->evalW = stot[2];
         }
-        cl.sync();  // positions delivered; partial slots free again
+        if (pp) {
+            if (!eval) spos = sother;
+        } else {
+            cl.sync();  // positions delivered; the partial slot is free again
+        }
         trace_mark(ctrl, eval ? TR_EVAL : TR_STEP);
     }
 
@@ -537,7 +588,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     }
     // lists in the global chunked layout (int indices), for gdb_get_nblist
     if (nbuild > 0) {
-        for (int q = warp; q < np; q += CL_THREADS / 32) {
+        for (int q = tid >> 5; q < np; q += CL_THREADS / 32) {
             const int cnt = snbc[q];
             const int lim = min(min(cnt, cap), a.max_nbs);
             for (int k = lane; k < lim; k += 32) a.nbl[nbl_index(p0 + q, k, a.stride)] = snbl[cl_nbl_index(q, k, P)];
@@ -594,16 +645,23 @@ void cluster_shape(int n, int target, int *C, int *tp) {
     *tp = t;
 }
 
-bool cluster_plan(int n, int C, int ncell, int max_nbs, int *cap, size_t *smem) {
+bool cluster_plan(int n, int C, int ncell, int max_nbs, int *cap, int *pingpong, int *sorted, size_t *smem) {
     const int P = (n + C - 1) / C;
     const int nc = ncell > 0 && ncell <= CL_MAX_CELLS ? ncell : 0;
-    int c = std::min((std::max(max_nbs, 4) + 3) & ~3, CL_CAP_MAX);
-    for (; c >= 64; c -= 16) {
-        const size_t bytes = cluster_smem_layout(n, P, nc, c).total;
-        if (bytes <= CL_SMEM_LIMIT) {
-            *cap = c;
-            *smem = bytes;
-            return true;
+    const int want = std::min((std::max(max_nbs, 4) + 3) & ~3, CL_CAP_MAX);
+    const int opts[3][2] = {{1, 1}, {0, 1}, {0, 0}};  // (pingpong, sorted), best first
+    for (int o = 0; o < 3; o++) {
+        const int pp = opts[o][0], so = opts[o][1];
+        const int floor_cap = o < 2 ? std::min(want, 160) : 64;
+        for (int c = want; c >= floor_cap; c -= 4) {
+            const size_t bytes = cluster_smem_layout(n, P, nc, c, pp, so).total;
+            if (bytes <= CL_SMEM_LIMIT) {
+                *cap = c;
+                *pingpong = pp;
+                *sorted = so;
+                *smem = bytes;
+                return true;
+            }
         }
     }
     return false;

@@ -563,9 +563,9 @@ static int run_cluster(gdb_sim *h, int steps) {
     a.ncy = nc[1];
     a.ncz = nc[2];
     const int ncell = nc[0] * nc[1] * nc[2];
-    int cap;
+    int cap, pingpong, sorted;
     size_t smem;
-    if (!cluster_plan(h->n, C, ncell, h->max_nbs, &cap, &smem)) {
+    if (!cluster_plan(h->n, C, ncell, h->max_nbs, &cap, &pingpong, &sorted, &smem)) {
         h->cluster_ok = false;
         return GDB_ERR_UNSUPPORTED;
     }
@@ -579,6 +579,8 @@ static int run_cluster(gdb_sim *h, int steps) {
     h->h_job->cur = h->cur;
     h->h_job->step0 = 0;
     h->h_job->cap = cap;
+    h->h_job->pingpong = pingpong;
+    h->h_job->sorted = sorted;
     CK(cudaMemcpyAsync(h->d_job, h->h_job, sizeof(ClusterJob), cudaMemcpyHostToDevice, h->st));
     cudaError_t e = launch_clusters(h->d_job, 1, C, tp, h->ntypes, h->integ, smem, steps, 1, h->st);
     if (e != cudaSuccess) {
@@ -1175,7 +1177,7 @@ struct gdb_batch {
         int kind = 0;  // 0 shared-memory clusters, 1 global-memory clusters
         int C = 0, tp = 0;
         size_t smem = 0;
-        std::vector<int> idx, cap;
+        std::vector<int> idx, cap, pp;
         void *d_jobs = nullptr, *h_jobs = nullptr;
         cudaStream_t st = nullptr;
         cudaEvent_t done = nullptr;
@@ -1308,14 +1310,15 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
         gdb_sim *h = sims[k];
         int nc[3];
         cluster_grid_of(h, nc);
-        int C, tp, cap;
+        int C, tp, cap, pingpong, sorted;
         size_t smem;
         cluster_shape(h->n, particles_per_cta, &C, &tp);
         if (h->cluster_ok && h->n <= CL_MAX_N &&
-            cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &smem)) {
+            cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &pingpong, &sorted, &smem)) {
             gdb_batch::Group *g = batch_group(b, 0, C, tp);
             g->idx.push_back(k);
             g->cap.push_back(cap);
+            g->pp.push_back(pingpong | (sorted << 1));
             g->smem = std::max(g->smem, smem);
         } else if (h->n <= CLG_MAX_N) {
             // about 1024 particles per CTA (one lane each), 4 to 16 CTAs
@@ -1324,6 +1327,7 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
             gdb_batch::Group *g = batch_group(b, 1, c, b->clg_tp);
             g->idx.push_back(k);
             g->cap.push_back(0);
+            g->pp.push_back(0);
         } else {
             b->solo.push_back(k);
         }
@@ -1390,6 +1394,8 @@ int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
                 j.cur = h->cur;
                 j.step0 = 0;
                 j.cap = g.cap[q];
+                j.pingpong = g.pp[q] & 1;
+                j.sorted = (g.pp[q] >> 1) & 1;
             } else {
                 ClusterRunJob &j = static_cast<ClusterRunJob *>(g.h_jobs)[q];
                 j.a = a;
