@@ -196,6 +196,7 @@ __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
     for (int g = 0; g < 64; g++) ctrl->bar_group[g] = 0;
     ctrl->abort = 0;
     ctrl->ticket = 0;
+    ctrl->work[0] = ctrl->work[1] = 0;
     if (ctrl->rebuild_next) {
         ctrl->rebuild = 1;
         ctrl->rebuild_next = 0;

@@ -118,6 +118,7 @@ __device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int n
     __shared__ NbScratch<WPB> scr;
     DevCtrl *ctrl = a.ctrl;
     int cur = cur0;
+    const int rounds = (a.n + (int)blockDim.x / TP - 1) / ((int)blockDim.x / TP);  // partial rows per step
     trace_mark(ctrl, TR_START);
     for (int s = 0; s < nsteps + do_eval; s++) {
         if (*(volatile int *)&ctrl->rebuild) {
@@ -131,7 +132,7 @@ __device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int n
             phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g);
             trace_mark(ctrl, TR_STEP_PHASE);
             ok = sync(ctrl, [&] {
-                finalize_step<MODE_STEP>(a, step, g.nb, s_red);
+                finalize_step<MODE_STEP>(a, step, rounds, s_red);
                 if (threadIdx.x == 0 && ctrl->rebuild_next) {
                     ctrl->rebuild = 1;
                     ctrl->rebuild_next = 0;
@@ -141,7 +142,10 @@ __device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int n
             trace_mark(ctrl, TR_STEP);
         } else {
             phase_step<TP, NT, INTEG, MODE_EVAL, false, true>(a, s_tab, nt, cur, step, s_red, g);
-            ok = sync(ctrl, [&] { finalize_step<MODE_EVAL>(a, step, g.nb, s_red); });
+            ok = sync(ctrl, [&] {
+                finalize_step<MODE_EVAL>(a, step, rounds, s_red);
+                if (threadIdx.x == 0) ctrl->work[(step + 1) & 1] = 0;
+            });
             trace_mark(ctrl, TR_EVAL);
         }
         if (!ok) return;

@@ -784,9 +784,15 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
 }
 
 // Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
-// only (MODE_EVAL).  Each block accumulates float64 partial sums over all the
-// particles it handles and writes them to partials[g.b].  Sets the
-// rebuild flag when a particle has moved more than skin/2 since the build.
+// only (MODE_EVAL).  A round is blockDim/TP consecutive particles.
+// Standalone launches (PERSIST false) take rounds g.b, g.b + g.nb, ... and
+// write one float64 partial row per block to partials[g.b].  The persistent
+// kernels (PERSIST true) hand rounds out through an atomic counter (blocks on
+// faster SMs take more) and write one row per round to partials[round], so
+// the fixed-order sum does not depend on which block ran which round.  Only
+// the sums the step needs are reduced: all of them on saved and reset steps,
+// the kinetic energy (NVT) otherwise.  Sets the rebuild flag when a particle
+// has moved more than skin/2 since the build.
 template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
 __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
                                   Span g = grid_span()) {
@@ -807,11 +813,20 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
     const size_t n = a.n;
     const int per_block = blockDim.x / TP;
     const int rounds_total = (a.n + per_block - 1) / per_block;
+    const bool full = rec || reset;
+    const bool needk = full || INTEG == GDB_INTEGRATOR_NVT;
     double red[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) red[q] = 0.0;
     bool moved = false;
-    for (int round = g.b; round < rounds_total; round += g.nb) {
+    __shared__ int s_round;
+    int round = g.b;
+    if (PERSIST) {
+        if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
+        __syncthreads();
+        round = s_round;
+    }
+    while (round < rounds_total) {
         const int i = round * per_block + threadIdx.x / TP;
         const int sub = threadIdx.x % TP;
         const bool active = i < a.n;
@@ -844,7 +859,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
                 }
             }
         }
-        if (!(active && sub == 0)) continue;
+        if (active && sub == 0) {
         // ConfigurationSaver: frame taken before this step's integration
         if (a.conf) {
             const int si = conf_save_index(step);
@@ -879,8 +894,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
         if (MODE == MODE_EVAL) {
             a.frc[i] = make_float4(fx, fy, fz, 0.f);
             if (shift_pending) a.vel[i] = v;
-            continue;
-        }
+        } else {
         const float m = v.w;
         float kin = 0.f;
         float r[3] = {pi.x, pi.y, pi.z};
@@ -947,6 +961,30 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
             red[7] += (double)m * vv[2];
             red[8] += m;
         }
+        }  // MODE_STEP
+        }  // integrating lane
+        if (PERSIST) {
+            // this round's sums to partials[round]; the next round
+            if (full) {
+                block_sum<NQ>(red, s_red);
+                if (threadIdx.x == 0) {
+#pragma unroll
+                    for (int q = 0; q < NQ; q++) a.partials[(size_t)round * NQ + q] = red[q];
+                }
+            } else if (needk) {
+                double rk[1] = {red[0]};
+                block_sum<1>(rk, s_red);
+                if (threadIdx.x == 0) a.partials[(size_t)round * NQ] = rk[0];
+            }
+#pragma unroll
+            for (int q = 0; q < NQ; q++) red[q] = 0.0;
+            __syncthreads();  // every thread has read s_round
+            if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
+            __syncthreads();
+            round = s_round;
+        } else {
+            round += g.nb;
+        }
     }
     if (MODE == MODE_STEP) {
         // inside the persistent kernel other blocks may still be reading
@@ -958,14 +996,16 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
                 ctrl->rebuild = 1;
         }
     }
-    block_sum<NQ>(red, s_red);
-    if (threadIdx.x == 0) {
+    if (!PERSIST) {
+        block_sum<NQ>(red, s_red);
+        if (threadIdx.x == 0) {
 #pragma unroll
-        for (int q = 0; q < NQ; q++) a.partials[(size_t)g.b * NQ + q] = red[q];
+            for (int q = 0; q < NQ; q++) a.partials[(size_t)g.b * NQ + q] = red[q];
+        }
     }
 }
 
-// Fixed-order float64 sum of the partials of `nblocks` blocks and the
+// Fixed-order float64 sum of `nblocks` partial rows (blocks or rounds) and the
 // bookkeeping of a finished step (NVT.py:226-237, scalar_saver.py:274-288,
 // momentum_reset.py:379-393).  Run by one whole block.
 template <int MODE>
@@ -974,14 +1014,23 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
     const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
     const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
     const int par = step & 1, ppar = par ^ 1;
+    const bool full = rec || reset;
+    const bool needk = full || a.omega2 > 0.f;
     double tot[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) tot[q] = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+    if (full) {
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
 #pragma unroll
-        for (int q = 0; q < NQ; q++) tot[q] += __ldcg(a.partials + (size_t)b * NQ + q);
+            for (int q = 0; q < NQ; q++) tot[q] += __ldcg(a.partials + (size_t)b * NQ + q);
+        }
+        block_sum<NQ>(tot, s_red);
+    } else if (needk) {
+        double t1[1] = {0.0};
+        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) t1[0] += __ldcg(a.partials + (size_t)b * NQ);
+        block_sum<1>(t1, s_red);
+        tot[0] = t1[0];
     }
-    block_sum<NQ>(tot, s_red);
     if (threadIdx.x == 0) {
         if (MODE == MODE_STEP) {
             const double time = ctrl->time_zero + (double)step * (double)a.dt;
@@ -1006,6 +1055,7 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
                 ctrl->pending[par] = 1;
             }
             ctrl->step = step + 1;
+            ctrl->work[(step + 1) & 1] = 0;  // round counter of the next step (persistent kernels)
         } else {
             ctrl->evalU = tot[1];
             ctrl->evalW = tot[2];
