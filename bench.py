@@ -108,6 +108,10 @@ class ClockSampler:
                  "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # sampling is running before the timed region starts
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0 and self.proc.poll() is None:
+                time.sleep(0.02)
         except OSError:
             self.proc = None
 
@@ -125,7 +129,9 @@ class ClockSampler:
             self.proc.kill()
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        # the first sample was taken before the timed region started
+        lines = self.lines[1:] if len(self.lines) > 1 else self.lines
+        for line in lines:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) < 9:
                 continue
@@ -150,9 +156,9 @@ def measured_peak_hbm():
 
 
 def ncu_traffic_per_atom_step():
-    """DRAM bytes per atom-step of the step kernel from the committed ncu
-    summary (profiles/step_kernel_ka.txt, line 'traffic_bytes_per_atom_step')."""
-    path = os.path.join(ROOT, "profiles", "step_kernel_ka.txt")
+    """DRAM bytes per atom-step of k_run (rebuilds included) from the committed
+    ncu summary (profiles/run_kernel_ka.txt, line 'traffic_bytes_per_atom_step')."""
+    path = os.path.join(ROOT, "profiles", "run_kernel_ka.txt")
     try:
         with open(path) as f:
             for line in f:
@@ -546,19 +552,24 @@ def main():
            "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
            "timeblock_steps": block, "note": "upload once + per-timeblock device->host copy of the state"}
 
-    # ---- roofline of the fused step kernel --------------------------------
+    # ---- roofline of the dominant kernel: k_run, one launch per timeblock --
+    # (block steps + the final evaluation, rebuilds included).  Algorithmic
+    # bytes per atom-step B = 4 n + 64 (one index per stored neighbour, float4
+    # r and v read and written); per launch B * N * block.  The launch time is
+    # the timeblock's CUDA-event time on the library's stream (the events
+    # bracket k_block_begin + k_run, nothing else runs on that stream).
     mean_nbs, max_nbs = dev.nblist_stats()
-    reps = 50
-    ms_launch = dev.time_step_kernel(reps)
     bytes_per_atom = 4.0 * mean_nbs + 64.0
-    achieved = bytes_per_atom * n / (ms_launch * 1e-3) / 1e9
+    ms_launch = t_max * 1e3 / nblocks
+    achieved = bytes_per_atom * n * block / (ms_launch * 1e-3) / 1e9
     peak, peak_kind = measured_peak_hbm()
     traffic = ncu_traffic_per_atom_step()
+    # the fused step alone (standalone k_step, no rebuild), for comparison
+    ms_step_only = dev.time_step_kernel(50)
 
-    # launches inside the timed region: per step the fused kernel + the
-    # 9-kernel rebuild chain (gated), per block the final evaluation with its
-    # chain, the block-begin kernel
-    launches_per_block = block * 10 + 10 + 1
+    # launches inside the timed region: per timeblock k_block_begin and the
+    # persistent k_run
+    launches_per_block = 2
     line = {
         "metric": METRIC, "value": mats, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / steps, "higher_is_better": True,
@@ -570,14 +581,17 @@ def main():
         "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
-                     "traffic": (traffic * n if traffic else None),
-                     "algorithmic_bytes_per_atom_step": bytes_per_atom, "kernel": "k_step (fused force+NVT)",
-                     "ms_per_launch": ms_launch},
+                     "traffic": (traffic * n * block if traffic else None),
+                     "algorithmic_bytes_per_atom_step": bytes_per_atom,
+                     "kernel": "k_run (persistent: steps, rebuilds, thermostat of one timeblock)",
+                     "ms_per_launch": ms_launch, "atom_steps_per_launch": n * block,
+                     "k_step_alone_ms": ms_step_only,
+                     "k_step_alone_gbs": bytes_per_atom * n / (ms_step_only * 1e-3) / 1e9},
         "clocks": clock_info,
         "gpu_launches": launches_per_block * nblocks,
     }
     if rank == 0 and world == 1:
-        cps = max(1, min(3, args.steps))
+        cps = max(1, min(50, args.steps))  # about 10 s of host work at N = 1M
         cmats, threads, secs = cpu_reference(args, n, cps)
         line["cpu_baseline"] = {"value": cmats, "unit": UNIT, "cores": threads, "kind": "port",
                                 "sample": f"{cps} steps of the same N={n} system ({secs:.1f} s)"}
