@@ -41,7 +41,7 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=2000)
     p.add_argument("--warmup", type=int, default=200)
-    p.add_argument("--n", type=int, default=1_048_576)
+    p.add_argument("--n", "--particles", dest="n", type=int, default=1_048_576)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--block", type=int, default=500, help="steps per timeblock")
     p.add_argument("--profile", action="store_true",
@@ -220,6 +220,8 @@ def run_reference_arm(args):
     rank, world, local, pg = dist_setup(args)
     if rank != 0:
         barrier(pg)
+        if pg is not None:
+            pg.destroy_process_group()
         return
     # bounded sample: a few steps of the full-size system (~tens of seconds)
     steps = max(1, min(args.steps, 5))
@@ -240,6 +242,8 @@ def run_reference_arm(args):
     }
     print(json.dumps(line), flush=True)
     barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
 
 
 def run_batch(args):

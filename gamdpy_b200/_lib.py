@@ -84,6 +84,7 @@ SIGNATURES = {
     "gdb_batch_run": ([_P, _d, _i, _P], _i),
     "gdb_batch_destroy": ([_P], _i),
     "gdb_batch_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
+    "gdb_selftest_barrier_timeout": ([_i, ctypes.c_longlong, _P], _i),
     "gdb_adj_create": ([_i, _i, _i, _P], _i),
     "gdb_adj_destroy": ([_P], _i),
     "gdb_adj_setup": ([_P, _P, _P, _P, _f, _i, _i, _i, _f, _f, _f, _i], _i),

@@ -70,6 +70,7 @@ struct DevCtrl {
     unsigned bar_group[64];  // arrivals per group of 16 blocks (grids up to 1024 blocks)
     int abort;            // set when a barrier wait timed out
     unsigned work[2];     // persistent step: next round to hand out, by step parity
+    long long bar_timeout;  // grid-barrier wait limit in SM clock cycles (0: the default, ~1 s)
     unsigned long long *trace;  // optional phase trace: (tag << 56) | globaltimer ns
     int trace_cap;
     int trace_len;

@@ -1472,6 +1472,32 @@ int gdb_batch_get_last_error(gdb_batch *b, char *buf, int n) {
 
 
 
+// Self-test of the bounded grid barrier: two blocks, the second leaves
+// without arriving, so the first block's wait runs out after `cycles`.
+__global__ void k_barrier_selftest(DevCtrl *c) {
+    if (blockIdx.x == 1) return;
+    grid_barrier(c, [] {});
+}
+
+int gdb_selftest_barrier_timeout(int device, long long cycles, unsigned *status) {
+    gdb_sim *h = nullptr;
+    if (!status || cycles <= 0) return set_err(h, GDB_ERR_ARG, "gdb_selftest_barrier_timeout: bad arguments");
+    CK(cudaSetDevice(device));
+    DevCtrl *c = nullptr;
+    CK(cudaMalloc(&c, sizeof(DevCtrl)));
+    cudaError_t e = cudaMemset(c, 0, sizeof(DevCtrl));
+    if (e == cudaSuccess) e = cudaMemcpy(&c->bar_timeout, &cycles, sizeof(cycles), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        k_barrier_selftest<<<2, GDB_BLOCK>>>(c);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpy(status, &c->status, sizeof(unsigned), cudaMemcpyDeviceToHost);
+    cudaFree(c);
+    if (e != cudaSuccess) return set_err(h, GDB_ERR_CUDA, "gdb_selftest_barrier_timeout: %s", cudaGetErrorString(e));
+    return GDB_OK;
+}
+
 int gdb_get_last_error(gdb_sim *h, char *buf, int n) {
     if (!buf || n < 1) return GDB_ERR_ARG;
     snprintf(buf, (size_t)n, "%s", h ? h->err : g_lib_error);

@@ -128,13 +128,14 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
         s_ok = 1;
         if (!s_last) {
             const long long t0 = clock64();
+            const long long limit = c->bar_timeout > 0 ? c->bar_timeout : BARRIER_TIMEOUT_CYCLES;
             int polls = 0;
             while (ld_acquire_gpu(&c->bar_gen) == gen) {
                 if (*(volatile int *)&c->abort) {
                     s_ok = 0;
                     break;
                 }
-                if ((++polls & 63) == 0 && clock64() - t0 > BARRIER_TIMEOUT_CYCLES) {
+                if ((++polls & 63) == 0 && clock64() - t0 > limit) {
                     atomicOr(&c->status, GDB_STATUS_BARRIER_TIMEOUT);
                     c->abort = 1;
                     s_ok = 0;

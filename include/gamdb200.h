@@ -249,6 +249,12 @@ int gdb_sq_compute_noalloc(int n, const float *r_dev, const float *ff_dev, const
                            const int32_t *n_vectors_dev, int n_max, double *rho_re_dev, double *rho_im_dev,
                            void *stream);
 
+/* Self-test of the bounded wait of the persistent kernels' grid barrier (no
+ * reference counterpart): a two-block kernel whose second block never
+ * arrives; the first gives up after `cycles` SM clock cycles and sets
+ * GDB_STATUS_BARRIER_TIMEOUT, returned in *status.  The device stays usable. */
+int gdb_selftest_barrier_timeout(int device, long long cycles, unsigned *status);
+
 /* ---- adjoint: gradients of trajectory averages w.r.t. pair parameters ----
  * No counterpart in the reference (gamdpy has no differentiation).  The
  * forward is the NVE leapfrog of integrators/NVE.py:78-97 with the

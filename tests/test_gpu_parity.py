@@ -363,3 +363,18 @@ def test_kob_andersen_reference_state_point():
     mu, mw = np.mean(U) / N, np.mean(W) / N
     assert abs(mu - (-6.346)) < 0.01, mu
     assert abs(mw - 5.534) < 0.03, mw
+
+
+def test_barrier_wait_runs_out_and_reports(oracle):
+    """The bounded grid-barrier wait gives up (a block that never arrives),
+    sets the status bit, and the device stays usable."""
+    import ctypes
+    st = ctypes.c_uint(0)
+    rc = _lib.lib().gdb_selftest_barrier_timeout(0, 2_000_000, ctypes.byref(st))
+    assert rc == _lib.GDB_OK
+    assert st.value & 0x2  # GDB_STATUS_BARRIER_TIMEOUT
+    conf = workloads.ka_configuration(500, seed=2)
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    sim = make_sim(conf["r"], conf.simbox.lengths, conf.ptype, table, nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.run(0.0, 10)
+    assert sim.status() == 0
