@@ -24,10 +24,15 @@
 // backward recomputes each segment's states from its checkpoint with the
 // same kernels (bit-identical) before sweeping it in reverse, in float64.
 //
-// Pairs are evaluated on the fly over all j with 32 lanes per particle (the
-// N^2 list of interactions/nblist.py gives the same pair set); every sum has a
-// fixed order, so runs are reproducible.  Sized for the small systems this is
-// meant for (N of a few thousand).
+// Pairs come from a neighbour list (all j within the largest cut or the RDF
+// kernel's reach plus a skin of 0.5, built N^2, rebuilt when a particle moves
+// more than half the skin); 32 lanes per particle, lane L taking its column
+// of the list, the neighbours j = L (mod 32) in ascending order.  Every per-lane sum
+// is then the same as a loop over all j (the NbList2 pair set), whatever the
+// list holds beyond the cutoff: results do not depend on when the list was
+// built, so recomputed segments are bit-identical to the forward.  Every sum
+// has a fixed order, so runs are reproducible.  Sized for the small systems
+// this is meant for (N of a few thousand; the build is N^2).
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>
@@ -78,7 +83,22 @@ struct AdjArgs {
     const float *mass;
     int nbins;
     float r_lo, dr, width;  // bin centres r_lo + (b + 1/2) dr
+    // neighbour list: all j within rl of i at the build; particle i's maxnb
+    // entries at nbl + i * maxnb as 32 columns (entry c of column L at
+    // c * 32 + L, the neighbours j = L (mod 32) ascending); nbc holds the 32
+    // column counts of each particle; rebuilt when a particle moves more than
+    // skin/2
+    const int *nbl, *nbc;
+    int maxnb;
+    float rl2;      // (max cut or RDF reach + skin)^2
+    float move2;    // (skin / 2 - margin)^2
+    float4 *rref;   // positions at the last build
+    int *flags;     // rebuild flags, by step parity
+    unsigned *status;
 };
+
+constexpr float ADJ_SKIN = 0.5f;
+constexpr unsigned ADJ_STATUS_OVERFLOW = 1u;
 
 __device__ __forceinline__ float mic_rint(float d, float L, float iL) { return d - L * rintf(d * iL); }
 
@@ -94,7 +114,8 @@ __device__ __forceinline__ T wsum(T v) {
 // gbins (fixed point, integer atomics: order-independent).
 __global__ void __launch_bounds__(ADJ_BLOCK) k_adj_step(AdjArgs a, Tables tab, const float4 *__restrict__ pos_in,
                                                         const float4 *__restrict__ vel_in, float4 *pos_out,
-                                                        float4 *vel_out, double *partials, unsigned long long *gbins) {
+                                                        float4 *vel_out, double *partials, unsigned long long *gbins,
+                                                        int *flag_out) {
     __shared__ Tab32 s_tab[ADJ_MAXT * ADJ_MAXT];
     __shared__ double s_red[ADJ_PPB][3];
     __shared__ unsigned long long s_bins[ADJ_MAXB];
@@ -115,8 +136,14 @@ __global__ void __launch_bounds__(ADJ_BLOCK) k_adj_step(AdjArgs a, Tables tab, c
         ti = a.type[i];
         const Tab32 *row = s_tab + ti * nt;
         const double rg_lo = (double)a.r_lo - ADJ_KW * a.width, rg_hi = (double)a.r_lo + a.nbins * (double)a.dr + ADJ_KW * a.width;
-        for (int j = lane; j < a.n; j += ADJ_LANES) {
-            if (j == i) continue;
+        // lane L takes its own column of the list: the neighbours j = L
+        // (mod 32) in ascending order, the same per-lane sums as a loop over
+        // all j whatever the list holds beyond the cutoff, so results do not
+        // depend on when it was built
+        const int *lst = a.nbl + (size_t)i * a.maxnb + lane;
+        const int cnt = min(a.nbc[(size_t)i * ADJ_LANES + lane], a.maxnb / ADJ_LANES);
+        for (int c = 0; c < cnt; c++) {
+            const int j = lst[c * ADJ_LANES];
             const float4 pj = pos_in[j];
             const float dx = mic_rint(pj.x - pi.x, a.Lx, iLx);
             const float dy = mic_rint(pj.y - pi.y, a.Ly, iLy);
@@ -183,6 +210,12 @@ __global__ void __launch_bounds__(ADJ_BLOCK) k_adj_step(AdjArgs a, Tables tab, c
         pos_out[i] = make_float4(r[0], r[1], r[2], pi.w);
         vel_out[i] = make_float4(vv[0], vv[1], vv[2], 0.f);
         kin = k;
+        if (flag_out) {
+            const float4 q = a.rref[i];
+            const float ex = mic_rint(r[0] - q.x, a.Lx, iLx), ey = mic_rint(r[1] - q.y, a.Ly, iLy),
+                        ez = mic_rint(r[2] - q.z, a.Lz, iLz);
+            if (ex * ex + ey * ey + ez * ez > a.move2) atomicOr(flag_out, 1);
+        }
     }
     if (lane == 0) {
         s_red[q][0] = i < a.n ? (double)u : 0.0;
@@ -285,8 +318,10 @@ __global__ void __launch_bounds__(ADJ_BLOCK) k_adj_back(AdjArgs a, Tables tab, c
         const float iLx = 1.0f / a.Lx, iLy = 1.0f / a.Ly, iLz = 1.0f / a.Lz;
         const double rg_lo = (double)a.r_lo - ADJ_KW * a.width, rg_hi = (double)a.r_lo + a.nbins * (double)a.dr + ADJ_KW * a.width;
         const double cdt = (double)a.dt / mi;
-        for (int j = lane; j < a.n; j += ADJ_LANES) {
-            if (j == i) continue;
+        const int *lst = a.nbl + (size_t)i * a.maxnb + lane;
+        const int cnt = min(a.nbc[(size_t)i * ADJ_LANES + lane], a.maxnb / ADJ_LANES);
+        for (int c = 0; c < cnt; c++) {  // lane L: the neighbours j = L (mod 32), ascending
+            const int j = lst[c * ADJ_LANES];
             const float4 pj = pos[j];
             // same float32 displacement and cutoff test as the forward
             const float fdx = mic_rint(pj.x - pi.x, a.Lx, iLx);
@@ -360,6 +395,51 @@ __global__ void __launch_bounds__(ADJ_BLOCK) k_adj_back(AdjArgs a, Tables tab, c
     }
 }
 
+// Neighbour list (gated): rebuilt when `force` or when flags[rd] is set;
+// block 0 clears flags[clr] for the next writer.  A warp per particle; lane L
+// tests j = L, L + 32, ... and appends its hits to column L of the particle's
+// rows (entry c of column L at c * 32 + L), so each column holds the
+// neighbours j = L (mod 32) in ascending order.
+__global__ void __launch_bounds__(ADJ_BLOCK) k_adj_build(AdjArgs a, const float4 *__restrict__ pos, int *nbl, int *nbc,
+                                                         int force, int rd, int clr) {
+    const bool go = force || *(volatile int *)&a.flags[rd] != 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.flags[clr] = 0;
+    if (!go) return;
+    const int lane = threadIdx.x & 31;
+    const int i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (i >= a.n) return;
+    const float iLx = 1.0f / a.Lx, iLy = 1.0f / a.Ly, iLz = 1.0f / a.Lz;
+    const float4 pi = pos[i];
+    const int rows = a.maxnb / ADJ_LANES;
+    int *col = nbl + (size_t)i * a.maxnb + lane;
+    int count = 0;
+    for (int j = lane; j < a.n; j += ADJ_LANES) {
+        if (j == i) continue;
+        const float4 pj = pos[j];
+        const float dx = mic_rint(pj.x - pi.x, a.Lx, iLx);
+        const float dy = mic_rint(pj.y - pi.y, a.Ly, iLy);
+        const float dz = mic_rint(pj.z - pi.z, a.Lz, iLz);
+        if (dx * dx + dy * dy + dz * dz < a.rl2) {
+            if (count < rows) col[count * ADJ_LANES] = j;
+            count++;
+        }
+    }
+    nbc[(size_t)i * ADJ_LANES + lane] = count;
+    if (count > rows) atomicOr(a.status, ADJ_STATUS_OVERFLOW);
+    if (lane == 0) a.rref[i] = pi;
+}
+
+// Sets flags[wr] when a particle of pos has moved more than skin/2 since the
+// last build (the backward sweep's positions come from a stored segment).
+__global__ void k_adj_check(AdjArgs a, const float4 *__restrict__ pos, int wr) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float4 p = pos[i], q = a.rref[i];
+    const float ex = mic_rint(p.x - q.x, a.Lx, 1.0f / a.Lx), ey = mic_rint(p.y - q.y, a.Ly, 1.0f / a.Ly),
+                ez = mic_rint(p.z - q.z, a.Lz, 1.0f / a.Lz);
+    if (ex * ex + ey * ey + ez * ez > a.move2) atomicOr(&a.flags[wr], 1);
+}
+
 __global__ void k_adj_pack(int n, const float *r, const float *v, const int *type, float4 *pos, float4 *vel) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -390,6 +470,11 @@ struct gdb_adj {
     double *d_part = nullptr, *d_acc = nullptr;
     unsigned long long *d_bins = nullptr;
     double *d_R = nullptr, *d_V = nullptr, *d_Vt = nullptr, *d_th = nullptr, *d_gG = nullptr;
+    int *d_nbl = nullptr, *d_nbc = nullptr, *d_flags = nullptr;
+    float4 *d_rref = nullptr;
+    unsigned *d_status = nullptr;
+    int maxnb = 0;
+    float rl = 0.f;
     int nsamples = 0;
     std::vector<double> obs;
     cudaStream_t st = nullptr;
@@ -421,7 +506,8 @@ void adj_free(gdb_adj *h) {
     if (h->st) cudaStreamSynchronize(h->st);
     void *ptrs[] = {h->d_type, h->d_mass, h->d_pos[0], h->d_pos[1], h->d_vel[0], h->d_vel[1], h->d_ck_pos,
                     h->d_ck_vel, h->d_seg_pos, h->d_seg_vel, h->d_part, h->d_acc, h->d_bins, h->d_R,
-                    h->d_V, h->d_Vt, h->d_th, h->d_gG};
+                    h->d_V, h->d_Vt, h->d_th, h->d_gG, h->d_nbl, h->d_nbc, h->d_flags, h->d_rref,
+                    h->d_status};
     for (void *p : ptrs)
         if (p) cudaFree(p);
     if (h->st) cudaStreamDestroy(h->st);
@@ -441,23 +527,69 @@ AdjArgs adj_args(const gdb_adj *h) {
     a.r_lo = h->r_lo;
     a.dr = h->nbins > 0 ? (h->r_hi - h->r_lo) / h->nbins : 1.f;
     a.width = h->width;
+    a.nbl = h->d_nbl;
+    a.nbc = h->d_nbc;
+    a.maxnb = h->maxnb;
+    a.rl2 = h->rl * h->rl;
+    const float mv = 0.5f * ADJ_SKIN - 0.01f;
+    a.move2 = mv * mv;
+    a.rref = h->d_rref;
+    a.flags = h->d_flags;
+    a.status = h->d_status;
     return a;
 }
 
 int nblocks_of(const gdb_adj *h) { return (h->n + ADJ_PPB - 1) / ADJ_PPB; }
 
+int build_blocks(const gdb_adj *h) { return (h->n * 32 + ADJ_BLOCK - 1) / ADJ_BLOCK; }
+
 // One forward step from buffers (pin, vin) into (pout, vout); step index s.
+// The list is rebuilt first when the previous step flagged it (or `force`);
+// step s flags into slot s & 1, which the build before it clears.
 int forward_step(gdb_adj *h, const float4 *pin, const float4 *vin, float4 *pout, float4 *vout, int s,
-                 bool accumulate) {
+                 bool accumulate, bool force) {
     const AdjArgs a = adj_args(h);
+    k_adj_build<<<build_blocks(h), ADJ_BLOCK, 0, h->st>>>(a, pin, h->d_nbl, h->d_nbc, force ? 1 : 0, (s + 1) & 1,
+                                                           s & 1);
+    ACK(cudaGetLastError());
     const bool rdf = accumulate && h->nbins > 0 && h->rdf_every > 0 && s % h->rdf_every == 0;
     k_adj_step<<<nblocks_of(h), ADJ_BLOCK, 0, h->st>>>(a, h->tab, pin, vin, pout, vout, h->d_part,
-                                                        rdf ? h->d_bins : nullptr);
+                                                        rdf ? h->d_bins : nullptr, h->d_flags + (s & 1));
     ACK(cudaGetLastError());
     if (accumulate) {
         k_adj_reduce<<<1, 256, 0, h->st>>>(h->d_part, nblocks_of(h), h->d_acc);
         ACK(cudaGetLastError());
     }
+    return GDB_OK;
+}
+
+// List reach (largest cut, or the RDF kernel's reach, plus the skin) and
+// capacity (32 columns, each twice its mean count at this density plus 8).
+int ensure_list(gdb_adj *h) {
+    float reach = 0.f;
+    for (int k = 0; k < h->nt * h->nt; k++) reach = std::max(reach, h->tab.t32[k].cut);
+    if (h->nbins > 0)
+        reach = std::max(reach, (float)((double)h->r_hi + ADJ_KW * h->width));
+    h->rl = reach + ADJ_SKIN;
+    const double vol = (double)h->box[0] * h->box[1] * h->box[2];
+    const double mean = 4.0 / 3.0 * M_PI * (double)h->rl * h->rl * h->rl * h->n / vol;
+    // 32 columns of rows entries: a column holds about mean / 32 neighbours
+    const int rows = std::min((int)(2.0 * mean / ADJ_LANES) + 8, (h->n + ADJ_LANES - 1) / ADJ_LANES);
+    const int want = rows * ADJ_LANES;
+    if (want > h->maxnb || !h->d_nbl) {
+        if (h->d_nbl) cudaFree(h->d_nbl);
+        h->d_nbl = nullptr;
+        ACK(cudaMalloc(&h->d_nbl, (size_t)h->n * want * sizeof(int)));
+        h->maxnb = want;
+    }
+    if (!h->d_nbc) {
+        ACK(cudaMalloc(&h->d_nbc, (size_t)h->n * ADJ_LANES * sizeof(int)));
+        ACK(cudaMalloc(&h->d_rref, h->n * sizeof(float4)));
+        ACK(cudaMalloc(&h->d_flags, 2 * sizeof(int)));
+        ACK(cudaMalloc(&h->d_status, sizeof(unsigned)));
+    }
+    ACK(cudaMemsetAsync(h->d_flags, 0, 2 * sizeof(int), h->st));
+    ACK(cudaMemsetAsync(h->d_status, 0, sizeof(unsigned), h->st));
     return GDB_OK;
 }
 
@@ -585,6 +717,8 @@ int gdb_adj_forward(gdb_adj *h, const double *params, const float *r0, const flo
     ACK(cudaSetDevice(h->dev));
     build_tables(h, params);
     const int n = h->n;
+    int rc = ensure_list(h);
+    if (rc) return rc;
     float *dr = nullptr, *dv = nullptr;
     ACK(cudaMallocAsync(&dr, (size_t)n * 3 * sizeof(float), h->st));
     ACK(cudaMallocAsync(&dv, (size_t)n * 3 * sizeof(float), h->st));
@@ -604,7 +738,7 @@ int gdb_adj_forward(gdb_adj *h, const double *params, const float *r0, const flo
             ACK(cudaMemcpyAsync(h->d_ck_pos + off, h->d_pos[cur], n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
             ACK(cudaMemcpyAsync(h->d_ck_vel + off, h->d_vel[cur], n * sizeof(float4), cudaMemcpyDeviceToDevice, h->st));
         }
-        int rc = forward_step(h, h->d_pos[cur], h->d_vel[cur], h->d_pos[cur ^ 1], h->d_vel[cur ^ 1], s, true);
+        rc = forward_step(h, h->d_pos[cur], h->d_vel[cur], h->d_pos[cur ^ 1], h->d_vel[cur ^ 1], s, true, s == 0);
         if (rc) return rc;
         if (h->nbins > 0 && h->rdf_every > 0 && s % h->rdf_every == 0) h->nsamples++;
         cur ^= 1;
@@ -613,7 +747,12 @@ int gdb_adj_forward(gdb_adj *h, const double *params, const float *r0, const flo
     std::vector<unsigned long long> bins(ADJ_MAXB);
     ACK(cudaMemcpyAsync(acc, h->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, h->st));
     ACK(cudaMemcpyAsync(bins.data(), h->d_bins, ADJ_MAXB * sizeof(unsigned long long), cudaMemcpyDeviceToHost, h->st));
+    unsigned status = 0;
+    ACK(cudaMemcpyAsync(&status, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->st));
     ACK(cudaStreamSynchronize(h->st));
+    if (status & ADJ_STATUS_OVERFLOW)
+        return aset(h, GDB_ERR_NBLIST, "gdb_adj_forward: a list column outgrew %d entries (reach %.3f)",
+                    h->maxnb / ADJ_LANES, h->rl);
     h->obs.assign(3 + h->nbins, 0.0);
     for (int q = 0; q < 3; q++) h->obs[q] = acc[q] / h->steps;
     if (h->nbins > 0 && h->nsamples > 0) {
@@ -671,12 +810,22 @@ int gdb_adj_backward(gdb_adj *h, const double *grad_obs, double *grad_params) {
         for (int k = 0; k < len; k++) {
             int rc = forward_step(h, h->d_seg_pos + (size_t)k * n, h->d_seg_vel + (size_t)k * n,
                                   h->d_seg_pos + (size_t)(k + 1) * n, h->d_seg_vel + (size_t)(k + 1) * n, s0 + k,
-                                  false);
+                                  false, k == 0);
             if (rc) return rc;
         }
-        // reverse sweep of the segment
+        // reverse sweep of the segment; the list follows the positions
+        // backwards (check -> gated build), slots by step parity
+        ACK(cudaMemsetAsync(h->d_flags, 0, 2 * sizeof(int), h->st));
         for (int k = len - 1; k >= 0; k--) {
             const int s = s0 + k;
+            {
+                const float4 *pk = h->d_seg_pos + (size_t)k * n;
+                k_adj_check<<<(n + 255) / 256, 256, 0, h->st>>>(a, pk, s & 1);
+                ACK(cudaGetLastError());
+                k_adj_build<<<build_blocks(h), ADJ_BLOCK, 0, h->st>>>(a, pk, h->d_nbl, h->d_nbc, k == len - 1 ? 1 : 0,
+                                                                       s & 1, (s + 1) & 1);
+                ACK(cudaGetLastError());
+            }
             if (h->window > 0 && (s + 1) % h->window == 0) {
                 // last step of a window: nothing flows back across its end
                 ACK(cudaMemsetAsync(h->d_R, 0, (size_t)n * 3 * sizeof(double), h->st));
@@ -693,8 +842,13 @@ int gdb_adj_backward(gdb_adj *h, const double *grad_obs, double *grad_params) {
         }
     }
     std::vector<double> th((size_t)nb * ADJ_NTH);
+    unsigned status = 0;
     ACK(cudaMemcpyAsync(th.data(), h->d_th, th.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+    ACK(cudaMemcpyAsync(&status, h->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, h->st));
     ACK(cudaStreamSynchronize(h->st));
+    if (status & ADJ_STATUS_OVERFLOW)
+        return aset(h, GDB_ERR_NBLIST, "gdb_adj_backward: a list column outgrew %d entries (reach %.3f)",
+                    h->maxnb / ADJ_LANES, h->rl);
     // fixed-order sum over blocks; a parameter of the unordered pair {a, b}
     // collects the (a, b) and (b, a) entries
     const int nt = h->nt;
