@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
     const int P = (n + C - 1) / C;
     const int ncx = a.ncx, ncy = a.ncy, ncz = a.ncz;
     const int ncell = ncx * ncy * ncz;
-    const bool use_cells = ncell > 0 && ncell <= CL_MAX_CELLS;
+    const bool use_cells = n > CL_NSQ_MAX && ncell > 0 && ncell <= CL_MAX_CELLS;
     const int cap = job.cap;
     const bool pp = job.pingpong != 0;
     const bool sorted = use_cells && job.sorted != 0;
@@ -647,7 +647,7 @@ void cluster_shape(int n, int target, int *C, int *tp) {
 
 bool cluster_plan(int n, int C, int ncell, int max_nbs, int *cap, int *pingpong, int *sorted, size_t *smem) {
     const int P = (n + C - 1) / C;
-    const int nc = ncell > 0 && ncell <= CL_MAX_CELLS ? ncell : 0;
+    const int nc = n > CL_NSQ_MAX && ncell > 0 && ncell <= CL_MAX_CELLS ? ncell : 0;
     const int want = std::min((std::max(max_nbs, 4) + 3) & ~3, CL_CAP_MAX);
     const int opts[3][2] = {{1, 1}, {0, 1}, {0, 0}};  // (pingpong, sorted), best first
     for (int o = 0; o < 3; o++) {

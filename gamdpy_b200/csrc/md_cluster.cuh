@@ -10,6 +10,7 @@ constexpr int CL_THREADS = 512;  // 128 registers a thread: the step keeps its s
 constexpr int CL_MAX_N = 4096;
 constexpr int CL_CAP_MAX = 1024;    // neighbour slots per particle: upper bound
 constexpr int CL_MAX_CELLS = 8192;  // shared cell table; sparser grids build N^2
+constexpr int CL_NSQ_MAX = 768;     // up to this size the list build is N^2 (measured: 2x faster at 512, 1.5x slower at 2048)
 constexpr int CL_NQ = 11;           // NQ sums + moved flag + max list length
 constexpr size_t CL_SMEM_LIMIT = 208 * 1024;  // dynamic; the kernel's static arrays take under 16 KB
 
