@@ -198,11 +198,26 @@ class Sim:
         self.call("gdb_download_state", ptr(out["r"]), ptr(out["v"]), ptr(out["f"]), ptr(out["r_im"]))
         return out
 
-    def download_scalars(self):
+    def download_scalars(self, out=None):
+        """Per-particle U, W, lapU, K, Fsq; `out` (a dict of (n,) float32
+        arrays) is filled in place when given."""
         n = self.n
-        out = {k: np.empty(n, np.float32) for k in ("U", "W", "lapU", "K", "Fsq")}
+        if out is None:
+            out = {k: np.empty(n, np.float32) for k in ("U", "W", "lapU", "K", "Fsq")}
+        for k in ("U", "W", "lapU", "K", "Fsq"):
+            a = out[k]
+            assert a.dtype == np.float32 and a.shape == (n,) and a.flags.c_contiguous
         self.call("gdb_download_scalars", *(ptr(out[k]) for k in ("U", "W", "lapU", "K", "Fsq")))
         return out
+
+    def download_into(self, r=None, v=None, f=None, r_im=None):
+        """Fill caller-owned (n, 3) arrays in place (float32; int32 for r_im):
+        no fresh host pages per call, which dominate large copies otherwise."""
+        n = self.n
+        for a, dt in ((r, np.float32), (v, np.float32), (f, np.float32), (r_im, np.int32)):
+            if a is not None:
+                assert a.dtype == dt and a.shape == (n, 3) and a.flags.c_contiguous
+        self.call("gdb_download_state", ptr(r), ptr(v), ptr(f), ptr(r_im))
 
     # --- configuration of the step ------------------------------------
     def set_pair_potential(self, kind, cutmode, table):

@@ -192,12 +192,22 @@ class Configuration:
         """Download r, v, f, images and the per-particle scalars."""
         if self._device is None:
             return
-        st = self._device.download()
-        self.vectors["r"] = st["r"]
-        self.vectors["v"] = st["v"]
-        self.vectors["f"] = st["f"]
-        self.r_im[:] = st["r_im"]
-        sc = self._device.download_scalars()
+        # straight into this configuration's arrays (and a kept scalar buffer)
+        vec = {k: self.vectors[k] for k in ("r", "v", "f")}
+        im = self.r_im
+        if all(a.dtype == np.float32 and a.flags.c_contiguous for a in vec.values()) and \
+                im.dtype == np.int32 and im.flags.c_contiguous:
+            self._device.download_into(vec["r"], vec["v"], vec["f"], im)
+        else:
+            st = self._device.download()
+            for k in ("r", "v", "f"):
+                self.vectors[k] = st[k]
+            self.r_im[:] = st["r_im"]
+        buf = getattr(self, "_scalar_buf", None)
+        if buf is None or buf["U"].shape[0] != self.N:
+            buf = {k: np.empty(self.N, np.float32) for k in ("U", "W", "lapU", "K", "Fsq")}
+            self._scalar_buf = buf
+        sc = self._device.download_scalars(buf)
         for k in ("U", "W", "lapU", "K", "Fsq"):
             if k in self.sid:
                 self.scalars[:, self.sid[k]] = sc[k]
