@@ -26,7 +26,8 @@ class SimulationBatch:
     All simulations need the same device, number of particle types,
     integrator kind, ``steps_per_timeblock`` and ``dt`` (the timeblock's start
     time is shared).  ``particles_per_cta`` shapes the clusters (about that
-    many particles per CTA, up to 16 CTAs per system; 0 = library default);
+    many particles per CTA, at most 256, up to 16 CTAs per system; 0 = the
+    single-system default, so every system gives the same bits as alone);
     ``autotune`` picks it by timing.
     """
 

@@ -632,9 +632,16 @@ const void *cluster_kernel(int tp, int ntypes, int integ) {
 }
 
 // Cluster size and lanes per particle for a system of n particles: about
-// `target` particles per CTA (0: 128), at most 16 CTAs.
+// `target` particles per CTA (at most CL_THREADS / 2), at most 16 CTAs.
 void cluster_shape(int n, int target, int *C, int *tp) {
-    if (target <= 0) target = 128;
+    // default: spread the system over 16 CTAs, at least 32 particles each
+    // (measured on B200, one KA system of 512: 6.7 us per step at 32
+    // particles per CTA, 12.1 us at 128); batches of many systems run faster
+    // with more particles per CTA (SimulationBatch.autotune)
+    if (target <= 0) target = std::max(32, (n + 15) / 16);
+    // every particle needs at least two lanes of the CTA (the kernel is
+    // instantiated for 2..32 lanes per particle)
+    target = std::min(target, CL_THREADS / 2);
     int c = 1;
     while (c < 16 && (n + c - 1) / c > target) c *= 2;
     const int P = (n + c - 1) / c;
@@ -647,6 +654,7 @@ void cluster_shape(int n, int target, int *C, int *tp) {
 
 bool cluster_plan(int n, int C, int ncell, int max_nbs, int *cap, int *pingpong, int *sorted, size_t *smem) {
     const int P = (n + C - 1) / C;
+    if (2 * P > CL_THREADS) return false;  // not every particle would have its lanes
     const int nc = n > CL_NSQ_MAX && ncell > 0 && ncell <= CL_MAX_CELLS ? ncell : 0;
     const int want = std::min((std::max(max_nbs, 4) + 3) & ~3, CL_CAP_MAX);
     const int opts[3][2] = {{1, 1}, {0, 1}, {0, 0}};  // (pingpong, sorted), best first

@@ -67,7 +67,8 @@ __host__ __device__ inline ClusterSmem cluster_smem_layout(int n, int P, int nce
 // Host side (md_cluster.cu).
 const void *cluster_kernel(int tp, int ntypes, int integ);
 // Cluster size C and lanes per particle for n particles, about `target`
-// particles per CTA (0: 128), C <= 16.
+// particles per CTA (0: spread over 16 CTAs, at least 32 each; at most 256),
+// C <= 16.
 void cluster_shape(int n, int target, int *C, int *tp);
 // Neighbour slots per particle, position double-buffering, the sorted copy and
 // dynamic shared memory for a system of n particles on C CTAs over ncell

@@ -550,7 +550,7 @@ static int status_to_rc(gdb_sim *h) {
 // cluster launch is not possible on this device.
 static int run_cluster(gdb_sim *h, int steps) {
     int C, tp;
-    cluster_shape(h->n, 0, &C, &tp);
+    cluster_shape(h->n, h->pb_req, &C, &tp);
     SimArgs a = make_args(h);
     // the cell grid of the global cell build, whatever list kind was chosen
     // (both kinds give the same sets)

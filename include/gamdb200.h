@@ -113,7 +113,9 @@ int gdb_set_nblist(gdb_sim *h, int kind, float skin, int max_nbs);
 
 /* Threads per particle (compute_plan['tp'], simulation/get_default_compute_plan.py:55-63):
  * 1, 2, 4, 8, 16 or 32 lanes share one particle's neighbours; 0 = choose.
- * pb (particles per block) is accepted for compatibility.  0 = choose. */
+ * pb (particles per block): for systems on the thread-block-cluster path
+ * (N <= 4096), about pb particles per CTA (at most 256); 0 = choose (spread
+ * over 16 CTAs). */
 int gdb_set_plan(gdb_sim *h, int tp, int pb);
 
 /* Integrators: NVE.get_params (integrators/NVE.py:29-31);
@@ -226,7 +228,9 @@ int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], i
  * per-system results are read from each handle as usual. */
 typedef struct gdb_batch gdb_batch;
 /* particles_per_cta: cluster shaping target (about that many particles per
- * CTA, up to 16 CTAs per system); 0 = 128.  Tuned by Batch.autotune. */
+ * CTA, at most 256, up to 16 CTAs per system); 0 = the single-system default
+ * (spread over 16 CTAs, at least 32 particles each), so a system gives the
+ * same bits in a batch as alone.  Tuned by SimulationBatch.autotune. */
 int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb_batch **out);
 int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms);
 int gdb_batch_destroy(gdb_batch *b);

@@ -211,3 +211,19 @@ def test_batch_continues_individual_runs_without_upload():
         sx, sy = state(x), state(y)
         for q in ("r", "v", "r_im"):
             assert np.array_equal(sx[q], sy[q]), q
+
+
+@pytest.mark.parametrize("pb", [32, 256, 512])
+def test_cluster_particles_per_cta_plan(pb, monkeypatch):
+    """Any particles-per-CTA request (requests above 256 are capped) gives the
+    same trajectory as the global path, to float32 round-off."""
+    a = ka_sim(2048, seed=31)
+    monkeypatch.setenv("GDB_CLUSTER", "0")
+    b = ka_sim(2048, seed=31)
+    monkeypatch.delenv("GDB_CLUSTER")
+    a._sim.set_plan(0, pb)
+    for s in (a, b):
+        s.configuration.copy_to_device()
+        s._sim.run(0.0, 20)
+    assert a._sim.last_path() == 2 and a._sim.status() == 0
+    assert np.max(np.abs(state(a)["r"] - state(b)["r"])) < 1e-4
