@@ -1322,9 +1322,11 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
             g->pp.push_back(pingpong | (sorted << 1));
             g->smem = std::max(g->smem, smem);
         } else if (h->n <= CLG_MAX_N) {
-            // about 1024 particles per CTA (one lane each), 4 to 16 CTAs
-            int c = 4;
-            while (c < 16 && h->n > c * 1024) c *= 2;
+            // about 4096 particles per CTA (four per lane), 1 to 16 CTAs
+            // (measured on B200, 128-replica sweep: 954 / 1048 / 1134 / 1272 /
+            // 1084 MATS at 512 / 1024 / 2048 / 4096 / 8192 per CTA)
+            int c = 1;
+            while (c < 16 && h->n > c * 4096) c *= 2;
             gdb_batch::Group *g = batch_group(b, 1, c, b->clg_tp);
             g->idx.push_back(k);
             g->cap.push_back(0);
