@@ -48,7 +48,7 @@ def parse():
                    help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
     p.add_argument("--tp", type=int, default=0, help="lanes per particle (0 = library default)")
     p.add_argument("--trace", action="store_true", help="with --profile: phase trace of the persistent kernel")
-    p.add_argument("--workload", default="ka", choices=["ka", "lj2048", "batch", "adjoint"],
+    p.add_argument("--workload", default="ka", choices=["ka", "lj2048", "lj8m", "batch", "adjoint"],
                    help="ka: one KA system of --n particles; batch: --replicas KA replicas of uneven N, "
                         "density and temperature advanced together, against the same replicas run one by one")
     p.add_argument("--replicas", type=int, default=128)
@@ -385,6 +385,74 @@ def run_lj_small(args):
         pg.destroy_process_group()
 
 
+def run_lj_large(args):
+    """Large-N LJ with on-the-fly structure: FCC 128^3 = 8 388 608 particles at
+    rho = 0.84, T = 1.0 (seeded), shifted-force rc = 2.5, NVE dt = 0.004, cell
+    lists skin 0.5; every 100 steps the RDF over [0, 5) with 1000 bins
+    (integer counts) and S(q) on the q-vectors of the first 200 |n|^2 shells
+    (the reference's non-negative generator), both from the device-resident
+    state.  MATS counts the analysis time too."""
+    import gamdpy_b200 as gp
+    from gamdpy_b200 import workloads
+    rank, world, local, pg = dist_setup(args)
+    conf = workloads.lj_configuration([128, 128, 128], 0.84, 1.0, seed=rank)
+    n = conf.N
+    pp = workloads.lj_pair_potential(cut=2.5, shifted_force=True, max_num_nbs=200)
+    every = 100
+    nblocks = max(1, args.steps // every)
+    steps = nblocks * every
+    plan = {"pb": 256, "tp": 1, "lanes": args.tp, "skin": 0.5, "UtilizeNIII": False, "gridsync": False,
+            "nblist": "linked lists"}
+    sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.004), [], num_timeblocks=nblocks, steps_per_timeblock=every,
+                        compute_plan=plan, storage="memory", device=local)
+    dev = sim._sim
+    rdf = gp.CalculatorRadialDistribution(conf, bins=1000, r_max=5.0)
+    sq = gp.CalculatorStructureFactor(conf)
+    L = float(conf.simbox.lengths[0])
+    sq.generate_q_vectors(2 * np.pi * np.sqrt(237.5) / L)
+    nq = len(sq.q_vectors)
+    dev.run(0.0, max(3, args.warmup))
+    rdf.update()
+    sq.update()
+    barrier(pg)
+    clocks = ClockSampler(local)
+    clocks.start()
+    t_md = t_rdf = t_sq = 0.0
+    t0 = time.perf_counter()
+    for b in range(nblocks):
+        t_md += dev.run(float(b * every * 0.004), every) / 1e3
+        t1 = time.perf_counter()
+        rdf.update()
+        t2 = time.perf_counter()
+        sq.update()
+        t3 = time.perf_counter()
+        t_rdf += t2 - t1
+        t_sq += t3 - t2
+    wall = time.perf_counter() - t0
+    clock_info = clocks.stop()
+    t_all = allreduce_max(pg, t_md + t_rdf + t_sq, local)
+    pairs = float(rdf.rdf_list[-1].sum())  # ordered pairs counted in one update
+    line = {
+        "metric": "MATS (million atom-timesteps/s), LJ N=8388608 NVE cells with RDF and S(q) every 100 steps, 1 B200",
+        "value": n * steps * world / t_all / 1e6, "unit": "Matom-steps/s", "n_gpus": world, "steps": steps,
+        "warmup": max(3, args.warmup), "ms_per_step": t_all * 1e3 / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)", "data": "synthetic (seeded FCC lattice)",
+        "config": {"workload": "LJ SF rc=2.5, FCC 128^3 rho=0.84 T=1.0, NVE dt=0.004, cells skin 0.5; RDF r<5 "
+                               "1000 bins and S(q) on the first 200 |n|^2 shells every 100 steps",
+                   "n": n, "nq": nq, "md_ms_per_step": t_md * 1e3 / steps,
+                   "rdf_ms_per_update": t_rdf * 1e3 / nblocks, "rdf_pairs_per_update": pairs,
+                   "rdf_pairs_per_s": pairs * nblocks / t_rdf if t_rdf > 0 else None,
+                   "sq_ms_per_update": t_sq * 1e3 / nblocks, "sq_terms_per_s": n * nq * nblocks / t_sq if t_sq > 0 else None,
+                   "wall_s": wall, "l2": "working set of several GB > 126 MB L2, no flush"},
+        "clocks": clock_info,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
 def run_adjoint(args):
     """Adjoint workload: KA N=4096, rho 1.2, T 0.6, an NVE trajectory of
     --steps steps (2000 by default) with checkpoints every 50; loss = squared
@@ -491,6 +559,9 @@ def main():
         return
     if args.workload == "lj2048":
         run_lj_small(args)
+        return
+    if args.workload == "lj8m":
+        run_lj_large(args)
         return
     rank, world, local, pg = dist_setup(args)
     import gamdpy_b200 as gp
