@@ -77,6 +77,7 @@ SIGNATURES = {
     "gdb_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
     "gdb_rdf_update": ([_P, _i, _d, _P], _i),
     "gdb_sq_update": ([_P, _i, _P, _P, _P, _P], _i),
+    "gdb_last_analysis_ms": ([_P, _P], _i),
     "gdb_rdf_compute": ([_i, _P, _P, _P, _i, _i, _d, _P], _i),
     "gdb_sq_compute": ([_i, _P, _P, _P, _i, _P, _P, _P], _i),
     "gdb_sq_compute_noalloc": ([_i, _P, _P, _P, _i, _P, _i, _P, _P, _P], _i),
@@ -320,6 +321,12 @@ class Sim:
     def rdf_update(self, bins, r_max, out):
         assert out.dtype == np.uint64 and out.flags.c_contiguous
         self.call("gdb_rdf_update", int(bins), float(r_max), ptr(out))
+
+    def last_analysis_ms(self):
+        """Device time of the last rdf_update / sq_update (CUDA events)."""
+        ms = ctypes.c_float()
+        self.call("gdb_last_analysis_ms", ctypes.byref(ms))
+        return float(ms.value)
 
     def sq_update(self, n_vectors, ff=None):
         nv = i32(n_vectors)

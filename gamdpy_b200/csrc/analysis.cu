@@ -5,11 +5,15 @@
 // (type_i, type_j) histogram, with the reference's mixed precision: dist_sq
 // in float32 (orthorhombic.py:59-73), the range test and d / width in
 // float64, d = sqrt(dist_sq) in float32.  Counts are exact integers (uint64).
+// dist_sq is symmetric bit for bit (the minimum image of -dr is -dr's), so
+// each unordered pair is evaluated once and counted in both orders.
 //   * r_max >= min(L)/3: all pairs, j tiles staged in shared memory.
-//   * smaller r_max: particles binned into cells of edge >= r_max (counting
-//     sort), 27-cell stencil.  Same pair set, so the same counts.
-// Per-block histograms live in shared memory (uint32) and are flushed with
-// 64-bit atomics.
+//   * smaller r_max: particles sorted into cells of edge >= r_max (counting
+//     sort), home cell and half shell of 13 neighbours.  Same pair set, so
+//     the same counts.
+// Pairs in range are queued per warp and binned 32 at a time.  Per-block
+// histograms live in shared memory (uint32) and are flushed with 64-bit
+// atomics.
 //
 // S(q) (calculators/calculator_structure_factor.py:131-156, :185-203):
 // rho_q = N_f^-1/2 sum_i f_i exp(i q.r_i) with q = 2 pi n / L.  Because q is
@@ -24,6 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <vector>
 
@@ -42,6 +47,22 @@ int gdb_internal_ntypes(gdb_sim *h);
 int gdb_internal_dev(gdb_sim *h);
 int gdb_internal_uploaded(gdb_sim *h);
 char *gdb_internal_err(gdb_sim *h);
+cudaEvent_t gdb_internal_event(gdb_sim *h, int k);
+void gdb_internal_set_analysis_ms(gdb_sim *h, float ms);
+}
+
+// Device time of one handle call: events on the handle's stream around its
+// device work (nothing for the stand-alone calculators, h == NULL).
+static cudaError_t timing_begin(gdb_sim *h, cudaStream_t st) {
+    return h ? cudaEventRecord(gdb_internal_event(h, 0), st) : cudaSuccess;
+}
+static cudaError_t timing_end(gdb_sim *h, cudaStream_t st) {
+    return h ? cudaEventRecord(gdb_internal_event(h, 1), st) : cudaSuccess;
+}
+static void timing_store(gdb_sim *h) {
+    float ms = 0.f;
+    if (h && cudaEventElapsedTime(&ms, gdb_internal_event(h, 0), gdb_internal_event(h, 1)) == cudaSuccess)
+        gdb_internal_set_analysis_ms(h, ms);
 }
 
 static int aset(gdb_sim *h, int code, const char *msg, cudaError_t e = cudaSuccess) {
@@ -58,75 +79,282 @@ static int aset(gdb_sim *h, int code, const char *msg, cudaError_t e = cudaSucce
 
 namespace {
 
-constexpr int RDF_TILE = 256;
+constexpr int RDF_THREADS = 256;
+constexpr int RDF_WARPS = RDF_THREADS / 32;
+constexpr int RDF_TILE = RDF_THREADS;     // j positions staged per block (all-pairs path)
 constexpr int RDF_SMEM_MAX_BINS = 12288;  // uint32 entries kept in shared memory
+constexpr int RDF_RING = 64;              // pending pairs per warp (< 32 + 32 before a drain)
 
 struct RdfArgs {
-    const float4 *pos;
     int n, nt, bins;
     float Lx, Ly, Lz;
-    double r_max, width, r_max_sq;
+    // smallest float32 >= r_max^2 and >= r_max: for a float32 x,
+    // (double)x < r_max^2  <=>  x < r2f, so the range tests stay in float32
+    float r2f, rf;
+    double width, inv_width;  // r_max / bins and its rounded reciprocal
     unsigned long long *out;
-    int fma;  // distance accumulation form (see dist_sq_exact)
 };
 
-__device__ __forceinline__ void rdf_pair(const RdfArgs &a, float4 pj, float4 pi, int ti, unsigned *hist,
-                                         bool shared_hist) {
-    const float d2 = a.fma ? dist_sq_exact<true>(pj, pi, a.Lx, a.Ly, a.Lz) : dist_sq_exact<false>(pj, pi, a.Lx, a.Ly, a.Lz);
-    if ((double)d2 < a.r_max_sq) {
-        const float d = __fsqrt_rn(d2);
-        if ((double)d < a.r_max) {
-            int b = (int)__ddiv_rn((double)d, a.width);
-            // d < r_max, yet d / width can round up to `bins`; the reference
-            // would index past its array there, this keeps the count in range
-            if (b >= a.bins) b = a.bins - 1;
-            const int tj = ptype_of(pj);
-            const int idx = (ti * a.nt + tj) * a.bins + b;
-            if (shared_hist)
-                atomicAdd(&hist[idx], 1u);
-            else
-                atomicAdd(&a.out[idx], 1ull);
-        }
-    }
+// Pairs within range wait in a per-warp ring until 32 of them are pending;
+// the square root, the float64 bin and the histogram increments then run with
+// every lane busy instead of at the hit rate (about 15 % of candidates).
+struct RdfRing {
+    float d2[RDF_RING];
+    int code[RDF_RING];  // t_i | t_j << 16
+};
+
+// int(d / width) as the float64 division gives it.  q = d * (1 / width) is
+// within 2.3e-16 q of d / width and the rounded quotient within 1.2e-16, so
+// their floors can differ only when an integer k >= 1 lies within
+// 3.3e-16 k of q; such quotients (|q - k| <= 1e-12 k) take the division.
+__device__ __forceinline__ int rdf_bin(const RdfArgs &a, float d) {
+    const double q = (double)d * a.inv_width;
+    const double k = rint(q);
+    int b = (k >= 1.0 && fabs(q - k) <= 1e-12 * k) ? (int)__ddiv_rn((double)d, a.width) : (int)q;
+    // d < r_max, yet d / width can round up to `bins`; the reference would
+    // index past its array there, this keeps the count in range
+    return b < a.bins ? b : a.bins - 1;
 }
 
-__device__ __forceinline__ void flush_hist(const RdfArgs &a, unsigned *hist, int total) {
+// One pending pair per lane (lane < take): both orders (i, j) and (j, i) of
+// the pair are counted, in (t_i, t_j) and (t_j, t_i).
+__device__ __forceinline__ void rdf_drain(const RdfArgs &a, const RdfRing &rg, int head, int take, int lane,
+                                          unsigned *hist, bool sh) {
+    __syncwarp();
+    if (lane < take) {
+        const int e = (head + lane) & (RDF_RING - 1);
+        const float d = __fsqrt_rn(rg.d2[e]);
+        if (d < a.rf) {
+            const int b = rdf_bin(a, d);
+            const int ti = rg.code[e] & 0xffff, tj = rg.code[e] >> 16;
+            const int k1 = (ti * a.nt + tj) * a.bins + b, k2 = (tj * a.nt + ti) * a.bins + b;
+            if (sh) {
+                if (k1 == k2) {
+                    atomicAdd(&hist[k1], 2u);
+                } else {
+                    atomicAdd(&hist[k1], 1u);
+                    atomicAdd(&hist[k2], 1u);
+                }
+            } else {
+                if (k1 == k2) {
+                    atomicAdd(&a.out[k1], 2ull);
+                } else {
+                    atomicAdd(&a.out[k1], 1ull);
+                    atomicAdd(&a.out[k2], 1ull);
+                }
+            }
+        }
+    }
+    __syncwarp();
+}
+
+// Lane's particle i against jn <= 32 staged positions js[0..jn).  First pass:
+// every candidate's dist_sq goes to the warp's d2s[q][lane] and in-range
+// candidates set bit q of the lane's mask; bits q <= lim are dropped (j at or
+// before i in the same cell or tile).  Second pass: lanes hand their hits to
+// the ring one per round, and full rounds of 32 are binned.  MIC: minimum
+// image per component, as the reference; without it the plain difference,
+// which callers use only where it gives the same pairs in range and the same
+// dist_sq for them.
+template <bool FMA, bool MIC>
+__device__ __forceinline__ float rdf_d2(const RdfArgs &a, float4 pj, float4 pi) {
+    float dx = __fsub_rn(pj.x, pi.x), dy = __fsub_rn(pj.y, pi.y), dz = __fsub_rn(pj.z, pi.z);
+    if (MIC) {
+        dx = mic(dx, a.Lx);
+        dy = mic(dy, a.Ly);
+        dz = mic(dz, a.Lz);
+    }
+    float d2 = __fmul_rn(dx, dx);
+    if (FMA) {
+        d2 = __fmaf_rn(dy, dy, d2);
+        d2 = __fmaf_rn(dz, dz, d2);
+    } else {
+        d2 = __fadd_rn(d2, __fmul_rn(dy, dy));
+        d2 = __fadd_rn(d2, __fmul_rn(dz, dz));
+    }
+    return d2;
+}
+
+template <bool FMA, bool MIC>
+__device__ __forceinline__ void rdf_warp_tile(const RdfArgs &a, float4 pi, int ti, bool act, const float4 *js, int jn,
+                                              int lim, float *d2s, RdfRing &rg, int &head, int &tail, int lane,
+                                              unsigned *hist, bool sh) {
+    unsigned mask = 0;
+    if (act) {
+        if (jn == 32) {
+#pragma unroll
+            for (int q = 0; q < 32; q++) {
+                const float d2 = rdf_d2<FMA, MIC>(a, js[q], pi);
+                d2s[q * 32 + lane] = d2;
+                if (d2 < a.r2f) mask |= 1u << q;
+            }
+        } else {
+            for (int q = 0; q < jn; q++) {
+                const float d2 = rdf_d2<FMA, MIC>(a, js[q], pi);
+                d2s[q * 32 + lane] = d2;
+                if (d2 < a.r2f) mask |= 1u << q;
+            }
+        }
+        if (lim >= 31)
+            mask = 0;
+        else if (lim >= 0)
+            mask &= ~0u << (lim + 1);
+    }
+    const unsigned below = (1u << lane) - 1u;
+    for (;;) {
+        const unsigned m = __ballot_sync(0xffffffffu, mask != 0);
+        if (m == 0) break;
+        if (mask) {
+            const int q = __ffs(mask) - 1;
+            mask &= mask - 1u;
+            const int e = (tail + __popc(m & below)) & (RDF_RING - 1);
+            rg.d2[e] = d2s[q * 32 + lane];
+            rg.code[e] = ti | (ptype_of(js[q]) << 16);
+        }
+        tail += __popc(m);
+        if (tail - head >= 32) {
+            rdf_drain(a, rg, head, 32, lane, hist, sh);
+            head += 32;
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ void rdf_clear(unsigned *hist, int total) {
+    for (int k = threadIdx.x; k < total; k += blockDim.x) hist[k] = 0;
+    __syncthreads();
+}
+
+__device__ __forceinline__ void rdf_flush(const RdfArgs &a, unsigned *hist, int total) {
     __syncthreads();
     for (int k = threadIdx.x; k < total; k += blockDim.x)
         if (hist[k]) atomicAdd(&a.out[k], (unsigned long long)hist[k]);
 }
 
-// all pairs: block = RDF_TILE particles i; j tiles through shared memory
-__global__ void __launch_bounds__(RDF_TILE) k_rdf_allpairs(RdfArgs a) {
+// All pairs, each unordered pair once.  Tiles of RDF_TILE particles; i-tile b
+// meets j-tiles b + k (mod T) for k = 0 .. T/2 (k = 0: j > i; for even T the
+// tile pair at distance T/2 belongs to the lower tile), so every i-tile has
+// the same work; blockIdx.y takes slice y of that k range (small systems still
+// fill the GPU).
+template <bool FMA>
+__global__ void __launch_bounds__(RDF_THREADS) k_rdf_allpairs(RdfArgs a, const float4 *pos) {
     extern __shared__ unsigned char smraw[];
     float4 *tile = (float4 *)smraw;
-    unsigned *hist = (unsigned *)(tile + RDF_TILE);
+    float *d2s = (float *)(tile + RDF_TILE);  // [RDF_WARPS][32][32]
+    RdfRing *rings = (RdfRing *)(d2s + RDF_WARPS * 1024);
+    unsigned *hist = (unsigned *)(rings + RDF_WARPS);
     const int total = a.nt * a.nt * a.bins;
     const bool sh = total <= RDF_SMEM_MAX_BINS;
-    if (sh)
-        for (int k = threadIdx.x; k < total; k += blockDim.x) hist[k] = 0;
-    const int i = blockIdx.x * RDF_TILE + threadIdx.x;
+    if (sh) rdf_clear(hist, total);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float *wd2 = d2s + w * 1024;
+    RdfRing &rg = rings[w];
+    int head = 0, tail = 0;
+    const int T = (a.n + RDF_TILE - 1) / RDF_TILE;
+    const int b = blockIdx.x;
+    const int i = b * RDF_TILE + threadIdx.x;
     const bool act = i < a.n;
-    const float4 pi = act ? a.pos[i] : make_float4(0, 0, 0, 0);
+    const float4 pi = act ? pos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const int ti = ptype_of(pi);
-    for (int j0 = 0; j0 < a.n; j0 += RDF_TILE) {
-        __syncthreads();
-        const int jl = j0 + threadIdx.x;
-        if (jl < a.n) tile[threadIdx.x] = a.pos[jl];
-        __syncthreads();
+    const int kmax = (T % 2 == 0 && b >= T / 2) ? T / 2 - 1 : T / 2;
+    const int per = (T / 2 + gridDim.y) / gridDim.y;  // ceil((T / 2 + 1) / S)
+    const int k_end = min(kmax + 1, ((int)blockIdx.y + 1) * per);
+    for (int k = blockIdx.y * per; k < k_end; k++) {
+        const int jt = (b + k) % T;
+        const int j0 = jt * RDF_TILE;
         const int jn = min(RDF_TILE, a.n - j0);
-        if (act)
-            for (int q = 0; q < jn; q++) {
-                if (j0 + q == i) continue;
-                rdf_pair(a, tile[q], pi, ti, hist, sh);
-            }
+        __syncthreads();
+        if (threadIdx.x < jn) tile[threadIdx.x] = pos[j0 + threadIdx.x];
+        __syncthreads();
+        for (int q0 = 0; q0 < jn; q0 += 32)
+            rdf_warp_tile<FMA, true>(a, pi, ti, act, tile + q0, min(32, jn - q0), k == 0 ? i - (j0 + q0) : -1, wd2,
+                                     rg, head, tail, lane, hist, sh);
     }
-    if (sh) flush_hist(a, hist, total);
+    rdf_drain(a, rg, head, tail - head, lane, hist, sh);
+    if (sh) rdf_flush(a, hist, total);
 }
 
-// cell-based pair search for r_max < L/3
+// Cell search for r_max < L/3: particles sorted by cell (cells of edge >=
+// r_max, at least 3 per side).  A unit of work is 32 home particles of one
+// cell (unit u: cell u / K, particles 32 (u % K) on, K = chunks of the
+// fullest cell; units past a cell's end are empty), taken a unit per warp,
+// against the home cell (j > i) and the 13 neighbour cells of the half shell
+// (offsets after the centre in z-y-x order).  Each pair of neighbouring cells
+// is visited from exactly one side, each pair of particles once.
+//
+// Plain differences between cells that are both off the box faces (cell
+// index 1 .. nc-2 in every dimension): such particles lie at least one cell
+// edge inside the box, so a pair whose difference the minimum image would
+// fold is more than two edges (>= 2 r_max) apart in that component in both
+// images; pairs in range have |dr| < L/2 and are left unchanged by it.  When
+// any position lies outside [-L/2, L/2] (*outside set by the binning) every
+// cell takes the minimum image.
+template <bool FMA>
+__global__ void __launch_bounds__(RDF_THREADS) k_rdf_cells(RdfArgs a, const float4 *spos, const int *start,
+                                                           const int *outside, int ncx, int ncy, int ncz) {
+    extern __shared__ unsigned char smraw[];
+    float4 *jbuf = (float4 *)smraw;  // [RDF_WARPS][32]
+    float *d2s = (float *)(jbuf + RDF_THREADS);
+    RdfRing *rings = (RdfRing *)(d2s + RDF_WARPS * 1024);
+    unsigned *hist = (unsigned *)(rings + RDF_WARPS);
+    const int total = a.nt * a.nt * a.bins;
+    const bool sh = total <= RDF_SMEM_MAX_BINS;
+    if (sh) rdf_clear(hist, total);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    float4 *js = jbuf + 32 * w;
+    float *wd2 = d2s + w * 1024;
+    RdfRing &rg = rings[w];
+    int head = 0, tail = 0;
+    const bool inside = *outside == 0;
+    const int ncell = ncx * ncy * ncz;
+    const int K = start[ncell + 1];
+    const long long units = (long long)ncell * K;
+    for (long long u = (long long)blockIdx.x * RDF_WARPS + w; u < units; u += (long long)gridDim.x * RDF_WARPS) {
+        const int c = (int)(u / K);
+        const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
+        const int h1 = start[c + 1];
+        const int i0 = start[c] + 32 * (int)(u % K);
+        if (i0 >= h1) continue;
+        const int i = i0 + lane;
+        const bool act = i < h1;
+        const float4 pi = act ? spos[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const int ti = ptype_of(pi);
+        const bool home_in = inside && cx >= 1 && cx <= ncx - 2 && cy >= 1 && cy <= ncy - 2 && cz >= 1 &&
+                             cz <= ncz - 2;
+        for (int s = 13; s < 27; s++) {
+            int j0, j1;
+            bool plain = home_in;
+            if (s == 13) {
+                j0 = i0;
+                j1 = h1;
+            } else {
+                const int x = cx + s % 3 - 1, y = cy + (s / 3) % 3 - 1, z = cz + s / 9 - 1;
+                plain = plain && x >= 1 && x <= ncx - 2 && y >= 1 && y <= ncy - 2 && z >= 1 && z <= ncz - 2;
+                const int nb = (((z + ncz) % ncz) * ncy + (y + ncy) % ncy) * ncx + (x + ncx) % ncx;
+                j0 = start[nb];
+                j1 = start[nb + 1];
+            }
+            for (; j0 < j1; j0 += 32) {
+                const int jn = min(32, j1 - j0);
+                __syncwarp();
+                if (lane < jn) js[lane] = spos[j0 + lane];
+                __syncwarp();
+                const int lim = s == 13 ? i - j0 : -1;
+                if (plain)
+                    rdf_warp_tile<FMA, false>(a, pi, ti, act, js, jn, lim, wd2, rg, head, tail, lane, hist, sh);
+                else
+                    rdf_warp_tile<FMA, true>(a, pi, ti, act, js, jn, lim, wd2, rg, head, tail, lane, hist, sh);
+            }
+        }
+    }
+    rdf_drain(a, rg, head, tail - head, lane, hist, sh);
+    if (sh) rdf_flush(a, hist, total);
+}
+
+// cell binning for the cell search: a counting sort of the positions;
+// *outside = 1 when a coordinate is outside [-L/2, L/2] (or not a number)
 __global__ void k_bin_cells(const float4 *pos, int n, float Lx, float Ly, float Lz, int ncx, int ncy, int ncz,
-                            int *pcell, int *prank, int *count) {
+                            int *pcell, int *prank, int *count, int *outside) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4 p = pos[i];
@@ -134,7 +362,10 @@ __global__ void k_bin_cells(const float4 *pos, int n, float Lx, float Ly, float 
     const float L[3] = {Lx, Ly, Lz};
     const int nc[3] = {ncx, ncy, ncz};
     int c[3];
+    bool out = false;
     for (int k = 0; k < 3; k++) {
+        const float h = 0.5f * L[k];
+        out = out || !(r[k] >= -h && r[k] <= h);
         float f = (r[k] / L[k] + 0.5f) * nc[k];
         int ci = (int)floorf(f);
         if (!(f == f)) ci = 0;
@@ -142,70 +373,61 @@ __global__ void k_bin_cells(const float4 *pos, int n, float Lx, float Ly, float 
         if (ci < 0) ci += nc[k];
         c[k] = ci;
     }
+    if (out) *outside = 1;
     const int cid = (c[2] * ncy + c[1]) * ncx + c[0];
     pcell[i] = cid;
     prank[i] = atomicAdd(&count[cid], 1);
 }
-
-__global__ void k_cells_scan_serial(const int *count, int *start, int ncell) {
-    // small cell grids only (r_max >= a few sigma): a single thread is enough
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        int s = 0;
-        for (int c = 0; c < ncell; c++) {
-            start[c] = s;
-            s += count[c];
+// exclusive prefix sum of the cell counts (start[ncell] = total) and the
+// 32-particle chunks of the fullest cell (start[ncell + 1]), one block of
+// 1024 threads, each over a contiguous run of cells
+constexpr int SCAN_THREADS = 1024;
+__global__ void __launch_bounds__(SCAN_THREADS) k_cells_scan(const int *count, int *start, int ncell) {
+    __shared__ int wsum[SCAN_THREADS / 32];
+    __shared__ int cmax;
+    if (threadIdx.x == 0) cmax = 0;
+    const int per = (ncell + SCAN_THREADS - 1) / SCAN_THREADS;
+    const int c0 = min(ncell, (int)threadIdx.x * per), c1 = min(ncell, c0 + per);
+    int s = 0, m = 0;
+    for (int c = c0; c < c1; c++) {
+        s += count[c];
+        m = max(m, count[c]);
+    }
+    __syncthreads();
+    atomicMax(&cmax, m);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    int x = s;  // inclusive scan within the warp
+    for (int o = 1; o < 32; o <<= 1) {
+        const int y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= o) x += y;
+    }
+    if (lane == 31) wsum[w] = x;
+    __syncthreads();
+    if (w == 0) {
+        int v = wsum[lane];
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, v, o);
+            if (lane >= o) v += y;
         }
-        start[ncell] = s;
+        wsum[lane] = v;
+    }
+    __syncthreads();
+    int run = x - s + (w > 0 ? wsum[w - 1] : 0);
+    for (int c = c0; c < c1; c++) {
+        start[c] = run;
+        run += count[c];
+    }
+    if (threadIdx.x == SCAN_THREADS - 1) {
+        start[ncell] = run;
+        start[ncell + 1] = (cmax + 31) / 32;
     }
 }
 
-__global__ void k_cells_scatter(const int *pcell, const int *prank, const int *start, int *perm, int n) {
+__global__ void k_cells_scatter(const float4 *pos, const int *pcell, const int *prank, const int *start,
+                                float4 *spos, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    perm[start[pcell[i]] + prank[i]] = i;
-}
-
-__global__ void __launch_bounds__(RDF_TILE) k_rdf_cells(RdfArgs a, const int *perm, const int *start, int ncx,
-                                                        int ncy, int ncz) {
-    extern __shared__ unsigned char smraw[];
-    unsigned *hist = (unsigned *)smraw;
-    const int total = a.nt * a.nt * a.bins;
-    const bool sh = total <= RDF_SMEM_MAX_BINS;
-    if (sh) {
-        for (int k = threadIdx.x; k < total; k += blockDim.x) hist[k] = 0;
-        __syncthreads();
-    }
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < a.n) {
-        const int i = perm[s];
-        const float4 pi = a.pos[i];
-        const int ti = ptype_of(pi);
-        // cell of particle i from its slot: find via position (same formula as k_bin_cells)
-        const float r[3] = {pi.x, pi.y, pi.z};
-        const float L[3] = {a.Lx, a.Ly, a.Lz};
-        const int nc[3] = {ncx, ncy, ncz};
-        int c[3];
-        for (int k = 0; k < 3; k++) {
-            float f = (r[k] / L[k] + 0.5f) * nc[k];
-            int ci = (int)floorf(f);
-            if (!(f == f)) ci = 0;
-            ci %= nc[k];
-            if (ci < 0) ci += nc[k];
-            c[k] = ci;
-        }
-        for (int dz = -1; dz <= 1; dz++)
-            for (int dy = -1; dy <= 1; dy++)
-                for (int dx = -1; dx <= 1; dx++) {
-                    const int x = (c[0] + dx + ncx) % ncx, y = (c[1] + dy + ncy) % ncy, z = (c[2] + dz + ncz) % ncz;
-                    const int cid = (z * ncy + y) * ncx + x;
-                    for (int q = start[cid]; q < start[cid + 1]; q++) {
-                        const int j = perm[q];
-                        if (j == i) continue;
-                        rdf_pair(a, a.pos[j], pi, ti, hist, sh);
-                    }
-                }
-    }
-    if (sh) flush_hist(a, hist, total);
+    spos[start[pcell[i]] + prank[i]] = pos[i];
 }
 
 // ---------------------------------------------------------------------------
@@ -299,35 +521,42 @@ __global__ void k_pack_pos(int n, const float *r, const int *pt, float4 *pos, in
 // ---------------------------------------------------------------------------
 // host implementations working on device-resident positions
 // ---------------------------------------------------------------------------
+// smallest float32 >= x
+static float float_at_or_above(double x) {
+    float f = (float)x;
+    if ((double)f < x) f = nextafterf(f, INFINITY);
+    return f;
+}
+
 static int rdf_device(gdb_sim *h, cudaStream_t st, const float4 *pos, int n, const float *box, int nt, int bins,
                       double r_max, uint64_t *out_host) {
     if (bins < 1 || nt < 1) return aset(h, GDB_ERR_ARG, "rdf: bins and ntypes must be positive");
+    if (nt > 0xffff) return aset(h, GDB_ERR_ARG, "rdf: too many particle types");
     float minL = fminf(box[0], fminf(box[1], box[2]));
     // the reference: min_box_dim float32, (min_box_dim / 2) float64
     const double half = (double)minL / 2.0;
     if (r_max <= 0.0) r_max = half;
     if (r_max > half) return aset(h, GDB_ERR_ARG, "rdf: r_max must not exceed min(L)/2");
     RdfArgs a;
-    a.pos = pos;
     a.n = n;
     a.nt = nt;
     a.bins = bins;
     a.Lx = box[0];
     a.Ly = box[1];
     a.Lz = box[2];
-    a.r_max = r_max;
+    a.r2f = float_at_or_above(r_max * r_max);
+    a.rf = float_at_or_above(r_max);
     a.width = r_max / (double)bins;
-    a.r_max_sq = r_max * r_max;
-    {
-        const char *fm = getenv("GDB_NBLIST_FMA");
-        a.fma = (fm && fm[0] == '0') ? 0 : 1;
-    }
+    a.inv_width = 1.0 / a.width;
+    const char *fm = getenv("GDB_NBLIST_FMA");
+    const bool fma = !(fm && fm[0] == '0');
     const size_t total = (size_t)nt * nt * bins;
+    ACK(timing_begin(h, st));
     unsigned long long *dout = nullptr;
     ACK(cudaMallocAsync(&dout, total * sizeof(unsigned long long), st));
     ACK(cudaMemsetAsync(dout, 0, total * sizeof(unsigned long long), st));
     a.out = dout;
-    const bool sh = total <= (size_t)RDF_SMEM_MAX_BINS;
+    const size_t hist_bytes = total <= (size_t)RDF_SMEM_MAX_BINS ? total * sizeof(unsigned) : 0;
     int nc[3];
     bool cells = true;
     for (int k = 0; k < 3; k++) {
@@ -336,38 +565,60 @@ static int rdf_device(gdb_sim *h, cudaStream_t st, const float4 *pos, int n, con
         nc[k] = (int)floor(box[k] / (r_max * (1.0 + 1e-4)));
         if (nc[k] < 3) cells = false;
     }
+    const long long ncell = cells ? (long long)nc[0] * nc[1] * nc[2] : 0;
+    if (ncell > (1LL << 28)) cells = false;  // r_max tiny against L: fall back to all pairs
     if (!cells) {
-        const size_t smem = RDF_TILE * sizeof(float4) + (sh ? total * sizeof(unsigned) : 0);
-        ACK(cudaFuncSetAttribute(k_rdf_allpairs, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_rdf_allpairs<<<(n + RDF_TILE - 1) / RDF_TILE, RDF_TILE, smem, st>>>(a);
+        const size_t smem = RDF_TILE * sizeof(float4) + RDF_WARPS * (1024 * sizeof(float) + sizeof(RdfRing)) +
+                            hist_bytes;
+        const int T = (n + RDF_TILE - 1) / RDF_TILE;
+        int dev = 0, sms = 0, per_sm = 0;
+        ACK(cudaGetDevice(&dev));
+        ACK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        auto kern = fma ? k_rdf_allpairs<true> : k_rdf_allpairs<false>;
+        ACK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ACK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RDF_THREADS, smem));
+        // slices of the tile-distance range: about two waves of blocks in all
+        const int slots = sms * std::max(per_sm, 1);
+        const int S = std::max(1, std::min(T / 2 + 1, (2 * slots + T - 1) / T));
+        kern<<<dim3(T, S), RDF_THREADS, smem, st>>>(a, pos);
         ACK(cudaGetLastError());
     } else {
-        const long long ncell = (long long)nc[0] * nc[1] * nc[2];
-        int *count = nullptr, *start = nullptr, *pcell = nullptr, *prank = nullptr, *perm = nullptr;
-        ACK(cudaMallocAsync(&count, ncell * sizeof(int), st));
-        ACK(cudaMallocAsync(&start, (ncell + 1) * sizeof(int), st));
+        int *count = nullptr, *start = nullptr, *pcell = nullptr, *prank = nullptr;
+        float4 *spos = nullptr;
+        ACK(cudaMallocAsync(&count, (ncell + 1) * sizeof(int), st));  // [ncell]: the outside flag
+        ACK(cudaMallocAsync(&start, (ncell + 2) * sizeof(int), st));
         ACK(cudaMallocAsync(&pcell, (size_t)n * sizeof(int), st));
         ACK(cudaMallocAsync(&prank, (size_t)n * sizeof(int), st));
-        ACK(cudaMallocAsync(&perm, (size_t)n * sizeof(int), st));
-        ACK(cudaMemsetAsync(count, 0, ncell * sizeof(int), st));
+        ACK(cudaMallocAsync(&spos, (size_t)n * sizeof(float4), st));
+        ACK(cudaMemsetAsync(count, 0, (ncell + 1) * sizeof(int), st));
         const int g = (n + 255) / 256;
-        k_bin_cells<<<g, 256, 0, st>>>(pos, n, box[0], box[1], box[2], nc[0], nc[1], nc[2], pcell, prank, count);
-        k_cells_scan_serial<<<1, 1, 0, st>>>(count, start, (int)ncell);
-        k_cells_scatter<<<g, 256, 0, st>>>(pcell, prank, start, perm, n);
-        const size_t smem = sh ? total * sizeof(unsigned) : 0;
-        ACK(cudaFuncSetAttribute(k_rdf_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        k_rdf_cells<<<(n + RDF_TILE - 1) / RDF_TILE, RDF_TILE, smem, st>>>(a, perm, start, nc[0], nc[1], nc[2]);
+        k_bin_cells<<<g, 256, 0, st>>>(pos, n, box[0], box[1], box[2], nc[0], nc[1], nc[2], pcell, prank, count,
+                                      count + ncell);
+        k_cells_scan<<<1, SCAN_THREADS, 0, st>>>(count, start, (int)ncell);
+        k_cells_scatter<<<g, 256, 0, st>>>(pos, pcell, prank, start, spos, n);
+        const size_t smem = RDF_THREADS * sizeof(float4) + RDF_WARPS * (1024 * sizeof(float) + sizeof(RdfRing)) +
+                            hist_bytes;
+        int dev = 0, sms = 0, per_sm = 0;
+        ACK(cudaGetDevice(&dev));
+        ACK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        auto kern = fma ? k_rdf_cells<true> : k_rdf_cells<false>;
+        ACK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        ACK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, RDF_THREADS, smem));
+        const int grid = sms * std::max(per_sm, 1);  // warps stride over the units
+        kern<<<grid, RDF_THREADS, smem, st>>>(a, spos, start, count + ncell, nc[0], nc[1], nc[2]);
         ACK(cudaGetLastError());
         ACK(cudaFreeAsync(count, st));
         ACK(cudaFreeAsync(start, st));
         ACK(cudaFreeAsync(pcell, st));
         ACK(cudaFreeAsync(prank, st));
-        ACK(cudaFreeAsync(perm, st));
+        ACK(cudaFreeAsync(spos, st));
     }
     std::vector<unsigned long long> tmp(total);
     ACK(cudaMemcpyAsync(tmp.data(), dout, total * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    ACK(timing_end(h, st));
     ACK(cudaFreeAsync(dout, st));
     ACK(cudaStreamSynchronize(st));
+    timing_store(h);
     for (size_t k = 0; k < total; k++) out_host[k] += tmp[k];
     return GDB_OK;
 }
@@ -396,6 +647,7 @@ static int sq_device(gdb_sim *h, cudaStream_t st, const float4 *pos, const int *
     int *dn = nullptr;
     float *dff = nullptr;
     double *acc = nullptr;
+    ACK(timing_begin(h, st));
     ACK(cudaMallocAsync(&dn, (size_t)nq * 3 * sizeof(int), st));
     ACK(cudaMallocAsync(&acc, (size_t)nq * 2 * sizeof(double), st));
     ACK(cudaMemcpyAsync(dn, nvec_host, (size_t)nq * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -417,10 +669,12 @@ static int sq_device(gdb_sim *h, cudaStream_t st, const float4 *pos, const int *
     ACK(cudaGetLastError());
     std::vector<double> tmp((size_t)nq * 2);
     ACK(cudaMemcpyAsync(tmp.data(), acc, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    ACK(timing_end(h, st));
     ACK(cudaFreeAsync(dn, st));
     ACK(cudaFreeAsync(acc, st));
     if (dff) ACK(cudaFreeAsync(dff, st));
     ACK(cudaStreamSynchronize(st));
+    timing_store(h);
     const double norm = 1.0 / sqrt(nf);
     for (int q = 0; q < nq; q++) {
         re[q] = tmp[2 * q] * norm;

@@ -107,6 +107,7 @@ struct gdb_sim {
     cudaGraphExec_t gexec[2] = {nullptr, nullptr};
     int graph_steps = 0;
     bool use_graphs = true;
+    float analysis_ms = 0.f;  // device time of the last RDF / S(q) call
     char err[512] = "";
 };
 
@@ -1516,5 +1517,13 @@ int gdb_internal_ntypes(gdb_sim *h) { return h->ntypes; }
 int gdb_internal_dev(gdb_sim *h) { return h->dev; }
 int gdb_internal_uploaded(gdb_sim *h) { return h->uploaded ? 1 : 0; }
 char *gdb_internal_err(gdb_sim *h) { return h ? h->err : g_lib_error; }
+cudaEvent_t gdb_internal_event(gdb_sim *h, int k) { return k ? h->ev1 : h->ev0; }
+void gdb_internal_set_analysis_ms(gdb_sim *h, float ms) { h->analysis_ms = ms; }
+
+int gdb_last_analysis_ms(gdb_sim *h, float *ms) {
+    if (!h || !ms) return set_err(h, GDB_ERR_ARG, "gdb_last_analysis_ms: NULL argument");
+    *ms = h->analysis_ms;
+    return GDB_OK;
+}
 
 }  // extern "C"

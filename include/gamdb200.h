@@ -208,6 +208,13 @@ int gdb_rdf_update(gdb_sim *h, int bins, double r_max, uint64_t *out);
 int gdb_sq_update(gdb_sim *h, int nq, const int32_t *n_vectors, const float *ff, double *rho_re,
                   double *rho_im);
 
+/* Device time in ms (CUDA events on the handle's stream) of the handle's
+ * last gdb_rdf_update or gdb_sq_update call: its device work, from the first
+ * copy or kernel to the result's copy back.  A measurement aid with no
+ * counterpart in the reference, which times its calculators with wall
+ * clocks around update() (e.g. examples/structure_factor.py). */
+int gdb_last_analysis_ms(gdb_sim *h, float *ms);
+
 /* Stand-alone calculators on host arrays (no handle): same semantics as the
  * two calls above, for callers that only hold a configuration
  * (CalculatorRadialDistribution.update / CalculatorStructureFactor.update). */

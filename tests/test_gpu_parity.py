@@ -220,6 +220,59 @@ def test_rdf_short_range_cells_vs_oracle(oracle):
     assert np.array_equal(allpairs, oracle.rdf(conf["r"], conf.ptype, L, 500, fma=1))
 
 
+def _random_types(n, nt, seed):
+    return np.random.default_rng(seed).integers(0, nt, n).astype(np.int32)
+
+
+@pytest.mark.parametrize("case", [
+    # (n, types, bins, r_max as a fraction of L, fused distance form)
+    (3000, 3, 200, 0.333, 1),  # three cells per side: the half shell wraps onto itself
+    (3000, 2, 7000, 0.25, 1),  # 28 000 bins: histogram in global memory (cell path)
+    (2501, 2, 7000, 0.0, 1),  # 28 000 bins, all pairs
+    (1000, 1, 64, 0.2, 0),  # unfused distance form, cell path
+    (777, 3, 50, 0.0, 0),  # unfused, all pairs, odd tile count
+    (2, 1, 10, 0.0, 1),  # one pair
+])
+def test_rdf_paths_and_edges_vs_oracle(oracle, case, monkeypatch):
+    """Cell and all-pairs searches, shared and global histograms, both
+    distance forms: bit-exact counts against the oracle's all pairs."""
+    n, nt, bins, frac, fma = case
+    conf = workloads.ka_configuration(max(n, 4), rho=1.1, seed=n, jitter=0.3)
+    r = conf["r"][:n].copy()
+    L = conf.simbox.lengths
+    pt = _random_types(n, nt, n)
+    r_max = frac * float(np.min(L))
+    monkeypatch.setenv("GDB_NBLIST_FMA", str(fma))
+    got = _lib.rdf_compute(r, pt, L, nt, bins, r_max=r_max)
+    ref = oracle.rdf(r, pt, L, bins, fma=fma, r_max=r_max)
+    if ref.shape[0] < nt:  # the oracle sizes its histogram by the largest type present
+        ref = np.pad(ref, ((0, nt - ref.shape[0]), (0, nt - ref.shape[1]), (0, 0)))
+    assert got.sum() == ref.sum() and np.array_equal(got, ref)
+    if n > 2:
+        assert got.sum() > 0
+
+
+@pytest.mark.parametrize("outside", [False, True])
+@pytest.mark.parametrize("frac", [0.1, 0.2, 0.333])
+def test_rdf_cells_faces_and_outside_positions_vs_oracle(oracle, frac, outside):
+    """Particles exactly on the +-L/2 faces (the +L/2 face bins into cell 0)
+    and, in the second form, particles one box length outside: the cell
+    search must count what the minimum image gives, bit for bit."""
+    conf = workloads.ka_configuration(4000, rho=1.1, seed=17, jitter=0.3)
+    r = conf["r"].copy()
+    L = conf.simbox.lengths.astype(np.float32)
+    for k, idx in enumerate((3, 40, 77, 150, 600, 901)):
+        r[idx, k % 3] = (L[k % 3] / np.float32(2.0)) * np.float32(1 if k % 2 == 0 else -1)
+    if outside:
+        r[1000:1040, 0] += L[0]
+        r[2000:2010, 2] -= L[2]
+    pt = conf.ptype
+    r_max = frac * float(np.min(L))
+    got = _lib.rdf_compute(r, pt, L, 2, 300, r_max=r_max)
+    ref = oracle.rdf(r, pt, L, 300, fma=1, r_max=r_max)
+    assert got.sum() > 0 and np.array_equal(got, ref)
+
+
 def test_rdf_device_path_matches_host_path(oracle):
     d = golden("ka1372_cells")
     conf = gp.Configuration(D=3)
@@ -232,6 +285,7 @@ def test_rdf_device_path_matches_host_path(oracle):
     out = np.zeros((2, 2, 100), np.uint64)
     sim.rdf_update(100, 0.0, out)
     assert np.array_equal(out, oracle.rdf(d["r"], d["ptype"], d["box"], 100, fma=1))
+    assert sim.last_analysis_ms() > 0.0
 
 
 def test_sq_vs_gamdpy_and_oracle(oracle):
