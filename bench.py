@@ -423,15 +423,18 @@ def run_lj_large(args):
     clocks.start()
     t_md = t_rdf = t_sq = 0.0  # device times (CUDA events on the library's stream)
     w_rdf = w_sq = 0.0  # wall times of the update() calls
+    each_rdf, each_sq = [], []
     t0 = time.perf_counter()
     for b in range(nblocks):
         t_md += dev.run(float(b * every * 0.004), every) / 1e3
         t1 = time.perf_counter()
         rdf.update()
-        t_rdf += dev.last_analysis_ms() / 1e3
+        each_rdf.append(dev.last_analysis_ms())
+        t_rdf += each_rdf[-1] / 1e3
         t2 = time.perf_counter()
         sq.update()
-        t_sq += dev.last_analysis_ms() / 1e3
+        each_sq.append(dev.last_analysis_ms())
+        t_sq += each_sq[-1] / 1e3
         t3 = time.perf_counter()
         w_rdf += t2 - t1
         w_sq += t3 - t2
@@ -450,6 +453,7 @@ def run_lj_large(args):
                    "rdf_ms_per_update": t_rdf * 1e3 / nblocks, "rdf_pairs_per_update": pairs,
                    "rdf_pairs_per_s": pairs * nblocks / t_rdf if t_rdf > 0 else None,
                    "sq_ms_per_update": t_sq * 1e3 / nblocks, "sq_terms_per_s": n * nq * nblocks / t_sq if t_sq > 0 else None,
+                   "rdf_ms_min_max": [min(each_rdf), max(each_rdf)], "sq_ms_min_max": [min(each_sq), max(each_sq)],
                    "rdf_wall_ms_per_update": w_rdf * 1e3 / nblocks, "sq_wall_ms_per_update": w_sq * 1e3 / nblocks,
                    "wall_s": wall, "timing": "device (CUDA events) for MD, RDF and S(q); wall times beside them",
                    "l2": "working set of several GB > 126 MB L2, no flush"},

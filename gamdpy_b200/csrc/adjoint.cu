@@ -44,6 +44,7 @@
 #include <vector>
 
 #include "../../include/gamdb200.h"
+#include "gdb_internal.cuh"
 
 namespace {
 
@@ -720,8 +721,8 @@ int gdb_adj_forward(gdb_adj *h, const double *params, const float *r0, const flo
     int rc = ensure_list(h);
     if (rc) return rc;
     float *dr = nullptr, *dv = nullptr;
-    ACK(cudaMallocAsync(&dr, (size_t)n * 3 * sizeof(float), h->st));
-    ACK(cudaMallocAsync(&dv, (size_t)n * 3 * sizeof(float), h->st));
+    ACK(gdb::pool_alloc(&dr, (size_t)n * 3 * sizeof(float), h->st));
+    ACK(gdb::pool_alloc(&dv, (size_t)n * 3 * sizeof(float), h->st));
     ACK(cudaMemcpyAsync(dr, r0, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, h->st));
     ACK(cudaMemcpyAsync(dv, v0, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, h->st));
     k_adj_pack<<<(n + 255) / 256, 256, 0, h->st>>>(n, dr, dv, h->d_type, h->d_pos[0], h->d_vel[0]);

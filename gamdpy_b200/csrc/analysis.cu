@@ -448,65 +448,112 @@ struct SqArgs {
     double *acc;  // nq x 2
 };
 
+// One (particle, q) term of rho_q: (e_x e_y) e_z, times the form factor w
+// when weighted, added to (tr, ti).  The roundings are written out, so every
+// kernel that sums with it gives the same float32 partial sums.
+__device__ __forceinline__ void sq_term(float2 ex, float2 ey, float2 ez, float w, bool weighted, float &tr,
+                                        float &ti) {
+    const float xr = __fmaf_rn(ex.x, ey.x, -__fmul_rn(ex.y, ey.y));
+    const float xi = __fmaf_rn(ex.x, ey.y, __fmul_rn(ex.y, ey.x));
+    const float cr = __fmaf_rn(xr, ez.x, -__fmul_rn(xi, ez.y));
+    const float ci = __fmaf_rn(xr, ez.y, __fmul_rn(xi, ez.x));
+    if (weighted) {
+        tr = __fmaf_rn(w, cr, tr);
+        ti = __fmaf_rn(w, ci, ti);
+    } else {
+        tr = __fadd_rn(tr, cr);
+        ti = __fadd_rn(ti, ci);
+    }
+}
+
+// One block: QPT x SQ_THREADS q-vectors (q = blockIdx.x QPT 256 + k 256 + t)
+// against SQ_CHUNK particles.  Per tile of SQ_TILE particles the block
+// tabulates e_d(k) = exp(2 pi i k x_d / L_d) once (sincospif, float32) and
+// every thread accumulates its QPT q-vectors from the table: two complex
+// products per (particle, q), float32 within a tile, float64 across tiles.
+template <int QPT, bool FF>
 __global__ void __launch_bounds__(SQ_THREADS) k_sq(SqArgs a) {
     extern __shared__ float2 tab[];  // [SQ_TILE][klen0 + klen1 + klen2]
     __shared__ float wsh[SQ_TILE];
-    const int row = a.klen[0] + a.klen[1] + a.klen[2];
-    const int q = blockIdx.x * SQ_THREADS + threadIdx.x;
-    int nx = 0, ny = 0, nz = 0;
-    if (q < a.nq) {
-        nx = a.nvec[3 * q] - a.kmin[0];
-        ny = a.nvec[3 * q + 1] - a.kmin[1] + a.klen[0];
-        nz = a.nvec[3 * q + 2] - a.kmin[2] + a.klen[0] + a.klen[1];
+    __shared__ float4 psh[SQ_TILE];
+    const int k0 = a.klen[0], k01 = a.klen[0] + a.klen[1];
+    const int row = k01 + a.klen[2];
+    int ix[QPT], iy[QPT], iz[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; k++) {
+        const int q = (blockIdx.x * QPT + k) * SQ_THREADS + threadIdx.x;
+        ix[k] = 0, iy[k] = 0, iz[k] = 0;  // inactive slots read entry 0 and are not stored
+        if (q < a.nq) {
+            ix[k] = a.nvec[3 * q] - a.kmin[0];
+            iy[k] = a.nvec[3 * q + 1] - a.kmin[1] + k0;
+            iz[k] = a.nvec[3 * q + 2] - a.kmin[2] + k01;
+        }
     }
-    double sr = 0.0, si = 0.0;
+    double sr[QPT], si[QPT];
+#pragma unroll
+    for (int k = 0; k < QPT; k++) sr[k] = si[k] = 0.0;
+    // this thread's table entries: (pl0, col0) then steps of SQ_THREADS
+    const int dpl = SQ_THREADS / row, dcol = SQ_THREADS % row;
+    const int pl0 = threadIdx.x / row, col0 = threadIdx.x % row;
     const int p_begin = blockIdx.y * SQ_CHUNK;
     const int p_end = min(a.n, p_begin + SQ_CHUNK);
     for (int p0 = p_begin; p0 < p_end; p0 += SQ_TILE) {
         const int np = min(SQ_TILE, p_end - p0);
         __syncthreads();
-        // tabulate e_d(k) = exp(2 pi i k x_d / L_d)
-        for (int e = threadIdx.x; e < np * row; e += SQ_THREADS) {
-            const int pl = e / row, col = e % row;
-            const float4 p = a.pos[p0 + pl];
-            int d, k;
-            if (col < a.klen[0]) {
-                d = 0;
-                k = col + a.kmin[0];
-            } else if (col < a.klen[0] + a.klen[1]) {
-                d = 1;
-                k = col - a.klen[0] + a.kmin[1];
-            } else {
-                d = 2;
-                k = col - a.klen[0] - a.klen[1] + a.kmin[2];
-            }
-            const float x = d == 0 ? p.x : (d == 1 ? p.y : p.z);
-            float s, c;
-            sincospif(2.0f * (float)k * (x * a.invL[d]), &s, &c);
-            tab[pl * row + col] = make_float2(c, s);
-        }
         if (threadIdx.x < np) {
-            const int slot = p0 + threadIdx.x;
-            wsh[threadIdx.x] = a.ff ? a.ff[a.orig[slot]] : 1.0f;
+            psh[threadIdx.x] = a.pos[p0 + threadIdx.x];
+            if (FF) wsh[threadIdx.x] = a.ff[a.orig[p0 + threadIdx.x]];
         }
         __syncthreads();
-        if (q < a.nq) {
-            float tr = 0.f, ti = 0.f;
-            for (int pl = 0; pl < np; pl++) {
-                const float2 ex = tab[pl * row + nx], ey = tab[pl * row + ny], ez = tab[pl * row + nz];
-                const float xr = ex.x * ey.x - ex.y * ey.y, xi = ex.x * ey.y + ex.y * ey.x;
-                const float w = wsh[pl];
-                tr += w * (xr * ez.x - xi * ez.y);
-                ti += w * (xr * ez.y + xi * ez.x);
+        for (int pl = pl0, col = col0; pl < np;) {
+            const int d = (col >= k0) + (col >= k01);
+            const int kk = col - (d == 0 ? 0 : (d == 1 ? k0 : k01)) + a.kmin[d];
+            const float4 p = psh[pl];
+            const float x = d == 0 ? p.x : (d == 1 ? p.y : p.z);
+            float sn, cs;
+            sincospif(2.0f * (float)kk * (x * a.invL[d]), &sn, &cs);
+            tab[pl * row + col] = make_float2(cs, sn);
+            col += dcol;
+            pl += dpl;
+            if (col >= row) {
+                col -= row;
+                pl++;
             }
-            sr += tr;
-            si += ti;
+        }
+        __syncthreads();
+        float tr[QPT], ti[QPT];
+#pragma unroll
+        for (int k = 0; k < QPT; k++) tr[k] = ti[k] = 0.f;
+        for (int pl = 0; pl < np; pl++) {
+            const float2 *t = tab + pl * row;
+            const float w = FF ? wsh[pl] : 1.0f;
+#pragma unroll
+            for (int k = 0; k < QPT; k++) {
+                sq_term(t[ix[k]], t[iy[k]], t[iz[k]], w, FF, tr[k], ti[k]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < QPT; k++) {
+            sr[k] += tr[k];
+            si[k] += ti[k];
         }
     }
-    if (q < a.nq) {
-        atomicAdd(&a.acc[2 * q], sr);
-        atomicAdd(&a.acc[2 * q + 1], si);
+#pragma unroll
+    for (int k = 0; k < QPT; k++) {
+        const int q = (blockIdx.x * QPT + k) * SQ_THREADS + threadIdx.x;
+        if (q < a.nq) {
+            atomicAdd(&a.acc[2 * q], sr[k]);
+            atomicAdd(&a.acc[2 * q + 1], si[k]);
+        }
     }
+}
+
+template <int QPT>
+static void launch_sq(dim3 grid, size_t smem, cudaStream_t st, const SqArgs &a) {
+    if (a.ff)
+        k_sq<QPT, true><<<grid, SQ_THREADS, smem, st>>>(a);
+    else
+        k_sq<QPT, false><<<grid, SQ_THREADS, smem, st>>>(a);
 }
 
 __global__ void k_pack_pos(int n, const float *r, const int *pt, float4 *pos, int *orig) {
@@ -553,7 +600,7 @@ static int rdf_device(gdb_sim *h, cudaStream_t st, const float4 *pos, int n, con
     const size_t total = (size_t)nt * nt * bins;
     ACK(timing_begin(h, st));
     unsigned long long *dout = nullptr;
-    ACK(cudaMallocAsync(&dout, total * sizeof(unsigned long long), st));
+    ACK(pool_alloc(&dout, total * sizeof(unsigned long long), st));
     ACK(cudaMemsetAsync(dout, 0, total * sizeof(unsigned long long), st));
     a.out = dout;
     const size_t hist_bytes = total <= (size_t)RDF_SMEM_MAX_BINS ? total * sizeof(unsigned) : 0;
@@ -585,11 +632,11 @@ static int rdf_device(gdb_sim *h, cudaStream_t st, const float4 *pos, int n, con
     } else {
         int *count = nullptr, *start = nullptr, *pcell = nullptr, *prank = nullptr;
         float4 *spos = nullptr;
-        ACK(cudaMallocAsync(&count, (ncell + 1) * sizeof(int), st));  // [ncell]: the outside flag
-        ACK(cudaMallocAsync(&start, (ncell + 2) * sizeof(int), st));
-        ACK(cudaMallocAsync(&pcell, (size_t)n * sizeof(int), st));
-        ACK(cudaMallocAsync(&prank, (size_t)n * sizeof(int), st));
-        ACK(cudaMallocAsync(&spos, (size_t)n * sizeof(float4), st));
+        ACK(pool_alloc(&count, (ncell + 1) * sizeof(int), st));  // [ncell]: the outside flag
+        ACK(pool_alloc(&start, (ncell + 2) * sizeof(int), st));
+        ACK(pool_alloc(&pcell, (size_t)n * sizeof(int), st));
+        ACK(pool_alloc(&prank, (size_t)n * sizeof(int), st));
+        ACK(pool_alloc(&spos, (size_t)n * sizeof(float4), st));
         ACK(cudaMemsetAsync(count, 0, (ncell + 1) * sizeof(int), st));
         const int g = (n + 255) / 256;
         k_bin_cells<<<g, 256, 0, st>>>(pos, n, box[0], box[1], box[2], nc[0], nc[1], nc[2], pcell, prank, count,
@@ -614,8 +661,8 @@ static int rdf_device(gdb_sim *h, cudaStream_t st, const float4 *pos, int n, con
         ACK(cudaFreeAsync(spos, st));
     }
     std::vector<unsigned long long> tmp(total);
-    ACK(cudaMemcpyAsync(tmp.data(), dout, total * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     ACK(timing_end(h, st));
+    ACK(cudaMemcpyAsync(tmp.data(), dout, total * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     ACK(cudaFreeAsync(dout, st));
     ACK(cudaStreamSynchronize(st));
     timing_store(h);
@@ -648,13 +695,13 @@ static int sq_device(gdb_sim *h, cudaStream_t st, const float4 *pos, const int *
     float *dff = nullptr;
     double *acc = nullptr;
     ACK(timing_begin(h, st));
-    ACK(cudaMallocAsync(&dn, (size_t)nq * 3 * sizeof(int), st));
-    ACK(cudaMallocAsync(&acc, (size_t)nq * 2 * sizeof(double), st));
+    ACK(pool_alloc(&dn, (size_t)nq * 3 * sizeof(int), st));
+    ACK(pool_alloc(&acc, (size_t)nq * 2 * sizeof(double), st));
     ACK(cudaMemcpyAsync(dn, nvec_host, (size_t)nq * 3 * sizeof(int), cudaMemcpyHostToDevice, st));
     ACK(cudaMemsetAsync(acc, 0, (size_t)nq * 2 * sizeof(double), st));
     double nf = 0.0;
     if (ff_host) {
-        ACK(cudaMallocAsync(&dff, (size_t)n * sizeof(float), st));
+        ACK(pool_alloc(&dff, (size_t)n * sizeof(float), st));
         ACK(cudaMemcpyAsync(dff, ff_host, (size_t)n * sizeof(float), cudaMemcpyHostToDevice, st));
         for (int i = 0; i < n; i++) nf += ff_host[i];
     } else {
@@ -663,13 +710,29 @@ static int sq_device(gdb_sim *h, cudaStream_t st, const float4 *pos, const int *
     a.nvec = dn;
     a.ff = dff;
     a.acc = acc;
-    ACK(cudaFuncSetAttribute(k_sq, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    dim3 grid((nq + SQ_THREADS - 1) / SQ_THREADS, (n + SQ_CHUNK - 1) / SQ_CHUNK);
-    k_sq<<<grid, SQ_THREADS, smem, st>>>(a);
+    // q-vectors per thread: up to 4, as few blocks along q as that allows,
+    // spread evenly over them (2219 q: 3 blocks of 3 x 256)
+    const int nbx = (nq + 4 * SQ_THREADS - 1) / (4 * SQ_THREADS);
+    const int qpt = (nq + nbx * SQ_THREADS - 1) / (nbx * SQ_THREADS);
+    const dim3 grid(nbx, (n + SQ_CHUNK - 1) / SQ_CHUNK);
+    const void *fn = nullptr;
+    switch (qpt) {
+        case 1: fn = a.ff ? (const void *)k_sq<1, true> : (const void *)k_sq<1, false>; break;
+        case 2: fn = a.ff ? (const void *)k_sq<2, true> : (const void *)k_sq<2, false>; break;
+        case 3: fn = a.ff ? (const void *)k_sq<3, true> : (const void *)k_sq<3, false>; break;
+        default: fn = a.ff ? (const void *)k_sq<4, true> : (const void *)k_sq<4, false>; break;
+    }
+    ACK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    switch (qpt) {
+        case 1: launch_sq<1>(grid, smem, st, a); break;
+        case 2: launch_sq<2>(grid, smem, st, a); break;
+        case 3: launch_sq<3>(grid, smem, st, a); break;
+        default: launch_sq<4>(grid, smem, st, a); break;
+    }
     ACK(cudaGetLastError());
     std::vector<double> tmp((size_t)nq * 2);
-    ACK(cudaMemcpyAsync(tmp.data(), acc, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     ACK(timing_end(h, st));
+    ACK(cudaMemcpyAsync(tmp.data(), acc, tmp.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     ACK(cudaFreeAsync(dn, st));
     ACK(cudaFreeAsync(acc, st));
     if (dff) ACK(cudaFreeAsync(dff, st));
@@ -781,13 +844,8 @@ __global__ void __launch_bounds__(SQ_THREADS) k_sqna(const float *__restrict__ r
         __syncthreads();
         if (ok) {
             float tr = 0.f, ti = 0.f;
-            for (int pl = 0; pl < np; pl++) {
-                const float2 ex = tab[pl * row + nx], ey = tab[pl * row + ny], ez = tab[pl * row + nz];
-                const float xr = ex.x * ey.x - ex.y * ey.y, xi = ex.x * ey.y + ex.y * ey.x;
-                const float w = wsh[pl];
-                tr += w * (xr * ez.x - xi * ez.y);
-                ti += w * (xr * ez.y + xi * ez.x);
-            }
+            for (int pl = 0; pl < np; pl++)
+                sq_term(tab[pl * row + nx], tab[pl * row + ny], tab[pl * row + nz], wsh[pl], true, tr, ti);
             sr += tr;
             si += ti;
         }
@@ -877,10 +935,10 @@ int gdb_rdf_compute(int n, const float *r, const int32_t *ptype, const float box
     int rc = GDB_OK;
     do {
         cudaError_t e;
-        if ((e = cudaMallocAsync(&dr, (size_t)n * 3 * sizeof(float), st)) ||
-            (e = cudaMallocAsync(&pos, (size_t)n * sizeof(float4), st)) ||
-            (e = cudaMallocAsync(&orig, (size_t)n * sizeof(int), st)) ||
-            (ptype && (e = cudaMallocAsync(&dpt, (size_t)n * sizeof(int), st))) ||
+        if ((e = pool_alloc(&dr, (size_t)n * 3 * sizeof(float), st)) ||
+            (e = pool_alloc(&pos, (size_t)n * sizeof(float4), st)) ||
+            (e = pool_alloc(&orig, (size_t)n * sizeof(int), st)) ||
+            (ptype && (e = pool_alloc(&dpt, (size_t)n * sizeof(int), st))) ||
             (e = cudaMemcpyAsync(dr, r, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, st)) ||
             (ptype && (e = cudaMemcpyAsync(dpt, ptype, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st)))) {
             rc = aset(h, GDB_ERR_CUDA, "gdb_rdf_compute: staging", e);
@@ -910,9 +968,9 @@ int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], i
     int rc = GDB_OK;
     do {
         cudaError_t e;
-        if ((e = cudaMallocAsync(&dr, (size_t)n * 3 * sizeof(float), st)) ||
-            (e = cudaMallocAsync(&pos, (size_t)n * sizeof(float4), st)) ||
-            (e = cudaMallocAsync(&orig, (size_t)n * sizeof(int), st)) ||
+        if ((e = pool_alloc(&dr, (size_t)n * 3 * sizeof(float), st)) ||
+            (e = pool_alloc(&pos, (size_t)n * sizeof(float4), st)) ||
+            (e = pool_alloc(&orig, (size_t)n * sizeof(int), st)) ||
             (e = cudaMemcpyAsync(dr, r, (size_t)n * 3 * sizeof(float), cudaMemcpyHostToDevice, st))) {
             rc = aset(h, GDB_ERR_CUDA, "gdb_sq_compute: staging", e);
             break;

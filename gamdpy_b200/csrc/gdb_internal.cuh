@@ -154,6 +154,17 @@ __device__ __forceinline__ void block_sum(double (&v)[NQ], double *smem /* NQ * 
     __syncthreads();
 }
 
+// Temporaries of the library's calls (staging copies, cell-sort scratch,
+// result buffers) come from a stream-ordered pool per device that the library
+// owns and that keeps up to 1 GiB mapped between calls; the default pool
+// hands its memory back to the driver at every synchronisation, and mapping a
+// few hundred MB again costs tens of ms per call.  Free with cudaFreeAsync.
+cudaError_t pool_alloc_raw(void **p, size_t bytes, cudaStream_t st);
+template <class T>
+inline cudaError_t pool_alloc(T **p, size_t bytes, cudaStream_t st) {
+    return pool_alloc_raw((void **)p, bytes, st);
+}
+
 }  // namespace gdb
 
 // Host-side helpers shared by the translation units.

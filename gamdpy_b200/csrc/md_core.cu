@@ -31,6 +31,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -596,6 +597,43 @@ static int run_cluster(gdb_sim *h, int steps) {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+namespace gdb {
+
+namespace {
+constexpr int POOL_DEVICES = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[POOL_DEVICES] = {};
+}  // namespace
+
+cudaError_t pool_alloc_raw(void **p, size_t bytes, cudaStream_t st) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= POOL_DEVICES) return cudaMallocAsync(p, bytes, st);
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lock(g_pool_mu);
+        if (!g_pool[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            cudaMemPool_t created = nullptr;
+            if ((e = cudaMemPoolCreate(&created, &props)) != cudaSuccess) return e;
+            uint64_t keep = 1ull << 30;
+            if ((e = cudaMemPoolSetAttribute(created, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+                cudaMemPoolDestroy(created);
+                return e;
+            }
+            g_pool[dev] = created;
+        }
+        pool = g_pool[dev];
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
+
+}  // namespace gdb
+
 extern "C" {
 
 int gdb_version(void) { return 100; }
@@ -720,7 +758,7 @@ int gdb_upload_state(gdb_sim *h, const float *r, const float *v, const float *m,
     // staging: one device buffer for the raw host arrays
     char *stage = nullptr;
     const size_t bytes = N * (3 + 3 + 1) * sizeof(float) + N * sizeof(int) + N * 3 * sizeof(int);
-    CK(cudaMallocAsync((void **)&stage, bytes, h->st));
+    CK(pool_alloc(&stage, bytes, h->st));
     float *dr = (float *)stage, *dv = dr + 3 * N, *dm = dv + 3 * N;
     int *dpt = (int *)(dm + N), *dim = dpt + N;
     CK(cudaMemcpyAsync(dr, r, 3 * N * sizeof(float), cudaMemcpyHostToDevice, h->st));
@@ -745,7 +783,7 @@ static int download_planes(gdb_sim *h, const void *src, int kind, void *dst) {
     const size_t N = h->n;
     const size_t bytes = (kind == 2 ? 1 : 3) * N * 4;
     void *tmp = nullptr;
-    CK(cudaMallocAsync(&tmp, bytes, h->st));
+    CK(pool_alloc(&tmp, bytes, h->st));
     if (kind == 0)
         k_unpack3<<<grid_for(h->n), GDB_BLOCK, 0, h->st>>>(h->n, (const float4 *)src, h->orig, (float *)tmp);
     else if (kind == 1)

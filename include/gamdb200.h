@@ -210,7 +210,7 @@ int gdb_sq_update(gdb_sim *h, int nq, const int32_t *n_vectors, const float *ff,
 
 /* Device time in ms (CUDA events on the handle's stream) of the handle's
  * last gdb_rdf_update or gdb_sq_update call: its device work, from the first
- * copy or kernel to the result's copy back.  A measurement aid with no
+ * copy or kernel to the last kernel (the result's copy back not included).  A measurement aid with no
  * counterpart in the reference, which times its calculators with wall
  * clocks around update() (e.g. examples/structure_factor.py). */
 int gdb_last_analysis_ms(gdb_sim *h, float *ms);
