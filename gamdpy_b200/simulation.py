@@ -47,7 +47,9 @@ def get_default_compute_plan(configuration):
     num_SM = B200_NUM_SM
     num_cc_cores = B200_CORES_PER_SM * num_SM
     pb = 512
-    while N // pb < 2 * num_SM:
+    # gamdpy's loop halves pb to zero (and divides by it) when N < 2 x 148;
+    # it stops at one here, and the clamp below makes that 8
+    while pb > 1 and N // pb < 2 * num_SM:
         pb = pb // 2
     pb = min(max(pb, 8), 256)
     tp = 1

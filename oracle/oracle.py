@@ -159,6 +159,38 @@ def forces(r, ptype, box, table, nbl, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF,
     return {"f": f, "U": U, "W": W, "lapU": lap, "Fsq": fsq}
 
 
+def forces_fp64(r, ptype, box, sigma, epsilon, cut, nbl):
+    """Forces of the shifted-force LJ_12_6_sigma_epsilon pair potential over
+    a neighbour list, every operation in float64 (the float32 positions taken
+    exactly): the formula of LJ_12_6_sigma_epsilon.py:26-36 with
+    apply_shifted_force_cutoff.py:30-37 (s -= s(cut)) and the minimum image
+    of orthorhombic.py:50-53.  The yardstick for the float32 paths' error."""
+    r = np.asarray(r, np.float64)
+    box = np.asarray(box, np.float64)
+    n = len(r)
+    pt = np.zeros(n, np.int64) if ptype is None else np.asarray(ptype, np.int64)
+    nbl = np.asarray(nbl)
+    cnt = np.minimum(nbl[:, -1], nbl.shape[1] - 1)
+    rows = np.repeat(np.arange(n), cnt)
+    cols = nbl[:, :-1][np.arange(nbl.shape[1] - 1)[None, :] < cnt[:, None]]
+    dr = r[cols] - r[rows]
+    dr -= box * np.where(2 * dr > box, 1.0, np.where(2 * dr < -box, -1.0, 0.0))
+    d2 = np.einsum("ij,ij->i", dr, dr)
+    sg = np.asarray(sigma, np.float64)[pt[rows], pt[cols]]
+    ep = np.asarray(epsilon, np.float64)[pt[rows], pt[cols]]
+    rc = np.asarray(cut, np.float64)[pt[rows], pt[cols]]
+
+    def s_of(x2):
+        x6 = (sg * sg / x2) ** 3
+        return 24.0 * ep * (2.0 * x6 * x6 - x6) / x2
+
+    inside = d2 < rc * rc
+    s = np.where(inside, s_of(d2) - s_of(rc * rc), 0.0)
+    f = np.zeros((n, 3))
+    np.add.at(f, rows, -dr * s[:, None])
+    return f
+
+
 def rdf(r, ptype, box, bins, fma=0, r_max=0.0):
     r, box = _f32(r), _f32(box)
     n = len(r)

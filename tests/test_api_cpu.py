@@ -79,6 +79,10 @@ def test_default_compute_plan_for_b200():
     assert plan["nblist"] == "N squared" and plan["gridsync"]
     big = gp.Configuration(D=3, N=65536)
     assert gp.get_default_compute_plan(big)["nblist"] == "linked lists"
+    # below 2 x 148 particles gamdpy's pb loop would reach zero; here pb stays 8
+    for n in (1, 100, 256, 295):
+        small = gp.Configuration(D=3, N=n)
+        assert gp.get_default_compute_plan(small)["pb"] == 8
 
 
 def test_param_table_and_untagged_potential_rejected():

@@ -131,6 +131,27 @@ def test_thread_per_particle_build_vs_oracle(oracle, n, monkeypatch):
     assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
 
 
+def test_force_error_against_float64(oracle):
+    """The float32 forces' error against every-operation-float64 forces on the
+    same list (KA, 30 000 particles, cell lists): the library's and gamdpy's
+    float32 form (the oracle) are both below 2e-6 relative RMS from float64,
+    and from each other."""
+    conf = workloads.ka_configuration(30000, seed=7, jitter=0.2)
+    L = conf.simbox.lengths
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    sim = make_sim(conf["r"], L, conf.ptype, table, nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.eval_forces()
+    nbl = sim.nblist(300)
+    f_gpu = sim.download()["f"]
+    f_ref32 = oracle.forces(conf["r"], conf.ptype, L, table, nbl, fma=1)["f"]
+    f64 = oracle.forces_fp64(conf["r"], conf.ptype, L, workloads.KA_SIGMA, workloads.KA_EPSILON,
+                             workloads.KA_CUT, nbl)
+    e_gpu, e_ref = rel_rms(f_gpu, f64), rel_rms(f_ref32, f64)
+    print("relative RMS against float64: library", e_gpu, "gamdpy float32 form", e_ref)
+    assert e_gpu < 2e-6 and e_ref < 2e-6
+    assert rel_rms(f_gpu, f_ref32) < FORCE_TOL
+
+
 def run_api_trajectory(d):
     """Golden trajectory through the public API (Simulation + runtime actions)."""
     n = len(d["r0"])

@@ -131,3 +131,21 @@ def test_sq_against_reference_backends(oracle):
         assert rel_rms(np.abs(got) ** 2, d[f"{key}_S"]) < 1e-3, key
     got = oracle.sq(d["r"], d["ff_q"], d["ff"])
     assert np.abs(got - d["ff_rho_q"]).max() < 2e-3 * max(1.0, np.abs(d["ff_rho_q"]).max())
+
+
+def test_float64_forces_pin_to_gamdpy(oracle):
+    """The every-operation-float64 force restatement against gamdpy's own
+    float32 forces on its golden list (LJ 256, shifted force): they differ by
+    float32 round-off only."""
+    d = golden("lj256_sf")
+    counts = np.asarray(d["nb_counts"])
+    n, width = len(counts), int(counts.max()) + 1
+    nbl = np.zeros((n, width), np.int32)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    for i in range(n):
+        nbl[i, :counts[i]] = d["nb_flat"][starts[i]:starts[i] + counts[i]]
+        nbl[i, -1] = counts[i]
+    one = np.ones((1, 1))
+    f64 = oracle.forces_fp64(d["r"], d["ptype"], d["box"], one * float(d["sigma"]), one * float(d["epsilon"]),
+                             one * float(d["cut"]), nbl)
+    assert rel_rms(d["f"], f64) < 2e-6
