@@ -52,6 +52,8 @@ def parse():
                    help="ka: one KA system of --n particles; batch: --replicas KA replicas of uneven N, "
                         "density and temperature advanced together, against the same replicas run one by one")
     p.add_argument("--replicas", type=int, default=128)
+    p.add_argument("--sweep", action="store_true",
+                   help="ka: MATS/TPS vs N over 512 ... 1 048 576, one JSON line per N with the oracle beside it")
     p.add_argument("--lj-cells", type=int, default=128,
                    help="lj8m: FCC unit cells per side (128: 8 388 608 particles; smaller for profiling)")
     p.add_argument("--autotune", action="store_true", help="batch: pick particles per CTA by timing")
@@ -209,13 +211,67 @@ def cpu_reference(args, n, steps, seed=0):
     from oracle import oracle as O
     conf = workloads.ka_configuration(n, seed=seed)
     tab = O.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
-    run = O.Run(conf["r"], conf["v"], conf["m"], conf.ptype, conf.simbox.lengths, tab, nblist="linked lists",
+    # the reference's default list kind by size (get_default_compute_plan.py:83-86)
+    nblist = "linked lists" if n > 6000 else "N squared"
+    run = O.Run(conf["r"], conf["v"], conf["m"], conf.ptype, conf.simbox.lengths, tab, nblist=nblist,
                 skin=0.3, max_nbs=300, integrator="NVT", dt=0.005, temperature=0.45, tau=0.2)
     run.run_timeblock(1)  # first list build outside the timing, as the GPU warm-up
     t0 = time.perf_counter()
     run.run_timeblock(steps)
     dt = time.perf_counter() - t0
     return n * steps / dt / 1e6, O.num_threads(), dt
+
+
+SWEEP_N = (512, 2048, 8192, 65536, 262144, 1048576)
+
+
+def run_sweep(args):
+    """MATS and TPS vs N for the KA workload (rho 1.2, NVT T 0.45, cells skin
+    0.3), N = 512 ... 1 048 576 as the reference's benchmark sweep
+    (benchmarks/benchmark_LJ.py:100-146): per N about 2e8 atom-steps on the
+    device (at most 10^5 steps, timeblocks of 500 or fewer), the path the
+    library chose, the HBM roofline fraction of the timed launches, and the
+    oracle on the host cores over a bounded sample of the same system."""
+    import gamdpy_b200 as gp
+    from gamdpy_b200 import workloads
+    rank, world, local, pg = dist_setup(args)
+    peak, peak_kind = measured_peak_hbm()
+    for n in SWEEP_N:
+        conf = workloads.ka_configuration(n, seed=1234 + rank)
+        pp = workloads.ka_pair_potential(max_num_nbs=300)
+        integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
+        block = 500
+        nblocks = max(2, min(200, int(2e8 / n / block)))
+        plan = {"pb": 64, "tp": 1, "lanes": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
+                "nblist": "linked lists"}
+        sim = gp.Simulation(conf, pp, integ, [gp.ScalarSaver(block // 8)], num_timeblocks=8,
+                            steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
+        dev = sim._sim
+        dev.run(0.0, max(3, args.warmup))
+        dev.clear_status()
+        barrier(pg)
+        ms = sum(dev.run(float(b * block * 0.005), block) for b in range(nblocks))
+        t_max = allreduce_max(pg, ms / 1e3, local)
+        steps = nblocks * block
+        mean_nbs, _ = dev.nblist_stats()
+        bpa = 4.0 * mean_nbs + 64.0
+        achieved = bpa * n * steps / t_max / 1e9
+        line = {"sweep": True, "n": n, "mats": n * steps * world / t_max / 1e6, "tps": steps / t_max,
+                "steps": steps, "ms_per_step": t_max * 1e3 / steps, "path": ["graph", "persistent", "cluster"][
+                    dev.last_path()] if 0 <= dev.last_path() <= 2 else dev.last_path(),
+                "hbm_frac": achieved / peak, "hbm_peak": peak, "peak_source": peak_kind,
+                "algorithmic_bytes_per_atom_step": bpa, "n_gpus": world}
+        if rank == 0 and world == 1:
+            cps = max(2, min(400, int(3e6 / n)))
+            cmats, threads, secs = cpu_reference(args, n, cps)
+            line["cpu_baseline"] = {"value": cmats, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "sample": f"{cps} steps ({secs:.1f} s)"}
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        del sim, dev
+    barrier(pg)
+    if pg is not None:
+        pg.destroy_process_group()
 
 
 def run_reference_arm(args):
@@ -575,6 +631,9 @@ def main():
         return
     if args.workload == "lj8m":
         run_lj_large(args)
+        return
+    if args.sweep:
+        run_sweep(args)
         return
     rank, world, local, pg = dist_setup(args)
     import gamdpy_b200 as gp
