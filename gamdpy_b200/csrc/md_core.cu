@@ -100,6 +100,7 @@ struct gdb_sim {
     int num_sms = 148;
     bool persistent = true;
     bool cluster_ok = true;  // small systems run resident in one thread-block cluster
+    bool cluster_force = false;  // GDB_CLUSTER=1: the cluster path whenever it fits
     int last_path = -1;      // 0 graph, 1 persistent grid, 2 cluster
     int grid_cap = 0;        // upper bound on the persistent grid (0: the whole GPU)
     ClusterJob *d_job = nullptr, *h_job = nullptr;
@@ -547,6 +548,21 @@ static int status_to_rc(gdb_sim *h) {
     return GDB_OK;
 }
 
+// Cluster path or persistent grid for a system that fits a cluster: the
+// cluster (at most 16 SMs, no grid barrier) wins while the list holds fewer
+// than about 160 000 entries, N x (4 pi / 3) (max_cut + skin)^3 N / V;
+// above that the whole GPU's grid kernel is faster despite its barriers
+// (measured on B200, TPS cluster vs grid: KA rho 1.2 N 1024 87k vs 58k,
+// N 2048 56k vs 56k, N 3000 38k vs 48k; LJ rho 0.973 N 2048 78k vs 89k).
+constexpr double CL_LIST_ENTRIES_MAX = 160000.0;
+static bool cluster_preferred(const gdb_sim *h) {
+    if (h->cluster_force) return true;
+    const double vol = (double)h->box[0] * h->box[1] * h->box[2];
+    const double rl = (double)h->max_cut + (double)h->skin;
+    const double per_particle = 4.0 / 3.0 * M_PI * rl * rl * rl * h->n / vol;
+    return h->n * per_particle <= CL_LIST_ENTRIES_MAX;
+}
+
 // One timeblock resident in a thread-block cluster (md_cluster.cu).  Returns
 // GDB_ERR_UNSUPPORTED (and disables the path for this handle) when the
 // cluster launch is not possible on this device.
@@ -663,6 +679,7 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (ps && ps[0] == '0') h->persistent = false;
     const char *cs = getenv("GDB_CLUSTER");
     if (cs && cs[0] == '0') h->cluster_ok = false;
+    if (cs && cs[0] == '1') h->cluster_force = true;
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
@@ -1000,7 +1017,7 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
     CK(cudaEventRecord(h->ev0, h->st));
     k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
     CKL();
-    if (h->cluster_ok && h->n <= CL_MAX_N) {
+    if (h->cluster_ok && h->n <= CL_MAX_N && cluster_preferred(h)) {
         rc = run_cluster(h, steps);
         if (rc == GDB_OK) {
             CK(cudaEventRecord(h->ev1, h->st));

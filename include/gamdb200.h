@@ -185,7 +185,10 @@ int gdb_get_nbflag(gdb_sim *h, int32_t out[3]);
 
 /* Which implementation ran the last gdb_sim_run: 0 CUDA-graph launch
  * sequence, 1 persistent cooperative kernel, 2 thread-block cluster
- * (N <= 4096), -1 none yet.  Diagnostic; no counterpart in the reference. */
+ * (N <= 4096 with fewer than about 160 000 list entries, N x the neighbours
+ * expected from the density; environment GDB_CLUSTER=1: whenever N <= 4096
+ * fits, GDB_CLUSTER=0: never), -1 none yet.  Diagnostic; no counterpart in
+ * the reference. */
 int gdb_get_last_path(gdb_sim *h);
 
 /* Status bits set by kernels since the last clear; gdb_clear_status resets. */

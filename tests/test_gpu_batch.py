@@ -1,6 +1,8 @@
 """Thread-block-cluster path and batched replicas on the GPU.
 
-The cluster path (systems up to 4096 particles in one thread-block cluster)
+The cluster path (systems up to 4096 particles in one thread-block cluster;
+GDB_CLUSTER=1 takes it for every system that fits, as single systems with
+larger lists otherwise run on the grid kernel)
 must give the same neighbour sets as the global builds and forces within
 float32 round-off; a system run in a batch must give bit-for-bit the result
 of the same system run alone on the same path; batches are reproducible.
@@ -29,6 +31,14 @@ def ka_sim(n, rho=1.2, temp=0.6, seed=0, skin=0.3, max_nbs=300, block=64, saver_
 def state(sim):
     st = sim._sim.download(r=True, v=True, f=True, r_im=True)
     return st
+
+
+@pytest.fixture(autouse=True)
+def cluster_whenever_it_fits(monkeypatch):
+    # a single system takes the cluster path only while its list is small;
+    # these tests compare that path with the global one and with batches
+    monkeypatch.setenv("GDB_CLUSTER", "1")
+    yield
 
 
 @pytest.fixture
