@@ -152,6 +152,26 @@ def test_force_error_against_float64(oracle):
     assert rel_rms(f_gpu, f_ref32) < FORCE_TOL
 
 
+def test_persistent_small_system_cell_request_vs_oracle(oracle, monkeypatch):
+    """Up to 3072 particles the persistent kernel answers a cell-list request
+    with the N^2 build: the same sets as the oracle's cell build, and the same
+    forces to float32 round-off."""
+    monkeypatch.setenv("GDB_CLUSTER", "0")
+    n = 2048
+    conf = workloads.ka_configuration(n, seed=19, jitter=0.25)
+    L = conf.simbox.lengths
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    sim = make_sim(conf["r"], L, conf.ptype, table, nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.run(0.0, 0)  # persistent kernel: rebuild + evaluation
+    assert sim.last_path() == 1
+    ref, _ = oracle.nblist_cells(conf["r"], L, 2.5, 0.3, 300, fma=1)
+    c1, f1 = sorted_rows(sim.nblist(300))
+    c2, f2 = sorted_rows(ref)
+    assert np.array_equal(c1, c2) and np.array_equal(f1, f2)
+    res = oracle.forces(conf["r"], conf.ptype, L, table, ref, fma=1)
+    assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
+
+
 def run_api_trajectory(d):
     """Golden trajectory through the public API (Simulation + runtime actions)."""
     n = len(d["r0"])
