@@ -336,6 +336,107 @@ void orc_nve_step(int n, float *r, float *v, const float *f, const float *m, int
     }
 }
 
+/* Random numbers of integrators/NVT_Langevin.py:48 and :105, which are
+ * numba.cuda.random's (numba 0.65.0, numba/cuda/random.py; a dependency of the
+ * reference, not vendored in it): xoroshiro128+ with the (55, 14, 36) update
+ * (xoroshiro128p_next); state 0 from SplitMix64 of the seed
+ * (init_xoroshiro128p_state), state i = state i-1 advanced 2^64 steps by the
+ * jump polynomial (init_xoroshiro128p_states_cpu, xoroshiro128p_jump);
+ * uniform float32 = float32((x >> 11) * 2^-53) (uint64_to_unit_float32);
+ * normal = sqrt(-2 log u1) cos(2 pi u2), float32, the first Box-Muller value
+ * of two draws (xoroshiro128p_normal_float32). */
+static uint64_t xr_rotl(uint64_t x, unsigned k) { return (x << k) | (x >> (64 - k)); }
+
+uint64_t orc_xoro_next(uint64_t *s) {
+    uint64_t s0 = s[0], s1 = s[1];
+    uint64_t result = s0 + s1;
+    s1 ^= s0;
+    s[0] = xr_rotl(s0, 55) ^ s1 ^ (s1 << 14);
+    s[1] = xr_rotl(s1, 36);
+    return result;
+}
+
+static void xoro_jump(uint64_t *s) {
+    static const uint64_t J[2] = {0xbeac0467eba5facbULL, 0xd86b048b86aa9922ULL};
+    uint64_t a = 0, b = 0;
+    for (int i = 0; i < 2; i++)
+        for (int k = 0; k < 64; k++) {
+            if (J[i] & (1ULL << k)) {
+                a ^= s[0];
+                b ^= s[1];
+            }
+            orc_xoro_next(s);
+        }
+    s[0] = a;
+    s[1] = b;
+}
+
+/* states: n x 2 uint64 (s0, s1) */
+void orc_xoro_init(int n, uint64_t seed, uint64_t *states) {
+    if (n < 1) return;
+    uint64_t z = seed + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    states[0] = z;
+    states[1] = z;
+    for (int i = 1; i < n; i++) {
+        states[2 * (size_t)i] = states[2 * (size_t)i - 2];
+        states[2 * (size_t)i + 1] = states[2 * (size_t)i - 1];
+        xoro_jump(states + 2 * (size_t)i);
+    }
+}
+
+float orc_xoro_uniform_f32(uint64_t *s) {
+    return (float)((double)(orc_xoro_next(s) >> 11) * (1.0 / 9007199254740992.0));
+}
+
+float orc_xoro_normal_f32(uint64_t *s) {
+    const float u1 = orc_xoro_uniform_f32(s);
+    const float u2 = orc_xoro_uniform_f32(s);
+    const float two_pi = (float)(2.0 * M_PI);
+    return sqrtf(-2.0f * logf(u1)) * cosf(two_pi * u2);
+}
+
+/* integrators/NVT_Langevin.py:86-128: leap-frog Langevin (Gronbech-Jensen and
+ * Farago, Eq. 16), per particle i (user order) and component k: one normal
+ * from state i, beta = sqrt(2 alpha T dt) z, K from the velocity before the
+ * update, v = a v + (b/m) f dt + (b/m) (beta + beta_old) / 2, r += v dt; then
+ * periodic boundaries.  T is the thermostat temperature (float32). */
+void orc_langevin_step(int n, float *r, float *v, const float *f, const float *m, int32_t *img, const float *box,
+                       float dt, float alpha, float T, uint64_t *states, float *old_beta, float *K) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) {
+        const float my_m = m[i];
+        float k_i = 0.0f;
+        for (int k = 0; k < 3; k++) {
+            const size_t e = 3 * (size_t)i + k;
+            const float z = orc_xoro_normal_f32(states + 2 * (size_t)i);
+            const float beta = sqrtf(2.0f * alpha * T * dt) * z;
+            const float numerator = 2.0f * my_m - alpha * dt;
+            const float denominator = 2.0f * my_m + alpha * dt;
+            const float a = numerator / denominator;
+            const float b_over_m = 2.0f / denominator;
+            k_i += 0.5f * my_m * v[e] * v[e];
+            v[e] = a * v[e] + b_over_m * f[e] * dt + b_over_m * 0.5f * (beta + old_beta[e]);
+            old_beta[e] = beta;
+            r[e] += v[e] * dt;
+        }
+        orc_apply_pbc(r + 3 * (size_t)i, img + 3 * (size_t)i, box);
+        if (K) K[i] = k_i;
+    }
+}
+
+/* Langevin state for orc_run_timeblock's integrator 2 (set before the call) */
+static uint64_t *g_lv_states = NULL;
+static float *g_lv_beta = NULL;
+static float g_lv_alpha = 0.0f;
+void orc_set_langevin(uint64_t *states, float *old_beta, float alpha) {
+    g_lv_states = states;
+    g_lv_beta = old_beta;
+    g_lv_alpha = alpha;
+}
+
 /* integrators/NVT.py:188-224 (step) and :226-237 (update_thermostat_state).
  * state[0] = xi (float32), the kinetic-energy sum is returned in float64
  * (the reference accumulates it with float32 atomics into state[1]).
@@ -399,7 +500,8 @@ void orc_momentum_reset(int n, float *v, const float *m) {
  *   ScalarSaver (scalar_saver.py:270-304) and MomentumReset
  *   (momentum_reset.py:400-408) in that order.
  *
- * integrator: 0 = NVE, 1 = NVT.  nvt_state[0] = xi (in/out).
+ * integrator: 0 = NVE, 1 = NVT, 2 = NVT_Langevin (state from orc_set_langevin).
+ * nvt_state[0] = xi (in/out).
  * nblist_kind: 0 = N squared, 1 = linked lists.  r_ref / have_list carry the
  * list state across calls (have_list = 0 forces a build).
  * scal_out: (steps/every) x 4 doubles: U, W, K, lapU sums per saved step
@@ -439,6 +541,8 @@ int orc_run_timeblock(int n, float *r, float *v, float *f, const float *m, int32
         if (step < steps) {
             if (integrator == 0) {
                 orc_nve_step(n, r, v, f, m, img, box, dt, K, NULL);
+            } else if (integrator == 2) {
+                orc_langevin_step(n, r, v, f, m, img, box, dt, g_lv_alpha, T, g_lv_states, g_lv_beta, K);
             } else {
                 double ks = orc_nvt_step(n, r, v, f, m, img, box, dt, nvt_state[0], K, NULL);
                 nvt_state[0] = orc_nvt_thermostat_update(nvt_state[0], ks, dt, omega2, degrees, T);

@@ -65,6 +65,16 @@ def lib():
         L.orc_run_timeblock.restype = i
         L.orc_rdf.argtypes = [i, P, P, P, i, i, P, i, d]
         L.orc_sq.argtypes = [i, P, P, i, P, P, P]
+        u64 = ctypes.c_uint64
+        L.orc_xoro_init.argtypes = [i, u64, P]
+        L.orc_xoro_next.argtypes = [P]
+        L.orc_xoro_next.restype = u64
+        L.orc_xoro_uniform_f32.argtypes = [P]
+        L.orc_xoro_uniform_f32.restype = f
+        L.orc_xoro_normal_f32.argtypes = [P]
+        L.orc_xoro_normal_f32.restype = f
+        L.orc_langevin_step.argtypes = [i, P, P, P, P, P, P, f, f, f, P, P, P]
+        L.orc_set_langevin.argtypes = [P, P, f]
         _lib = L
     return _lib
 
@@ -210,13 +220,36 @@ def sq(r, q, ff=None):
     return re + 1j * im
 
 
+def xoro_states(n, seed):
+    """numba.cuda.random.create_xoroshiro128p_states(n, seed) restated:
+    (n, 2) uint64 (s0, s1)."""
+    st = np.zeros((n, 2), np.uint64)
+    lib().orc_xoro_init(int(n), int(seed) & 0xFFFFFFFFFFFFFFFF, _p(st))
+    return st
+
+
+def xoro_next(states, index):
+    """xoroshiro128p_next on states[index] (advances it)."""
+    row = states[index]
+    out = lib().orc_xoro_next(row.ctypes.data_as(ctypes.c_void_p))
+    return np.uint64(out)
+
+
+def xoro_normal_f32(states, index):
+    """xoroshiro128p_normal_float32 on states[index] (advances it twice)."""
+    row = states[index]
+    return np.float32(lib().orc_xoro_normal_f32(row.ctypes.data_as(ctypes.c_void_p)))
+
+
 class Run:
     """State of one oracle simulation, advanced one timeblock at a time with
-    the reference's composed loop (gamdpy/simulation/Simulation.py:330-346)."""
+    the reference's composed loop (gamdpy/simulation/Simulation.py:330-346).
+    integrator "NVT_Langevin" takes temperature, alpha and seed
+    (integrators/NVT_Langevin.py:44-53)."""
 
     def __init__(self, r, v, m, ptype, box, table, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF,
                  nblist="N squared", skin=0.5, max_nbs=300, integrator="NVE", dt=0.005,
-                 temperature=None, tau=None, every=0, reset_every=0, fma=0):
+                 temperature=None, tau=None, every=0, reset_every=0, fma=0, alpha=None, seed=0):
         n = len(r)
         self.n = n
         self.r = _f32(r).copy()
@@ -228,7 +261,11 @@ class Run:
         self.kind, self.cutmode = kind, cutmode
         self.nblist_kind = 0 if nblist == "N squared" else 1
         self.skin, self.max_nbs = float(skin), int(max_nbs)
-        self.integrator = 0 if integrator == "NVE" else 1
+        self.integrator = {"NVE": 0, "NVT": 1, "NVT_Langevin": 2}[integrator]
+        if self.integrator == 2:
+            self.alpha = np.float32(alpha)
+            self.rng = xoro_states(n, seed)
+            self.old_beta = np.zeros((n, 3), np.float32)
         self.dt = np.float32(dt)
         self.T = np.float32(temperature or 0.0)
         self.omega2 = np.float32(4.0 * np.pi * np.pi / tau / tau) if tau else np.float32(0)
@@ -246,6 +283,8 @@ class Run:
         nsave = steps // self.every if self.every else 0
         scal = np.zeros((max(nsave, 1), 4), np.float64)
         nt, _, npar = self.table.shape
+        if self.integrator == 2:
+            lib().orc_set_langevin(_p(self.rng), _p(self.old_beta), float(self.alpha))
         rc = lib().orc_run_timeblock(
             self.n, _p(self.r), _p(self.v), _p(self.f), _p(self.m), _p(self.img), _p(self.ptype),
             _p(self.box), _p(self.table), npar, nt, self.kind, self.cutmode, self.nblist_kind,

@@ -149,3 +149,20 @@ def test_float64_forces_pin_to_gamdpy(oracle):
     f64 = oracle.forces_fp64(d["r"], d["ptype"], d["box"], one * float(d["sigma"]), one * float(d["epsilon"]),
                              one * float(d["cut"]), nbl)
     assert rel_rms(d["f"], f64) < 2e-6
+
+
+def test_langevin_random_numbers_pin_to_numba(oracle):
+    """The oracle's restatement of numba.cuda.random (the generator of
+    integrators/NVT_Langevin.py:48, :105) against numba's own CPU output:
+    states, raw 64-bit outputs and float32 normals, all bit-exact."""
+    d = golden("langevin_rng")
+    n = len(d["states_s0"])
+    st = oracle.xoro_states(n, int(d["seed"]))
+    assert np.array_equal(st[:, 0], d["states_s0"]) and np.array_equal(st[:, 1], d["states_s1"])
+    raw = st.copy()
+    for row, i in enumerate(d["next_index"]):
+        got = [oracle.xoro_next(raw, int(i)) for _ in range(d["next_u64"].shape[1])]
+        assert np.array_equal(np.array(got, np.uint64), d["next_u64"][row])
+    normals = np.array([[oracle.xoro_normal_f32(st, i) for _ in range(d["normals"].shape[1])] for i in range(n)],
+                       np.float32)
+    assert np.array_equal(normals.view(np.int32), d["normals"].view(np.int32))
