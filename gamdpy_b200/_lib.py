@@ -77,6 +77,8 @@ SIGNATURES = {
     "gdb_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
     "gdb_rdf_update": ([_P, _i, _d, _P], _i),
     "gdb_sq_update": ([_P, _i, _P, _P, _P, _P], _i),
+    "gdb_set_integrator_langevin": ([_P, _f, _f, ctypes.c_uint64, _i, _P], _i),
+    "gdb_get_langevin_state": ([_P, _P, _P], _i),
     "gdb_last_analysis_ms": ([_P, _P], _i),
     "gdb_rdf_compute": ([_i, _P, _P, _P, _i, _i, _d, _P], _i),
     "gdb_sq_compute": ([_i, _P, _P, _P, _i, _P, _P, _P], _i),
@@ -238,6 +240,18 @@ class Sim:
     def set_nvt(self, dt, tau, tfunc, tparams):
         tp = f32(np.resize(np.asarray(tparams, np.float32), 4))
         self.call("gdb_set_integrator_nvt", float(dt), float(tau), int(tfunc), ptr(tp))
+
+    def set_langevin(self, dt, alpha, seed, tfunc, tparams):
+        tp = f32(np.resize(np.asarray(tparams, np.float32), 4))
+        self.call("gdb_set_integrator_langevin", float(dt), float(alpha), int(seed) & 0xFFFFFFFFFFFFFFFF, int(tfunc),
+                  ptr(tp))
+
+    def langevin_state(self):
+        """(states (n, 2) uint64, old_beta (n, 3) float32) in user order."""
+        st = np.zeros((self.n, 2), np.uint64)
+        ob = np.zeros((self.n, 3), np.float32)
+        self.call("gdb_get_langevin_state", ptr(st), ptr(ob))
+        return st, ob
 
     def thermostat_state(self):
         s = np.zeros(2, np.float32)

@@ -118,6 +118,10 @@ struct gdb_sim {
     int graph_steps = 0;
     bool use_graphs = true;
     float analysis_ms = 0.f;  // device time of the last RDF / S(q) call
+    // NVT_Langevin: per-particle generators and previous random forces (user index)
+    ulonglong2 *rng = nullptr;
+    float4 *lbeta = nullptr;
+    float alpha = 0.f;
     char err[512] = "";
 };
 
@@ -436,6 +440,9 @@ static SimArgs make_args(gdb_sim *h) {
     a.reset_every = h->momentum_every;
     a.nrows = h->rows ? h->rows_cap : 0;
     a.conf_per_block = h->conf_per_block;
+    a.rng = h->rng;
+    a.lbeta = h->lbeta;
+    a.alpha = h->alpha;
     return a;
 }
 
@@ -751,7 +758,7 @@ int gdb_sim_destroy(gdb_sim *h) {
     void *bufs[] = {h->pos[0], h->pos[1], h->vel,        h->frc,       h->rref,  h->pos_tmp, h->vel_tmp,
                     h->img,    h->img_tmp, h->orig,      h->orig_tmp,  h->nbl,   h->nbc,     h->pscal,
                     h->pscal_tmp, h->cell_count, h->cell_start, h->pcell, h->prank, h->perm, h->scell,
-                    h->bsum,   h->ctrl,   h->partials,   h->rows,  h->conf, h->trace};
+                    h->bsum,   h->ctrl,   h->partials,   h->rows,  h->conf, h->trace, h->rng, h->lbeta};
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
@@ -914,6 +921,82 @@ int gdb_set_integrator_nve(gdb_sim *h, float dt) {
     return GDB_OK;
 }
 
+// numba.cuda.random.create_xoroshiro128p_states(n, seed) (numba/cuda/random.py:
+// init_xoroshiro128p_state, xoroshiro128p_jump, init_xoroshiro128p_states_cpu):
+// SplitMix64 of the seed for state 0, state i = state i-1 advanced 2^64 steps.
+static void xoro_host_next(unsigned long long &s0, unsigned long long &s1) {
+    const unsigned long long a = s0;
+    unsigned long long b = s1;
+    b ^= a;
+    s0 = ((a << 55) | (a >> 9)) ^ b ^ (b << 14);
+    s1 = (b << 36) | (b >> 28);
+}
+static void xoro_states(int n, uint64_t seed, std::vector<ulonglong2> &out) {
+    out.resize(n);
+    if (n < 1) return;
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ULL;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    z = z ^ (z >> 31);
+    out[0] = make_ulonglong2(z, z);
+    static const unsigned long long J[2] = {0xbeac0467eba5facbULL, 0xd86b048b86aa9922ULL};
+    for (int i = 1; i < n; i++) {
+        unsigned long long s0 = out[i - 1].x, s1 = out[i - 1].y, j0 = 0, j1 = 0;
+        for (int w = 0; w < 2; w++)
+            for (int b = 0; b < 64; b++) {
+                if (J[w] & (1ULL << b)) {
+                    j0 ^= s0;
+                    j1 ^= s1;
+                }
+                xoro_host_next(s0, s1);
+            }
+        out[i] = make_ulonglong2(j0, j1);
+    }
+}
+
+int gdb_set_integrator_langevin(gdb_sim *h, float dt, float alpha, uint64_t seed, int tfunc, const float *tparams) {
+    if (!h || !(dt > 0.f) || !(alpha >= 0.f) || !tparams)
+        return set_err(h, GDB_ERR_ARG, "gdb_set_integrator_langevin: bad arguments");
+    if (tfunc != GDB_TFUNC_CONSTANT && tfunc != GDB_TFUNC_RAMP)
+        return set_err(h, GDB_ERR_UNSUPPORTED, "unsupported temperature function %d", tfunc);
+    CK(cudaSetDevice(h->dev));
+    if (!h->rng) CK(cudaMalloc(&h->rng, (size_t)h->n * sizeof(ulonglong2)));
+    if (!h->lbeta) CK(cudaMalloc(&h->lbeta, (size_t)h->n * sizeof(float4)));
+    std::vector<ulonglong2> st;
+    xoro_states(h->n, seed, st);
+    CK(cudaMemcpyAsync(h->rng, st.data(), (size_t)h->n * sizeof(ulonglong2), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemsetAsync(h->lbeta, 0, (size_t)h->n * sizeof(float4), h->st));
+    CK(cudaStreamSynchronize(h->st));
+    h->integ = GDB_INTEGRATOR_LANGEVIN;
+    h->dt = dt;
+    h->alpha = alpha;
+    h->tfunc = tfunc;
+    const int np_ = tfunc == GDB_TFUNC_RAMP ? 4 : 1;
+    for (int k = 0; k < 4; k++) h->tparams[k] = k < np_ ? tparams[k] : 0.f;
+    free_graphs(h);
+    return GDB_OK;
+}
+
+int gdb_get_langevin_state(gdb_sim *h, uint64_t *states, float *old_beta) {
+    if (!h) return set_err(h, GDB_ERR_ARG, "NULL handle");
+    if (!h->rng || !h->lbeta) return set_err(h, GDB_ERR_STATE, "no Langevin integrator set");
+    CK(cudaSetDevice(h->dev));
+    const size_t n = h->n;
+    if (states) CK(cudaMemcpyAsync(states, h->rng, n * sizeof(ulonglong2), cudaMemcpyDeviceToHost, h->st));
+    std::vector<float4> b;
+    if (old_beta) {
+        b.resize(n);
+        CK(cudaMemcpyAsync(b.data(), h->lbeta, n * sizeof(float4), cudaMemcpyDeviceToHost, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    for (size_t i = 0; old_beta && i < n; i++) {
+        old_beta[3 * i] = b[i].x;
+        old_beta[3 * i + 1] = b[i].y;
+        old_beta[3 * i + 2] = b[i].z;
+    }
+    return GDB_OK;
+}
+
 int gdb_set_integrator_nvt(gdb_sim *h, float dt, float tau, int tfunc, const float *tparams) {
     if (!h || !(dt > 0.f) || !(tau > 0.f) || !tparams)
         return set_err(h, GDB_ERR_ARG, "gdb_set_integrator_nvt: bad arguments");
@@ -1033,7 +1116,7 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
     CK(cudaEventRecord(h->ev0, h->st));
     k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
     CKL();
-    if (h->cluster_ok && h->n <= CL_MAX_N && cluster_preferred(h)) {
+    if (h->cluster_ok && h->n <= CL_MAX_N && h->integ != GDB_INTEGRATOR_LANGEVIN && cluster_preferred(h)) {
         rc = run_cluster(h, steps);
         if (rc == GDB_OK) {
             CK(cudaEventRecord(h->ev1, h->st));
@@ -1356,6 +1439,10 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
             batch_free(b);
             return bset(nullptr, GDB_ERR_ARG,
                         "gdb_batch_create: every system needs the same device, type count and integrator");
+        }
+        if (h->integ == GDB_INTEGRATOR_LANGEVIN) {
+            batch_free(b);
+            return bset(nullptr, GDB_ERR_UNSUPPORTED, "gdb_batch_create: Langevin systems run one at a time");
         }
         for (int q = 0; q < k; q++)
             if (sims[q] == h) {

@@ -209,6 +209,8 @@ GDB_DECLARE_NT(ntg)
             k_step<TP, NT, 0, MODE_EVAL><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);                           \
         else if (integ == GDB_INTEGRATOR_NVT)                                                                \
             k_step<TP, NT, GDB_INTEGRATOR_NVT, MODE_STEP><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);          \
+        else if (integ == GDB_INTEGRATOR_LANGEVIN)                                                           \
+            k_step<TP, NT, GDB_INTEGRATOR_LANGEVIN, MODE_STEP><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);     \
         else                                                                                                 \
             k_step<TP, NT, GDB_INTEGRATOR_NVE, MODE_STEP><<<grid, GDB_BLOCK, 0, st>>>(a, tab, cur);          \
     }                                                                                                        \
@@ -225,8 +227,9 @@ GDB_DECLARE_NT(ntg)
     }                                                                                                        \
     template <int TP>                                                                                        \
     static const void *run_tp_##NTNAME(int integ) {                                                          \
-        return integ == GDB_INTEGRATOR_NVT ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVT>                 \
-                                           : (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVE>;                \
+        return integ == GDB_INTEGRATOR_NVT        ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVT>          \
+               : integ == GDB_INTEGRATOR_LANGEVIN ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_LANGEVIN>     \
+                                                  : (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVE>;         \
     }                                                                                                        \
     const void *run_kernel_##NTNAME(int tp, int integ) {                                                     \
         switch (tp) {                                                                                        \

@@ -59,6 +59,10 @@ struct SimArgs {
     int tfunc;
     float tp0, tp1, tp2, tp3;
     int every, reset_every, nrows, conf_per_block;
+    // NVT_Langevin: generator (s0, s1) and previous random force per user index
+    ulonglong2 *rng;
+    float4 *lbeta;
+    float alpha;
 };
 
 __device__ __forceinline__ float4 *cur_pos(const SimArgs &a, int cur) { return cur ? a.pos1 : a.pos0; }
@@ -681,6 +685,27 @@ __device__ __forceinline__ double target_temperature(const SimArgs &a, double t)
     return a.tp0;
 }
 
+// numba.cuda.random's generator, the one of integrators/NVT_Langevin.py:105:
+// xoroshiro128+ with the (55, 14, 36) update, uniform float32 =
+// float32((x >> 11) 2^-53), normal = first Box-Muller value of two draws.
+__device__ __forceinline__ unsigned long long xoro_next(ulonglong2 &s) {
+    const unsigned long long s0 = s.x;
+    unsigned long long s1 = s.y;
+    const unsigned long long result = s0 + s1;
+    s1 ^= s0;
+    s.x = ((s0 << 55) | (s0 >> 9)) ^ s1 ^ (s1 << 14);
+    s.y = (s1 << 36) | (s1 >> 28);
+    return result;
+}
+__device__ __forceinline__ float xoro_uniform(ulonglong2 &s) {
+    return (float)((double)(xoro_next(s) >> 11) * (1.0 / 9007199254740992.0));
+}
+__device__ __forceinline__ float xoro_normal(ulonglong2 &s) {
+    const float u1 = xoro_uniform(s);
+    const float u2 = xoro_uniform(s);
+    return sqrtf(-2.0f * logf(u1)) * cosf(6.28318530717958647692f * u2);
+}
+
 // ConfigurationSaver slot of a step (runtime_actions/configuration_saver.py:
 // 115-141): step 0 -> 0, step 2^b -> b + 1, others -> -1.
 __device__ __forceinline__ int conf_save_index(int step) {
@@ -918,6 +943,27 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
                 kin += 0.5f * m * v_mean * v_mean;
                 r[k] += vv[k] * a.dt;
             }
+        } else if (INTEG == GDB_INTEGRATOR_LANGEVIN) {  // integrators/NVT_Langevin.py:98-122
+            const size_t uidx = (size_t)a.orig[i];
+            ulonglong2 st = a.rng[uidx];
+            float4 ob = a.lbeta[uidx];
+            float obk[3] = {ob.x, ob.y, ob.z};
+            const float T = (float)target_temperature(a, ctrl->time_zero + (double)step * (double)a.dt);
+            const float numerator = 2.0f * m - a.alpha * a.dt;
+            const float denominator = 2.0f * m + a.alpha * a.dt;
+            const float fa = numerator / denominator;
+            const float b_over_m = 2.0f / denominator;
+            const float bscale = sqrtf(2.0f * a.alpha * T * a.dt);
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                const float beta = bscale * xoro_normal(st);
+                kin += 0.5f * m * vv[k] * vv[k];  // the velocity before the update
+                vv[k] = fa * vv[k] + b_over_m * ff[k] * a.dt + b_over_m * 0.5f * (beta + obk[k]);
+                obk[k] = beta;
+                r[k] += vv[k] * a.dt;
+            }
+            a.rng[uidx] = st;
+            a.lbeta[uidx] = make_float4(obk[0], obk[1], obk[2], 0.f);
         } else {  // integrators/NVT.py:196-215
             const float factor = 0.5f * xi * a.dt;
             const float plus = 1.0f / (1.0f + factor);

@@ -1,4 +1,4 @@
-"""Integrators (gamdpy/integrators/NVE.py, NVT.py).
+"""Integrators (gamdpy/integrators/NVE.py, NVT.py, NVT_Langevin.py).
 
 The step itself runs fused with the force evaluation in libgamdb200's step
 kernel; these classes carry the parameters with gamdpy's names and
@@ -78,3 +78,37 @@ class NVT(Integrator):
     def sync_from_device(self):
         if self._device is not None:
             self.thermostat_state[:] = self._device.thermostat_state()
+
+
+class NVT_Langevin(Integrator):
+    """Leap-frog Langevin thermostat (integrators/NVT_Langevin.py:12-138;
+    Gronbech-Jensen and Farago, arXiv:1303.7011, Eq. 16):
+    m a = f - alpha v + beta, with beta = sqrt(2 alpha T dt) times a normal
+    number from a per-particle xoroshiro128+ generator seeded as
+    numba.cuda.random.create_xoroshiro128p_states(N, seed).  ``temperature``
+    is a number or a function of time from make_function_constant /
+    make_function_ramp.  Runs on the persistent and graph paths; systems with
+    it are not batched."""
+
+    def __init__(self, temperature, alpha: float, dt: float, seed: int) -> None:
+        self.temperature = temperature
+        self.alpha = alpha
+        self.dt = dt
+        self.seed = seed
+
+    def get_params(self, configuration, interactions_params=None, verbose=False):
+        return (np.float32(self.dt), np.float32(self.alpha), self.seed)
+
+    def _tfunc(self):
+        T = self.temperature
+        if not callable(T):
+            T = make_function_constant(value=float(T))
+        kind = getattr(T, "_gdb_tfunc", None)
+        if kind is None:
+            raise NotImplementedError("NVT_Langevin temperature must be a number, make_function_constant or "
+                                      "make_function_ramp (the step runs in CUDA)")
+        return kind, T._gdb_tparams
+
+    def configure_device(self, sim, configuration):
+        kind, tparams = self._tfunc()
+        sim.set_langevin(np.float32(self.dt), np.float32(self.alpha), int(self.seed), kind, tparams)

@@ -14,7 +14,7 @@ import numpy as np
 
 from . import _lib
 from .configuration import Configuration, get_default_compute_flags, unit_cells
-from .integrators import NVE, NVT
+from .integrators import NVE, NVT, NVT_Langevin
 from .interactions import PairPotential
 from .runtime_actions import ConfigurationSaver, MomentumReset, ScalarSaver
 
@@ -93,8 +93,8 @@ class Simulation:
         if len(self.interactions) != 1 or not isinstance(self.interactions[0], PairPotential):
             raise NotImplementedError("gamdpy_b200 runs exactly one PairPotential per simulation")
         self.integrator = integrator
-        if not isinstance(integrator, (NVE, NVT)):
-            raise NotImplementedError("gamdpy_b200 supports the NVE and NVT integrators")
+        if not isinstance(integrator, (NVE, NVT, NVT_Langevin)):
+            raise NotImplementedError("gamdpy_b200 supports the NVE, NVT and NVT_Langevin integrators")
         self.dt = integrator.dt
         if num_timeblocks == 0:
             if num_steps == 0:

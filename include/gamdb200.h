@@ -58,6 +58,7 @@ extern "C" {
 /* integrators */
 #define GDB_INTEGRATOR_NVE 0 /* integrators/NVE.py */
 #define GDB_INTEGRATOR_NVT 1 /* integrators/NVT.py */
+#define GDB_INTEGRATOR_LANGEVIN 2 /* integrators/NVT_Langevin.py */
 /* NVT target temperature T(t): misc/make_function.py */
 #define GDB_TFUNC_CONSTANT 0 /* make_function_constant :6-13, tparams = {T} */
 #define GDB_TFUNC_RAMP 1     /* make_function_ramp :16-34, tparams = {T0, t0, T1, t1} */
@@ -122,6 +123,20 @@ int gdb_set_plan(gdb_sim *h, int tp, int pb);
  * NVT.get_params (integrators/NVT.py:33-37). */
 int gdb_set_integrator_nve(gdb_sim *h, float dt);
 int gdb_set_integrator_nvt(gdb_sim *h, float dt, float tau, int tfunc, const float *tparams);
+
+/* NVT_Langevin (integrators/NVT_Langevin.py:44-53 get_params, :86-128 step):
+ * leap-frog Langevin with friction alpha and temperature tfunc/tparams (as
+ * gdb_set_integrator_nvt).  One xoroshiro128+ generator per particle (user
+ * index), seeded as numba.cuda.random.create_xoroshiro128p_states(N, seed);
+ * the stored random forces start at zero.  Runs on the persistent and graph
+ * paths (not on thread-block clusters, not in batches). */
+int gdb_set_integrator_langevin(gdb_sim *h, float dt, float alpha, uint64_t seed, int tfunc, const float *tparams);
+
+/* The Langevin state in user order (no counterpart in the reference, whose
+ * rng_states and old_beta device arrays live inside the integrator's
+ * parameters, NVT_Langevin.py:48-50): states n x 2 uint64 (s0, s1) and the
+ * previous random forces n x 3 float32; either pointer may be NULL. */
+int gdb_get_langevin_state(gdb_sim *h, uint64_t *states, float *old_beta);
 /* NVT.thermostat_state = {xi, sumK} (integrators/NVT.py:30). */
 int gdb_get_thermostat_state(gdb_sim *h, float state[2]);
 int gdb_set_thermostat_state(gdb_sim *h, const float state[2]);
