@@ -52,6 +52,8 @@ def parse():
                    help="ka: one KA system of --n particles; batch: --replicas KA replicas of uneven N, "
                         "density and temperature advanced together, against the same replicas run one by one")
     p.add_argument("--replicas", type=int, default=128)
+    p.add_argument("--langevin", action="store_true",
+                   help="ka: NVT_Langevin (T 0.45, alpha 0.2, seed 1) in place of the Nose-Hoover thermostat")
     p.add_argument("--sweep", action="store_true",
                    help="ka: MATS/TPS vs N over 512 ... 1 048 576, one JSON line per N with the oracle beside it")
     p.add_argument("--lj-cells", type=int, default=128,
@@ -642,7 +644,10 @@ def main():
     n = args.n
     conf = workloads.ka_configuration(n, seed=1234 + rank)
     pp = workloads.ka_pair_potential(max_num_nbs=300)
-    integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
+    if args.langevin:
+        integ = gp.integrators.NVT_Langevin(temperature=0.45, alpha=0.2, dt=0.005, seed=1 + rank)
+    else:
+        integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
     block = min(args.block, max(1, args.steps))
     plan = {"pb": 64, "tp": 1, "lanes": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
             "nblist": "linked lists"}
@@ -721,7 +726,8 @@ def main():
         "metric": METRIC, "value": mats, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattice)",
-        "config": {"workload": f"KA-LJ NVT rho=1.2 T=0.45 dt=0.005 cells skin=0.3 N={n}", "n": n,
+        "config": {"workload": f"KA-LJ {'NVT_Langevin alpha=0.2' if args.langevin else 'NVT'} rho=1.2 T=0.45 "
+                               f"dt=0.005 cells skin=0.3 N={n}", "n": n,
                    "tps": tps, "timeblock_steps": block, "parallelism": f"replicas x{world}",
                    "l2": "per-step working set (neighbour list) > 126 MB L2, no flush",
                    "mean_neighbours": mean_nbs, "max_neighbours": max_nbs},
