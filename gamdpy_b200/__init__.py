@@ -1,9 +1,9 @@
 """gamdpy_b200: gamdpy's molecular-dynamics hot path on NVIDIA B200.
 
 Drop-in for the part of gamdpy's API that runs the simulation hot path --
-pair-potential forces/virial/energy over N^2 or cell neighbour lists, the NVE
-and NVT (Nose-Hoover) steps, ScalarSaver / MomentumReset / ConfigurationSaver,
-and the RDF and S(q) calculators.  The compute path is the hand-written
+pair-potential forces/virial/energy over N^2 or cell neighbour lists, the NVE,
+NVT (Nose-Hoover) and NVT_Langevin steps, ScalarSaver / MomentumReset /
+ConfigurationSaver, and the RDF and S(q) calculators.  The compute path is the hand-written
 sm_100a CUDA library libgamdb200.so (include/gamdb200.h), called through
 ctypes.  There is no CPU fallback: operations raise if the library is missing.
 

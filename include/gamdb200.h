@@ -1,9 +1,9 @@
 /*
  * gamdb200.h -- C ABI of libgamdb200.so, the B200 (sm_100a) implementation of
  * gamdpy's simulation hot path: pair-potential forces/virial/energy over a
- * neighbour list (N-squared or cell-list build), the NVE leapfrog and NVT
- * Nose-Hoover steps, the ScalarSaver/MomentumReset runtime actions, and the
- * radial-distribution and structure-factor calculators.
+ * neighbour list (N-squared or cell-list build), the NVE leapfrog, NVT
+ * Nose-Hoover and NVT Langevin steps, the ScalarSaver/MomentumReset runtime
+ * actions, and the radial-distribution and structure-factor calculators.
  *
  * Plain C: opaque handles, host pointers and sizes, int status codes
  * (GDB_OK == 0).  No torch or CUDA types appear in the signatures.  A handle
