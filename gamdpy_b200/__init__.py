@@ -21,7 +21,7 @@ from .runtime_actions import ConfigurationSaver, MomentumReset, RuntimeAction, S
 from .simulation import Simulation, get_default_compute_plan, get_default_sim
 from .batch import SimulationBatch
 from .simulation_boxes import Orthorhombic
-from .tools import Evaluator
+from .tools import Evaluator, calc_dynamics
 
 integrators = _integrators_mod
 

@@ -79,6 +79,7 @@ SIGNATURES = {
     "gdb_sq_update": ([_P, _i, _P, _P, _P, _P], _i),
     "gdb_set_integrator_langevin": ([_P, _f, _f, ctypes.c_uint64, _i, _P], _i),
     "gdb_get_langevin_state": ([_P, _P, _P], _i),
+    "gdb_calc_dynamics": ([_i, _i, _i, _P, _P, _i, _P, _i, _P, _i, _P, _P, _P, _P], _i),
     "gdb_last_analysis_ms": ([_P, _P], _i),
     "gdb_rdf_compute": ([_i, _P, _P, _P, _i, _i, _d, _P], _i),
     "gdb_sq_compute": ([_i, _P, _P, _P, _i, _P, _P, _P], _i),
@@ -360,6 +361,24 @@ def rdf_compute(r, ptype, box, ntypes, bins, r_max=0.0):
     check(lib().gdb_rdf_compute(int(n), ptr(r), ptr(pt), ptr(L), int(ntypes), int(bins), float(r_max), ptr(out)),
           None, "gdb_rdf_compute")
     return out
+
+
+def calc_dynamics(frames, ptype, box, first_block, qvalues, total_times):
+    """gdb_calc_dynamics: (msd, m4d, fs, count) for ConfigurationSaver frames."""
+    frames = f32(frames)
+    nb, cpb, two, n, d = frames.shape
+    if two != 2 or d != 3:
+        raise ValueError("frames must be (num_blocks, conf_per_block, 2, N, 3)")
+    pt = i32(ptype, (n,))
+    nt = int(len(qvalues))
+    q = np.ascontiguousarray(np.asarray(qvalues, np.float64))
+    L = f32(box, (3,))
+    msd, m4d, fs = (np.zeros((total_times, nt)) for _ in range(3))
+    count = np.zeros((total_times, 1), np.int32)
+    check(lib().gdb_calc_dynamics(int(nb), int(cpb), int(n), ptr(frames), ptr(pt), nt, ptr(L), int(first_block),
+                                  ptr(q), int(total_times), ptr(msd), ptr(m4d), ptr(fs), ptr(count)), None,
+          "gdb_calc_dynamics")
+    return msd, m4d, fs, count
 
 
 def sq_compute(r, box, n_vectors, ff=None):

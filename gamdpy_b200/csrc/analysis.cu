@@ -556,6 +556,60 @@ static void launch_sq(dim3 grid, size_t smem, cudaStream_t st, const SqArgs &a) 
         k_sq<QPT, false><<<grid, SQ_THREADS, smem, st>>>(a);
 }
 
+// ---------------------------------------------------------------------------
+// trajectory dynamics (tools/calc_dynamics.py:6-75)
+// ---------------------------------------------------------------------------
+constexpr int DYN_THREADS = 256;
+constexpr int DYN_MAX_TYPES = 8;
+
+// Frame pair p (frames f0 -> f1, each 2 x n x 3 float32: positions, then
+// image counts): dR = (r1 - r0) + (i1 - i0) L in float32 as the reference,
+// dR^2 summed over x, y, z in float32; per type the float64 sums of dR^2,
+// (dR^2)^2 and cos(q_t dR_k) over particles and components, into
+// acc[(p * nt + t) * 3 + {0, 1, 2}].
+__global__ void __launch_bounds__(DYN_THREADS) k_dynamics(const float *frames, int n, const int *ptype, int nt,
+                                                          float Lx, float Ly, float Lz, const int2 *pairs,
+                                                          const double *q, double *acc) {
+    __shared__ double red[DYN_MAX_TYPES * 3];
+    for (int k = threadIdx.x; k < nt * 3; k += blockDim.x) red[k] = 0.0;
+    __syncthreads();
+    const int2 pr = pairs[blockIdx.y];
+    const float *A = frames + (size_t)pr.x * 2 * n * 3;
+    const float *B = frames + (size_t)pr.y * 2 * n * 3;
+    const float L[3] = {Lx, Ly, Lz};
+    double s[DYN_MAX_TYPES][3];
+#pragma unroll
+    for (int t = 0; t < DYN_MAX_TYPES; t++) s[t][0] = s[t][1] = s[t][2] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int t = ptype[i];
+        float d[3];
+#pragma unroll
+        for (int k = 0; k < 3; k++) {
+            const float dr = __fsub_rn(B[3 * i + k], A[3 * i + k]);
+            const float di = __fsub_rn(B[3 * n + 3 * i + k], A[3 * n + 3 * i + k]);
+            d[k] = __fadd_rn(dr, __fmul_rn(di, L[k]));
+        }
+        const float sq = __fadd_rn(__fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1])), __fmul_rn(d[2], d[2]));
+        const double qt = q[t];
+        const double c = cos((double)d[0] * qt) + cos((double)d[1] * qt) + cos((double)d[2] * qt);
+#pragma unroll
+        for (int u = 0; u < DYN_MAX_TYPES; u++)
+            if (u == t) {
+                s[u][0] += sq;
+                s[u][1] += (double)__fmul_rn(sq, sq);
+                s[u][2] += c;
+            }
+    }
+    for (int t = 0; t < nt; t++)
+        for (int k = 0; k < 3; k++) {
+            const double v = warp_sum(s[t][k]);
+            if ((threadIdx.x & 31) == 0) atomicAdd(&red[t * 3 + k], v);
+        }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nt * 3; k += blockDim.x)
+        atomicAdd(&acc[(size_t)blockIdx.y * nt * 3 + k], red[k]);
+}
+
 __global__ void k_pack_pos(int n, const float *r, const int *pt, float4 *pos, int *orig) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -981,6 +1035,111 @@ int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], i
     if (dr) cudaFreeAsync(dr, st);
     if (pos) cudaFreeAsync(pos, st);
     if (orig) cudaFreeAsync(orig, st);
+    cudaStreamSynchronize(st);
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+int gdb_calc_dynamics(int num_blocks, int conf_per_block, int n, const float *frames, const int32_t *ptype,
+                      int ntypes, const float box[3], int first_block, const double *qvalues, int total_times,
+                      double *msd, double *m4d, double *fs, int32_t *count) {
+    gdb_sim *h = nullptr;
+    if (num_blocks < 1 || conf_per_block < 1 || n < 1 || !frames || !ptype || !box || !qvalues || !msd || !m4d ||
+        !fs || !count || ntypes < 1)
+        return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: bad arguments");
+    if (ntypes > DYN_MAX_TYPES) return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: more than 8 particle types");
+    if (first_block < 0 || first_block >= num_blocks)
+        return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: first_block outside [0, num_blocks)");
+    int extra = 0;  // int(log2(num_blocks - first_block)) - 1
+    while ((2 << extra) <= num_blocks - first_block) extra++;
+    extra -= 1;
+    if (extra < 0)  // the reference indexes past its arrays there
+        return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: needs at least two blocks from first_block on");
+    if (total_times != conf_per_block - 1 + extra)
+        return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: total_times must be conf_per_block - 1 + log2 term");
+    std::vector<int> nper(ntypes, 0);
+    for (int i = 0; i < n; i++) {
+        if (ptype[i] < 0 || ptype[i] >= ntypes) return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: type out of range");
+        nper[ptype[i]]++;
+    }
+    // frame pairs in the reference's loop order (calc_dynamics.py:52-68)
+    std::vector<int2> pairs;
+    std::vector<int> tindex;
+    for (int k = 0; k < total_times; k++) count[k] = 0;
+    for (int b = first_block; b < num_blocks; b++)
+        for (int i = 0; i < conf_per_block - 1; i++) {
+            count[i]++;
+            pairs.push_back(make_int2(b * conf_per_block + i + 1, b * conf_per_block));
+            tindex.push_back(i);
+        }
+    for (int b = first_block; b < num_blocks; b++)
+        for (int i = 0; i < extra; i++) {
+            const int other = b + (2 << i);
+            if (other < num_blocks) {
+                count[conf_per_block - 1 + i]++;
+                pairs.push_back(make_int2(other * conf_per_block, b * conf_per_block));
+                tindex.push_back(conf_per_block - 1 + i);
+            }
+        }
+    const int np_ = (int)pairs.size();
+    for (int k = 0; k < total_times * ntypes; k++) msd[k] = m4d[k] = fs[k] = 0.0;
+    if (np_ == 0) return GDB_OK;
+    cudaStream_t st;
+    ACK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    const size_t fbytes = (size_t)num_blocks * conf_per_block * 2 * n * 3 * sizeof(float);
+    float *dframes = nullptr;
+    int *dpt = nullptr;
+    int2 *dpairs = nullptr;
+    double *dq = nullptr, *dacc = nullptr;
+    std::vector<double> acc((size_t)np_ * ntypes * 3);
+    int rc = GDB_OK;
+    do {
+        cudaError_t e;
+        if ((e = pool_alloc(&dframes, fbytes, st)) || (e = pool_alloc(&dpt, (size_t)n * sizeof(int), st)) ||
+            (e = pool_alloc(&dpairs, (size_t)np_ * sizeof(int2), st)) ||
+            (e = pool_alloc(&dq, (size_t)ntypes * sizeof(double), st)) ||
+            (e = pool_alloc(&dacc, acc.size() * sizeof(double), st)) ||
+            (e = cudaMemcpyAsync(dframes, frames, fbytes, cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(dpt, ptype, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(dpairs, pairs.data(), (size_t)np_ * sizeof(int2), cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemcpyAsync(dq, qvalues, (size_t)ntypes * sizeof(double), cudaMemcpyHostToDevice, st)) ||
+            (e = cudaMemsetAsync(dacc, 0, acc.size() * sizeof(double), st))) {
+            rc = aset(h, GDB_ERR_CUDA, "gdb_calc_dynamics: staging", e);
+            break;
+        }
+        const int gx = std::min((n + DYN_THREADS - 1) / DYN_THREADS, 64);
+        k_dynamics<<<dim3(gx, np_), DYN_THREADS, 0, st>>>(dframes, n, dpt, ntypes, box[0], box[1], box[2], dpairs,
+                                                          dq, dacc);
+        if ((e = cudaGetLastError()) ||
+            (e = cudaMemcpyAsync(acc.data(), dacc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
+            (e = cudaStreamSynchronize(st))) {
+            rc = aset(h, GDB_ERR_CUDA, "gdb_calc_dynamics: kernel", e);
+            break;
+        }
+        // per pair and type: the means over the type's particles (and, for
+        // Fs, components) added at the pair's time index, then / count
+        for (int p = 0; p < np_; p++)
+            for (int t = 0; t < ntypes; t++) {
+                if (nper[t] == 0) continue;
+                const double *a = &acc[((size_t)p * ntypes + t) * 3];
+                const size_t o = (size_t)tindex[p] * ntypes + t;
+                msd[o] += a[0] / nper[t];
+                m4d[o] += a[1] / nper[t];
+                fs[o] += a[2] / (3.0 * nper[t]);
+            }
+        for (int k = 0; k < total_times; k++)
+            for (int t = 0; t < ntypes; t++) {
+                const size_t o = (size_t)k * ntypes + t;
+                msd[o] /= count[k];
+                m4d[o] /= count[k];
+                fs[o] /= count[k];
+            }
+    } while (0);
+    if (dframes) cudaFreeAsync(dframes, st);
+    if (dpt) cudaFreeAsync(dpt, st);
+    if (dpairs) cudaFreeAsync(dpairs, st);
+    if (dq) cudaFreeAsync(dq, st);
+    if (dacc) cudaFreeAsync(dacc, st);
     cudaStreamSynchronize(st);
     cudaStreamDestroy(st);
     return rc;

@@ -39,3 +39,30 @@ class Evaluator:
             if k in conf.sid:
                 conf.scalars[:, conf.sid[k]] = sc[k]
         self.interactions[0].check_datastructure_validity()
+
+
+def calc_dynamics(trajectory, first_block, qvalues=None):
+    """Mean square displacement, non-Gaussian parameter and self-intermediate
+    scattering function from ConfigurationSaver frames, as
+    tools/calc_dynamics.py:23-75 (same lags, same return dictionary), with
+    the sums over particles on the GPU (gdb_calc_dynamics).  ``trajectory``
+    is a Simulation's output (``block`` frames, ``ptype``, attrs ``dt`` and
+    ``simbox_initial``); ``qvalues`` a float or one value per type."""
+    import math
+    ptype = np.asarray(trajectory["ptype"][:]).copy()
+    attrs = trajectory.attrs
+    simbox = np.asarray(attrs["simbox_initial"]).copy()
+    num_types = int(np.max(ptype)) + 1
+    if isinstance(qvalues, float):
+        qvalues = np.ones(num_types) * qvalues
+    blocks = np.asarray(trajectory["block"])
+    num_blocks, conf_per_block, _, n, d = blocks.shape
+    if first_block > num_blocks - 1:
+        print("Warning [calc_dynamics] first_block greater than number of blocks. Remainder will be taken")
+    first_block = first_block % num_blocks
+    extra_times = int(math.log2(num_blocks - first_block)) - 1
+    total_times = conf_per_block - 1 + extra_times
+    msd, m4d, fs, count = _lib.calc_dynamics(blocks, ptype, simbox, first_block, qvalues, total_times)
+    times = attrs["dt"] * 2 ** np.arange(total_times)
+    alpha2 = 3 * m4d / (5 * msd ** 2) - 1
+    return {"times": times, "msd": msd, "alpha2": alpha2, "qvalues": qvalues, "Fs": fs, "count": count}

@@ -241,6 +241,19 @@ int gdb_rdf_compute(int n, const float *r, const int32_t *ptype, const float box
 int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], int nq, const int32_t *n_vectors,
                    double *rho_re, double *rho_im);
 
+/* Trajectory dynamics (tools/calc_dynamics.py:6-75) of ConfigurationSaver
+ * frames: frames num_blocks x conf_per_block x 2 x n x 3 float32 (positions,
+ * then image counts; the `block` dataset), ptype n int32 in [0, ntypes),
+ * ntypes <= 8, box the initial box, qvalues ntypes float64.  Lags as the
+ * reference: frame i+1 against frame 0 of each block from first_block on,
+ * then first frames 2^(i+1) blocks apart; total_times = conf_per_block - 1 +
+ * int(log2(num_blocks - first_block)) - 1.  Outputs total_times x ntypes
+ * float64 msd, m4d (mean dr^4) and fs (mean cos(q dr) over particles and
+ * components), already divided by count (total_times int32). */
+int gdb_calc_dynamics(int num_blocks, int conf_per_block, int n, const float *frames, const int32_t *ptype,
+                      int ntypes, const float box[3], int first_block, const double *qvalues, int total_times,
+                      double *msd, double *m4d, double *fs, int32_t *count);
+
 /* Batched replicas (no counterpart in the reference, whose users loop over
  * state points one Simulation at a time, e.g. examples/isomorph.py:27-82):
  * advance many independent, fully configured and uploaded systems together.

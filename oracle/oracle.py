@@ -10,6 +10,7 @@ int32, parameter tables (ntypes, ntypes, nparams) float32 with the cut last
 int32 with the count in the last column (gamdpy/interactions/nblist.py:8).
 """
 import ctypes
+import math
 import os
 import subprocess
 
@@ -218,6 +219,53 @@ def sq(r, q, ff=None):
     im = np.zeros(len(q), np.float64)
     lib().orc_sq(len(r), _p(r), _p(ffa), len(q), _p(q), _p(re), _p(im))
     return re + 1j * im
+
+
+def calc_dynamics(block, ptype, box, dt, first_block, qvalues=None):
+    """tools/calc_dynamics.py:6-75 restated: per time lag and type, the mean
+    square displacement, the mean fourth power, and the self-intermediate
+    scattering function (the mean of cos(q dr) over particles and
+    components); lags inside a block (frame i+1 against frame 0) and across
+    blocks (first frames 2^(i+1) blocks apart); displacements unwrapped with
+    the image counts; alpha2 = 3 m4d / (5 msd^2) - 1."""
+    block = np.asarray(block)
+    ptype = np.asarray(ptype)
+    box = np.asarray(box, np.float32)
+    num_types = int(ptype.max()) + 1
+    if isinstance(qvalues, float):
+        qvalues = np.ones(num_types) * qvalues
+    num_blocks, conf_per_block, _, n, d = block.shape
+    first_block = first_block % num_blocks
+    extra = int(math.log2(num_blocks - first_block)) - 1
+    total = conf_per_block - 1 + extra
+    count = np.zeros((total, 1), np.int32)
+    msd, m4d, fs = (np.zeros((total, num_types)) for _ in range(3))
+
+    def add(b0, c0, b1, c1, ti):
+        dr = block[b1, c1, 0] - block[b0, c0, 0]
+        dr += (block[b1, c1, 1] - block[b0, c0, 1]) * box
+        for t in range(num_types):
+            dt_ = dr[ptype == t]
+            sq = np.sum(dt_ ** 2, axis=1)
+            msd[ti, t] += np.mean(sq)
+            m4d[ti, t] += np.mean(sq ** 2)
+            fs[ti, t] += np.mean(np.cos(dt_ * qvalues[t]))
+
+    for b in range(first_block, num_blocks):
+        for i in range(conf_per_block - 1):
+            count[i] += 1
+            add(b, i + 1, b, 0, i)
+    for b in range(first_block, num_blocks):
+        for i in range(extra):
+            other = b + 2 ** (i + 1)
+            if other < num_blocks:
+                count[conf_per_block - 1 + i] += 1
+                add(other, 0, b, 0, conf_per_block - 1 + i)
+    msd /= count
+    m4d /= count
+    fs /= count
+    return {"times": dt * 2 ** np.arange(total), "msd": msd, "alpha2": 3 * m4d / (5 * msd ** 2) - 1,
+            "qvalues": qvalues, "Fs": fs, "count": count}
 
 
 def xoro_states(n, seed):

@@ -166,3 +166,18 @@ def test_langevin_random_numbers_pin_to_numba(oracle):
     normals = np.array([[oracle.xoro_normal_f32(st, i) for _ in range(d["normals"].shape[1])] for i in range(n)],
                        np.float32)
     assert np.array_equal(normals.view(np.int32), d["normals"].view(np.int32))
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_calc_dynamics_restatement_vs_gamdpy(oracle, tag):
+    """The oracle's restatement of tools/calc_dynamics.py against the output
+    of gamdpy's own function on the same synthetic trajectory."""
+    d = golden("dynamics")
+    q = d[f"{tag}_qvalues"]
+    q = float(q[0]) if tag == "a" else q
+    res = oracle.calc_dynamics(d["block"], d["ptype"], d["simbox_initial"], float(d["dt"]),
+                               int(d[f"{tag}_first_block"]), qvalues=q)
+    assert np.array_equal(res["count"], d[f"{tag}_count"])
+    np.testing.assert_allclose(res["times"], d[f"{tag}_times"], rtol=1e-12)
+    for k in ("msd", "alpha2", "Fs"):
+        np.testing.assert_allclose(res[k], d[f"{tag}_{k}"], rtol=1e-12, atol=1e-12)
