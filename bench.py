@@ -34,6 +34,20 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MATS (million atom-timesteps/s), KA-LJ NVT cell lists, 1 B200"
 UNIT = "Matom-steps/s"
+MOMENTUM_RESET_EVERY = 100  # the only runtime action, as benchmarks/benchmark_LJ.py:28-47
+
+
+def ka_workload(n, langevin=False):
+    """The workload string both arms print in ``config`` (the same system,
+    integrator, list and runtime actions)."""
+    thermo = "NVT_Langevin alpha=0.2" if langevin else "NVT Nose-Hoover tau=0.2"
+    return (f"KA-LJ 80:20 SF rc=2.5 sigma_ab, rho=1.2, {thermo} T=0.45, dt=0.005, cells skin=0.3, "
+            f"MomentumReset({MOMENTUM_RESET_EVERY}), N={n}")
+
+
+def ka_config(n, langevin=False):
+    return {"workload": ka_workload(n, langevin), "n": n,
+            "l2": "per-step working set (neighbour list, ~0.45 GB at N=1M) > 126 MB L2, no flush"}
 
 
 def parse():
@@ -59,6 +73,8 @@ def parse():
     p.add_argument("--lj-cells", type=int, default=128,
                    help="lj8m: FCC unit cells per side (128: 8 388 608 particles; smaller for profiling)")
     p.add_argument("--autotune", action="store_true", help="batch: pick particles per CTA by timing")
+    p.add_argument("--no-extras", action="store_true",
+                   help="default line without the small-N and batch sub-measurements")
     return p.parse_args()
 
 
@@ -216,12 +232,14 @@ def cpu_reference(args, n, steps, seed=0):
     # the reference's default list kind by size (get_default_compute_plan.py:83-86)
     nblist = "linked lists" if n > 6000 else "N squared"
     run = O.Run(conf["r"], conf["v"], conf["m"], conf.ptype, conf.simbox.lengths, tab, nblist=nblist,
-                skin=0.3, max_nbs=300, integrator="NVT", dt=0.005, temperature=0.45, tau=0.2)
+                skin=0.3, max_nbs=300, integrator="NVT", dt=0.005, temperature=0.45, tau=0.2,
+                reset_every=MOMENTUM_RESET_EVERY)
     run.run_timeblock(1)  # first list build outside the timing, as the GPU warm-up
+    r0 = run.rebuilds
     t0 = time.perf_counter()
     run.run_timeblock(steps)
     dt = time.perf_counter() - t0
-    return n * steps / dt / 1e6, O.num_threads(), dt
+    return n * steps / dt / 1e6, O.num_threads(), dt, run.rebuilds - r0
 
 
 SWEEP_N = (512, 2048, 8192, 65536, 262144, 1048576)
@@ -246,7 +264,7 @@ def run_sweep(args):
         nblocks = max(2, min(200, int(2e8 / n / block)))
         plan = {"pb": 64, "tp": 1, "lanes": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
                 "nblist": "linked lists"}
-        sim = gp.Simulation(conf, pp, integ, [gp.ScalarSaver(block // 8)], num_timeblocks=8,
+        sim = gp.Simulation(conf, pp, integ, [gp.MomentumReset(MOMENTUM_RESET_EVERY)], num_timeblocks=8,
                             steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
         dev = sim._sim
         dev.run(0.0, max(3, args.warmup))
@@ -265,7 +283,7 @@ def run_sweep(args):
                 "algorithmic_bytes_per_atom_step": bpa, "n_gpus": world}
         if rank == 0 and world == 1:
             cps = max(2, min(400, int(3e6 / n)))
-            cmats, threads, secs = cpu_reference(args, n, cps)
+            cmats, threads, secs, _ = cpu_reference(args, n, cps)
             line["cpu_baseline"] = {"value": cmats, "unit": UNIT, "cores": threads, "kind": "port",
                                     "sample": f"{cps} steps ({secs:.1f} s)"}
         if rank == 0:
@@ -283,21 +301,18 @@ def run_reference_arm(args):
         if pg is not None:
             pg.destroy_process_group()
         return
-    # bounded sample: a few steps of the full-size system (~tens of seconds)
-    steps = max(1, min(args.steps, 5))
-    vals = []
-    for _ in range(max(1, min(args.warmup, 1))):
-        cpu_reference(args, args.n, 1)
-    mats, threads, secs = cpu_reference(args, args.n, steps)
-    vals.append(mats)
+    # bounded sample of the same workload: up to 50 steps of the full-size
+    # system after the first list build (~10 s on 16 host threads at N = 1M),
+    # so the sample holds neighbour-list rebuilds as the GPU arm's steps do
+    steps = max(1, min(args.steps, 50))
+    mats, threads, secs, rebuilds = cpu_reference(args, args.n, steps)
+    sample = f"{steps} steps of the N={args.n} system after one list build ({rebuilds} list rebuilds inside)"
     line = {
         "impl": "reference", "metric": METRIC, "value": mats, "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": 1, "ms_per_step": secs / steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattice)",
-        "config": {"workload": f"KA-LJ NVT rho=1.2 T=0.45 cells skin=0.3 N={args.n}", "n": args.n,
-                   "parallelism": "host threads"},
-        "cpu_baseline": {"value": mats, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": f"{steps} steps of N={args.n} after one list build"},
+        "config": ka_config(args.n),
+        "cpu_baseline": {"value": mats, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": mats, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -306,18 +321,20 @@ def run_reference_arm(args):
         pg.destroy_process_group()
 
 
-def run_batch(args):
-    """Batched replicas: ``--replicas`` KA systems (N log-uniform 256-32768,
+def measure_batch(local, replicas, steps, block, warmup, autotune=False, seed=2024, e2e_blocks=0):
+    """Batched replicas: ``replicas`` KA systems (N log-uniform 256-32768,
     rho in [1.1, 1.3], T in [0.4, 1.0], NVT dt 0.005, cells skin 0.3) advanced
     together by SimulationBatch, against the same systems advanced one after
-    another through Simulation (each its own launches)."""
-    rank, world, local, pg = dist_setup(args)
+    another through Simulation (each its own launches).  Device times in ms;
+    with e2e_blocks > 0 also the wall time of that many timeblocks through
+    SimulationBatch.run_timeblocks (upload once, per timeblock every
+    replica's state back to the host)."""
     import gamdpy_b200 as gp
     from gamdpy_b200 import workloads
 
-    points = workloads.ka_replica_sweep(args.replicas, seed=2024 + rank)
-    block = min(args.block, max(1, args.steps))
-    nblocks = max(1, args.steps // block)
+    points = workloads.ka_replica_sweep(replicas, seed=seed)
+    block = min(block, max(1, steps))
+    nblocks = max(1, steps // block)
     steps = nblocks * block
     plan = {"pb": 64, "tp": 1, "lanes": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
             "nblist": "linked lists"}
@@ -326,27 +343,26 @@ def run_batch(args):
         conf = workloads.ka_configuration(n, rho=rho, temperature=temp, seed=k)
         integ = gp.integrators.NVT(temperature=temp, tau=0.2, dt=0.005)
         sims.append(gp.Simulation(conf, workloads.ka_pair_potential(max_num_nbs=300), integ,
-                                  [gp.ScalarSaver(max(1, block // 8))], num_timeblocks=nblocks,
+                                  [gp.MomentumReset(MOMENTUM_RESET_EVERY)], num_timeblocks=max(nblocks, e2e_blocks),
                                   steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local))
     total_n = sum(p[0] for p in points)
     batch = gp.SimulationBatch(sims)
-    tuned = batch.autotune(steps=min(block, 200)) if args.autotune else batch.particles_per_cta
-    # warm-up of both paths
-    for s in sims:
-        s.configuration.copy_to_device()
-        s._sim.run(0.0, max(3, min(args.warmup, block)))
-    batch.integrate_self(0.0, max(3, min(args.warmup, block)))
-    barrier(pg)
+    tuned = batch.autotune(steps=min(block, 200)) if autotune else batch.particles_per_cta
+    w = max(3, min(warmup, block))
+    for s_ in sims:  # warm-up of both paths
+        s_.configuration.copy_to_device()
+        s_._sim.run(0.0, w)
+    batch.integrate_self(0.0, w)
     # sequential: every replica's timeblocks, one replica after another
-    for s in sims:
-        s.configuration.copy_to_device()
+    for s_ in sims:
+        s_.configuration.copy_to_device()
     ms_seq = 0.0
-    for s in sims:
+    for s_ in sims:
         for b in range(nblocks):
-            ms_seq += s._sim.run(float(b * block * 0.005), block)
-    # batched: one launch per timeblock for all replicas
-    for s in sims:
-        s.configuration.copy_to_device()
+            ms_seq += s_._sim.run(float(b * block * 0.005), block)
+    # batched: one call per timeblock for all replicas
+    for s_ in sims:
+        s_.configuration.copy_to_device()
     clocks = ClockSampler(local)
     clocks.start()
     ms_bat = 0.0
@@ -354,36 +370,52 @@ def run_batch(args):
         ms_bat += batch.integrate_self(float(b * block * 0.005), block)
     clock_info = clocks.stop()
     paths = batch.paths()
-    t_bat = allreduce_max(pg, ms_bat / 1e3, local)
-    t_seq = allreduce_max(pg, ms_seq / 1e3, local)
-    # end to end through the public API: SimulationBatch.run_timeblocks
-    # (upload once, per timeblock the state of every replica back to the host)
-    e2e_blocks = max(1, min(nblocks, 2))
-    t0 = time.perf_counter()
-    for _ in batch.run_timeblocks(e2e_blocks):
-        pass
-    e2e_s = allreduce_max(pg, time.perf_counter() - t0, local)
+    out = {"workload": f"{replicas} KA-LJ NVT replicas (N 256-32768 log-uniform, rho 1.1-1.3, T 0.4-1.0), "
+                       f"cells skin=0.3, MomentumReset({MOMENTUM_RESET_EVERY}), total N={total_n}",
+           "replicas": replicas, "total_n": total_n, "steps": steps, "timeblock_steps": block,
+           "ms_batched": ms_bat, "ms_sequential": ms_seq,
+           "mats_batched": total_n * steps / ms_bat / 1e3, "mats_sequential": total_n * steps / ms_seq / 1e3,
+           "speedup_vs_sequential": ms_seq / ms_bat, "particles_per_cta": tuned,
+           "cluster_systems": int(sum(1 for p in paths if p == 2)),
+           "grid_systems": int(sum(1 for p in paths if p != 2)), "clocks": clock_info}
+    if e2e_blocks > 0:
+        t0 = time.perf_counter()
+        for _ in batch.run_timeblocks(e2e_blocks):
+            pass
+        out["e2e_s"] = time.perf_counter() - t0
+        out["e2e_blocks"] = e2e_blocks
+    del batch, sims
+    return out
+
+
+def run_batch(args):
+    rank, world, local, pg = dist_setup(args)
+    r = measure_batch(local, args.replicas, args.steps, args.block, args.warmup, autotune=args.autotune,
+                      seed=2024 + rank, e2e_blocks=2)
+    steps, block, total_n = r["steps"], r["timeblock_steps"], r["total_n"]
+    t_bat = allreduce_max(pg, r["ms_batched"] / 1e3, local)
+    t_seq = allreduce_max(pg, r["ms_sequential"] / 1e3, local)
+    e2e_s = allreduce_max(pg, r["e2e_s"], local)
+    e2e_steps = r["e2e_blocks"] * block
     h2d = total_n * (12 + 12 + 4 + 4 + 12)
     d2h = total_n * (12 + 12 + 12 + 12 + 4 * 5)
-    mats = total_n * steps * world / t_bat / 1e6
     line = {
-        "metric": "MATS batched KA replicas (N 256-32768, rho 1.1-1.3, T 0.4-1.0), 1 B200", "value": mats,
-        "unit": UNIT, "n_gpus": world, "steps": steps, "warmup": max(3, min(args.warmup, block)),
-        "ms_per_step": t_bat * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f32", "data": "synthetic (seeded KA lattices)",
-        "config": {"workload": f"{args.replicas} KA-LJ NVT replicas, cells skin=0.3, total N={total_n}",
-                   "replicas": args.replicas, "total_n": total_n, "timeblock_steps": block,
-                   "particles_per_cta": tuned, "cluster_systems": int(sum(1 for p in paths if p == 2)),
-                   "grid_systems": int(sum(1 for p in paths if p != 2)),
+        "metric": "MATS batched KA replicas (N 256-32768, rho 1.1-1.3, T 0.4-1.0), 1 B200",
+        "value": total_n * steps * world / t_bat / 1e6, "unit": UNIT, "n_gpus": world, "steps": steps,
+        "warmup": max(3, min(args.warmup, block)), "ms_per_step": t_bat * 1e3 / steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattices)",
+        "config": {"workload": r["workload"], "replicas": args.replicas, "total_n": total_n,
+                   "timeblock_steps": block, "particles_per_cta": r["particles_per_cta"],
+                   "cluster_systems": r["cluster_systems"], "grid_systems": r["grid_systems"],
                    "l2": "working set of all replicas > 126 MB L2, no flush"},
         "sequential": {"value": total_n * steps * world / t_seq / 1e6, "unit": UNIT,
                        "ms_per_step": t_seq * 1e3 / steps,
                        "note": "the same replicas, one Simulation after another (device time summed)"},
         "speedup_vs_sequential": t_seq / t_bat,
-        "e2e": {"value": total_n * e2e_blocks * block * world / e2e_s / 1e6, "unit": UNIT,
-                "h2d_bytes_per_step": h2d / (e2e_blocks * block), "d2h_bytes_per_step": d2h / (e2e_blocks * block),
+        "e2e": {"value": total_n * e2e_steps * world / e2e_s / 1e6, "unit": UNIT,
+                "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
                 "timeblock_steps": block},
-        "clocks": clock_info,
+        "clocks": r["clocks"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -392,51 +424,92 @@ def run_batch(args):
         pg.destroy_process_group()
 
 
-def run_lj_small(args):
+def measure_lj2048(local, steps, block, warmup, seed=0, e2e_blocks=0):
     """The reference's small plain case: single-component LJ (shifted force,
     rc = 2.5), FCC 8x8x8 = 2048 particles at rho = 0.973, Maxwell-Boltzmann
-    velocities at T = 0.7 (seeded), NVE dt = 0.005, N^2 list with skin 0.5.
-    TPS and MATS over the timeblocks' device time."""
+    velocities at T = 0.7 (seeded), NVE dt = 0.005, N^2 list with skin 0.5,
+    MomentumReset(100) as the reference's benchmark.  TPS and MATS over the
+    timeblocks' device time."""
     import gamdpy_b200 as gp
     from gamdpy_b200 import workloads
-    rank, world, local, pg = dist_setup(args)
-    conf = workloads.lj_configuration([8, 8, 8], 0.973, 0.7, seed=rank)
+    conf = workloads.lj_configuration([8, 8, 8], 0.973, 0.7, seed=seed)
     n = conf.N
     pp = workloads.lj_pair_potential(cut=2.5, shifted_force=True, max_num_nbs=300)
-    block = min(args.block, max(1, args.steps))
-    nblocks = max(1, args.steps // block)
+    block = min(block, max(1, steps))
+    nblocks = max(1, steps // block)
     steps = nblocks * block
-    plan = {"pb": 8, "tp": 16, "lanes": args.tp, "skin": 0.5, "UtilizeNIII": False, "gridsync": True,
+    plan = {"pb": 8, "tp": 16, "lanes": 0, "skin": 0.5, "UtilizeNIII": False, "gridsync": True,
             "nblist": "N squared"}
-    sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.005), [gp.MomentumReset(100)], num_timeblocks=nblocks,
-                        steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
+    sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.005), [gp.MomentumReset(MOMENTUM_RESET_EVERY)],
+                        num_timeblocks=nblocks, steps_per_timeblock=block, compute_plan=plan, storage="memory",
+                        device=local)
     dev = sim._sim
-    dev.run(0.0, max(3, args.warmup))
-    barrier(pg)
+    dev.run(0.0, max(3, warmup))
     clocks = ClockSampler(local)
     clocks.start()
     ms = sum(dev.run(float(b * block * 0.005), block) for b in range(nblocks))
     clock_info = clocks.stop()
-    t_max = allreduce_max(pg, ms / 1e3, local)
-    e2e_blocks = max(1, min(nblocks, 4))
-    t0 = time.perf_counter()
-    conf.copy_to_device()
-    for b in range(e2e_blocks):
-        dev.run(float(b * block * 0.005), block)
-        conf.copy_to_host()
-    e2e_s = allreduce_max(pg, time.perf_counter() - t0, local)
+    out = {"workload": "LJ SF rc=2.5, FCC 8x8x8 N=2048 rho=0.973 T=0.7, NVE dt=0.005, N^2 list skin 0.5, "
+                       f"MomentumReset({MOMENTUM_RESET_EVERY})",
+           "n": n, "steps": steps, "timeblock_steps": block, "ms": ms, "tps": steps / ms * 1e3,
+           "mats": n * steps / ms / 1e3, "ms_per_step": ms / steps, "path": dev.last_path(), "clocks": clock_info}
+    if e2e_blocks > 0:
+        t0 = time.perf_counter()
+        conf.copy_to_device()
+        for b in range(e2e_blocks):
+            dev.run(float(b * block * 0.005), block)
+            conf.copy_to_host()
+        out["e2e_s"] = time.perf_counter() - t0
+        out["e2e_blocks"] = e2e_blocks
+    return out
+
+
+def measure_ka(local, n, steps, block, warmup, seed=1234, tp=0):
+    """KA workload at N particles (the default line's system at another
+    size): TPS and MATS over the timeblocks' device time, with the path the
+    library chose."""
+    import gamdpy_b200 as gp
+    from gamdpy_b200 import workloads
+    conf = workloads.ka_configuration(n, seed=seed)
+    pp = workloads.ka_pair_potential(max_num_nbs=300)
+    integ = gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
+    block = min(block, max(1, steps))
+    nblocks = max(1, steps // block)
+    steps = nblocks * block
+    plan = {"pb": 64, "tp": 1, "lanes": tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
+            "nblist": "linked lists"}
+    sim = gp.Simulation(conf, pp, integ, [gp.MomentumReset(MOMENTUM_RESET_EVERY)], num_timeblocks=nblocks,
+                        steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
+    dev = sim._sim
+    dev.run(0.0, max(3, warmup))
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms = sum(dev.run(float(b * block * 0.005), block) for b in range(nblocks))
+    clock_info = clocks.stop()
+    path = dev.last_path()
+    return {"workload": ka_workload(n), "n": n, "steps": steps, "timeblock_steps": block, "ms": ms,
+            "tps": steps / ms * 1e3, "mats": n * steps / ms / 1e3, "ms_per_step": ms / steps,
+            "path": ["graph", "persistent", "cluster"][path] if 0 <= path <= 2 else path, "clocks": clock_info}
+
+
+def run_lj_small(args):
+    rank, world, local, pg = dist_setup(args)
+    r = measure_lj2048(local, args.steps, args.block, args.warmup, seed=rank, e2e_blocks=4)
+    n, steps, block = r["n"], r["steps"], r["timeblock_steps"]
+    t_max = allreduce_max(pg, r["ms"] / 1e3, local)
+    e2e_s = allreduce_max(pg, r["e2e_s"], local)
     tps = steps / t_max
+    e2e_blocks = r["e2e_blocks"]
     line = {
         "metric": "TPS (time steps/s), LJ N=2048 NVE N^2 list, 1 B200", "value": tps * world, "unit": "steps/s",
         "n_gpus": world, "steps": steps, "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded FCC lattice)",
-        "config": {"workload": "LJ SF rc=2.5, FCC 8x8x8 N=2048 rho=0.973 T=0.7, NVE dt=0.005, N^2 list skin 0.5",
-                   "n": n, "mats": n * tps * world / 1e6, "timeblock_steps": block, "path": dev.last_path(),
-                   "l2": "working set < L2; the metric is step latency, so no flush"},
+        "config": {"workload": r["workload"], "n": n, "mats": n * tps * world / 1e6, "timeblock_steps": block,
+                   "path": r["path"], "l2": "working set < L2; the metric is step latency, so no flush"},
         "e2e": {"value": e2e_blocks * block * world / e2e_s, "unit": "steps/s",
                 "h2d_bytes_per_step": n * 44 / (e2e_blocks * block), "d2h_bytes_per_step": n * 68 / block},
-        "clocks": clock_info,
+        "clocks": r["clocks"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -651,16 +724,18 @@ def main():
     block = min(args.block, max(1, args.steps))
     plan = {"pb": 64, "tp": 1, "lanes": args.tp, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
             "nblist": "linked lists"}
-    sim = gp.Simulation(conf, pp, integ, [gp.ScalarSaver(max(1, block // 8))], num_timeblocks=8,
-                        steps_per_timeblock=block, compute_plan=plan, storage="memory", device=local)
+    nblocks = max(1, args.steps // block)
+    steps = nblocks * block
+    e2e_blocks = max(1, min(nblocks, 4))
+    sim = gp.Simulation(conf, pp, integ, [gp.MomentumReset(MOMENTUM_RESET_EVERY)],
+                        num_timeblocks=max(nblocks, e2e_blocks), steps_per_timeblock=block, compute_plan=plan,
+                        storage="memory", device=local)
     dev = sim._sim
-    # warm-up (device resident), includes graph capture
+    # warm-up (device resident)
     dev.run(0.0, max(3, args.warmup))
     dev.clear_status()
 
     # ---- timed: K steps, device-resident inputs ---------------------------
-    nblocks = max(1, args.steps // block)
-    steps = nblocks * block
     if args.profile:
         if args.trace:
             dev.set_trace(1 << 20)
@@ -685,24 +760,24 @@ def main():
     t_max = allreduce_max(pg, ms_total / 1e3, local)
     mats = n * steps * world / t_max / 1e6
     tps = steps / t_max
+    mean_nbs, max_nbs = dev.nblist_stats()
 
     # ---- end to end through the public API (host buffers) ------------------
     # gamdpy's pattern (Simulation.run_timeblocks): upload once, then every
-    # timeblock run on the device and copy r, v, f, images and scalars back
-    e2e_blocks = max(1, min(nblocks, 4))
+    # timeblock run on the device and copy r, v, f, images and the per-particle
+    # scalars back into the Configuration's arrays
     barrier(pg)
     t0 = time.perf_counter()
-    conf.copy_to_device()
-    for b in range(e2e_blocks):
-        dev.run(float(b * block * 0.005), block)
-        conf.copy_to_host()
+    for _ in sim.run_timeblocks(e2e_blocks):
+        pass
     e2e_s = allreduce_max(pg, time.perf_counter() - t0, local)
     e2e_steps = e2e_blocks * block
     h2d = n * (12 + 12 + 4 + 4 + 12)  # r, v, m, type, images
     d2h = n * (12 + 12 + 12 + 12 + 4 * 5)  # r, v, f, images, 5 scalar planes
     e2e = {"value": n * e2e_steps * world / e2e_s / 1e6, "unit": UNIT,
            "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": d2h / e2e_steps,
-           "timeblock_steps": block, "note": "upload once + per-timeblock device->host copy of the state"}
+           "timeblock_steps": block, "note": "Simulation.run_timeblocks: upload once + per-timeblock "
+                                             "device->host copy of the state into the Configuration"}
 
     # ---- roofline of the dominant kernel: k_run, one launch per timeblock --
     # (block steps + the final evaluation, rebuilds included).  Algorithmic
@@ -710,7 +785,6 @@ def main():
     # r and v read and written); per launch B * N * block.  The launch time is
     # the timeblock's CUDA-event time on the library's stream (the events
     # bracket k_block_begin + k_run, nothing else runs on that stream).
-    mean_nbs, max_nbs = dev.nblist_stats()
     bytes_per_atom = 4.0 * mean_nbs + 64.0
     ms_launch = t_max * 1e3 / nblocks
     achieved = bytes_per_atom * n * block / (ms_launch * 1e-3) / 1e9
@@ -726,11 +800,9 @@ def main():
         "metric": METRIC, "value": mats, "unit": UNIT, "n_gpus": world, "steps": steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_max * 1e3 / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattice)",
-        "config": {"workload": f"KA-LJ {'NVT_Langevin alpha=0.2' if args.langevin else 'NVT'} rho=1.2 T=0.45 "
-                               f"dt=0.005 cells skin=0.3 N={n}", "n": n,
-                   "tps": tps, "timeblock_steps": block, "parallelism": f"replicas x{world}",
-                   "l2": "per-step working set (neighbour list) > 126 MB L2, no flush",
-                   "mean_neighbours": mean_nbs, "max_neighbours": max_nbs},
+        "config": ka_config(n, args.langevin),
+        "measured": {"tps": tps, "timeblock_steps": block, "parallelism": f"replicas x{world}",
+                     "mean_neighbours": mean_nbs, "max_neighbours": max_nbs, "path": dev.last_path()},
         "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,
@@ -743,11 +815,22 @@ def main():
         "clocks": clock_info,
         "gpu_launches": launches_per_block * nblocks,
     }
+    del sim, dev
+    if not args.no_extras:
+        # the reference's small plain case and the KA system at N = 2048 (TPS,
+        # 10^4 steps each), and batched replicas against sequential runs; each
+        # with its own clock record, measured after the main timed region
+        line["small_n"] = {
+            "lj2048": measure_lj2048(local, 10_000, 1000, 200, seed=rank),
+            "ka2048": measure_ka(local, 2048, 10_000, 1000, 200, seed=1234 + rank),
+        }
+        line["batch"] = measure_batch(local, 128, 1000, 500, 10, seed=2024 + rank)
     if rank == 0 and world == 1:
         cps = max(1, min(50, args.steps))  # about 10 s of host work at N = 1M
-        cmats, threads, secs = cpu_reference(args, n, cps)
+        cmats, threads, secs, rebuilds = cpu_reference(args, n, cps)
         line["cpu_baseline"] = {"value": cmats, "unit": UNIT, "cores": threads, "kind": "port",
-                                "sample": f"{cps} steps of the same N={n} system ({secs:.1f} s)"}
+                                "sample": f"{cps} steps of the same N={n} system ({secs:.1f} s, "
+                                          f"{rebuilds} list rebuilds)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(pg)

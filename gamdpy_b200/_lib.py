@@ -370,8 +370,12 @@ def calc_dynamics(frames, ptype, box, first_block, qvalues, total_times):
     if two != 2 or d != 3:
         raise ValueError("frames must be (num_blocks, conf_per_block, 2, N, 3)")
     pt = i32(ptype, (n,))
-    nt = int(len(qvalues))
-    q = np.ascontiguousarray(np.asarray(qvalues, np.float64))
+    # one column per type 0 ... max(ptype), as tools/calc_dynamics.py:30
+    nt = int(pt.max()) + 1
+    qv = np.asarray(qvalues, np.float64).reshape(-1)
+    if qv.shape[0] < nt:
+        raise ValueError(f"calc_dynamics: {qv.shape[0]} q-values for {nt} particle types")
+    q = np.ascontiguousarray(qv[:nt])
     L = f32(box, (3,))
     msd, m4d, fs = (np.zeros((total_times, nt)) for _ in range(3))
     count = np.zeros((total_times, 1), np.int32)

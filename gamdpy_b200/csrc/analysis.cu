@@ -1040,6 +1040,31 @@ int gdb_sq_compute(int n, const float *r, const float *ff, const float box[3], i
     return rc;
 }
 
+// Frames of the blocks from first_block on are uploaded in groups of whole
+// blocks that fit a staging budget (1 GiB, GDB_DYN_STAGE_BYTES overrides it),
+// plus one buffer with the first frame of every such block for the lags
+// longer than a block; frame pairs are launched at most 65535 per grid
+// (GDB_DYN_PAIR_CHUNK lowers it), the y extent of a CUDA grid.
+static size_t env_size(const char *name, size_t dflt) {
+    const char *v = getenv(name);
+    if (!v || !*v) return dflt;
+    const long long x = atoll(v);
+    return x > 0 ? (size_t)x : dflt;
+}
+
+static cudaError_t dyn_launch(cudaStream_t st, int gx, const float *frames, int n, const int *dpt, int nt,
+                              const float *box, const int2 *dpairs, const double *dq, double *dacc, int count,
+                              int chunk) {
+    for (int off = 0; off < count; off += chunk) {
+        const int c = std::min(chunk, count - off);
+        k_dynamics<<<dim3(gx, c), DYN_THREADS, 0, st>>>(frames, n, dpt, nt, box[0], box[1], box[2], dpairs + off, dq,
+                                                        dacc + (size_t)off * nt * 3);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
 int gdb_calc_dynamics(int num_blocks, int conf_per_block, int n, const float *frames, const int32_t *ptype,
                       int ntypes, const float box[3], int first_block, const double *qvalues, int total_times,
                       double *msd, double *m4d, double *fs, int32_t *count) {
@@ -1062,44 +1087,54 @@ int gdb_calc_dynamics(int num_blocks, int conf_per_block, int n, const float *fr
         if (ptype[i] < 0 || ptype[i] >= ntypes) return aset(h, GDB_ERR_ARG, "gdb_calc_dynamics: type out of range");
         nper[ptype[i]]++;
     }
-    // frame pairs in the reference's loop order (calc_dynamics.py:52-68)
+    const int fb = first_block, nblk = num_blocks - first_block, cpb = conf_per_block;
+    const size_t frame_floats = (size_t)2 * n * 3;
+    const size_t block_bytes = (size_t)cpb * frame_floats * sizeof(float);
+    const int group = (int)std::max<size_t>(1, std::min<size_t>(nblk, env_size("GDB_DYN_STAGE_BYTES", 1ull << 30) /
+                                                                       block_bytes));
+    const int chunk = (int)std::min<size_t>(65535, env_size("GDB_DYN_PAIR_CHUNK", 65535));
+    // frame pairs in the reference's loop order (calc_dynamics.py:50-63),
+    // as indices into the staging buffers: within-block lags into the
+    // group's buffer, longer lags into the buffer of first frames
     std::vector<int2> pairs;
     std::vector<int> tindex;
     for (int k = 0; k < total_times; k++) count[k] = 0;
-    for (int b = first_block; b < num_blocks; b++)
-        for (int i = 0; i < conf_per_block - 1; i++) {
+    for (int b = fb; b < num_blocks; b++) {
+        const int base = ((b - fb) % group) * cpb;
+        for (int i = 0; i < cpb - 1; i++) {
             count[i]++;
-            pairs.push_back(make_int2(b * conf_per_block + i + 1, b * conf_per_block));
+            pairs.push_back(make_int2(base + i + 1, base));
             tindex.push_back(i);
         }
-    for (int b = first_block; b < num_blocks; b++)
+    }
+    const int np_in = (int)pairs.size();
+    for (int b = fb; b < num_blocks; b++)
         for (int i = 0; i < extra; i++) {
             const int other = b + (2 << i);
             if (other < num_blocks) {
-                count[conf_per_block - 1 + i]++;
-                pairs.push_back(make_int2(other * conf_per_block, b * conf_per_block));
-                tindex.push_back(conf_per_block - 1 + i);
+                count[cpb - 1 + i]++;
+                pairs.push_back(make_int2(other - fb, b - fb));
+                tindex.push_back(cpb - 1 + i);
             }
         }
     const int np_ = (int)pairs.size();
     for (int k = 0; k < total_times * ntypes; k++) msd[k] = m4d[k] = fs[k] = 0.0;
-    if (np_ == 0) return GDB_OK;
     cudaStream_t st;
     ACK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
-    const size_t fbytes = (size_t)num_blocks * conf_per_block * 2 * n * 3 * sizeof(float);
-    float *dframes = nullptr;
+    float *dgroup = nullptr, *dfirst = nullptr;
     int *dpt = nullptr;
     int2 *dpairs = nullptr;
     double *dq = nullptr, *dacc = nullptr;
-    std::vector<double> acc((size_t)np_ * ntypes * 3);
+    std::vector<double> acc((size_t)std::max(np_, 1) * ntypes * 3);
     int rc = GDB_OK;
     do {
         cudaError_t e;
-        if ((e = pool_alloc(&dframes, fbytes, st)) || (e = pool_alloc(&dpt, (size_t)n * sizeof(int), st)) ||
-            (e = pool_alloc(&dpairs, (size_t)np_ * sizeof(int2), st)) ||
+        if ((e = pool_alloc(&dgroup, (size_t)group * block_bytes, st)) ||
+            (e = pool_alloc(&dfirst, (size_t)nblk * frame_floats * sizeof(float), st)) ||
+            (e = pool_alloc(&dpt, (size_t)n * sizeof(int), st)) ||
+            (e = pool_alloc(&dpairs, (size_t)std::max(np_, 1) * sizeof(int2), st)) ||
             (e = pool_alloc(&dq, (size_t)ntypes * sizeof(double), st)) ||
             (e = pool_alloc(&dacc, acc.size() * sizeof(double), st)) ||
-            (e = cudaMemcpyAsync(dframes, frames, fbytes, cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(dpt, ptype, (size_t)n * sizeof(int), cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(dpairs, pairs.data(), (size_t)np_ * sizeof(int2), cudaMemcpyHostToDevice, st)) ||
             (e = cudaMemcpyAsync(dq, qvalues, (size_t)ntypes * sizeof(double), cudaMemcpyHostToDevice, st)) ||
@@ -1108,16 +1143,34 @@ int gdb_calc_dynamics(int num_blocks, int conf_per_block, int n, const float *fr
             break;
         }
         const int gx = std::min((n + DYN_THREADS - 1) / DYN_THREADS, 64);
-        k_dynamics<<<dim3(gx, np_), DYN_THREADS, 0, st>>>(dframes, n, dpt, ntypes, box[0], box[1], box[2], dpairs,
-                                                          dq, dacc);
-        if ((e = cudaGetLastError()) ||
-            (e = cudaMemcpyAsync(acc.data(), dacc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
+        // lags within a block, one group of blocks at a time (stream order
+        // keeps a group's kernels ahead of the next group's upload)
+        for (int g0 = 0; g0 < nblk && !e; g0 += group) {
+            const int gb = std::min(group, nblk - g0);
+            const float *src = frames + (size_t)(fb + g0) * cpb * frame_floats;
+            if ((e = cudaMemcpyAsync(dgroup, src, (size_t)gb * block_bytes, cudaMemcpyHostToDevice, st))) break;
+            for (int b = 0; b < gb && !e; b++) {
+                const float *f0 = src + (size_t)b * cpb * frame_floats;
+                e = cudaMemcpyAsync(dfirst + (size_t)(g0 + b) * frame_floats, f0, frame_floats * sizeof(float),
+                                    cudaMemcpyHostToDevice, st);
+            }
+            if (e) break;
+            const int p0 = g0 * (cpb - 1), pc = gb * (cpb - 1);
+            e = dyn_launch(st, gx, dgroup, n, dpt, ntypes, box, dpairs + p0, dq, dacc + (size_t)p0 * ntypes * 3, pc,
+                           chunk);
+        }
+        // lags of whole blocks, between first frames
+        if (!e && np_ > np_in)
+            e = dyn_launch(st, gx, dfirst, n, dpt, ntypes, box, dpairs + np_in, dq,
+                           dacc + (size_t)np_in * ntypes * 3, np_ - np_in, chunk);
+        if (e || (e = cudaMemcpyAsync(acc.data(), dacc, acc.size() * sizeof(double), cudaMemcpyDeviceToHost, st)) ||
             (e = cudaStreamSynchronize(st))) {
             rc = aset(h, GDB_ERR_CUDA, "gdb_calc_dynamics: kernel", e);
             break;
         }
         // per pair and type: the means over the type's particles (and, for
-        // Fs, components) added at the pair's time index, then / count
+        // Fs, components) added at the pair's time index, then / count; a
+        // type without particles is NaN, as numpy's mean of an empty array
         for (int p = 0; p < np_; p++)
             for (int t = 0; t < ntypes; t++) {
                 if (nper[t] == 0) continue;
@@ -1130,12 +1183,17 @@ int gdb_calc_dynamics(int num_blocks, int conf_per_block, int n, const float *fr
         for (int k = 0; k < total_times; k++)
             for (int t = 0; t < ntypes; t++) {
                 const size_t o = (size_t)k * ntypes + t;
+                if (nper[t] == 0) {
+                    msd[o] = m4d[o] = fs[o] = NAN;
+                    continue;
+                }
                 msd[o] /= count[k];
                 m4d[o] /= count[k];
                 fs[o] /= count[k];
             }
     } while (0);
-    if (dframes) cudaFreeAsync(dframes, st);
+    if (dgroup) cudaFreeAsync(dgroup, st);
+    if (dfirst) cudaFreeAsync(dfirst, st);
     if (dpt) cudaFreeAsync(dpt, st);
     if (dpairs) cudaFreeAsync(dpairs, st);
     if (dq) cudaFreeAsync(dq, st);

@@ -32,7 +32,7 @@ namespace gdb {
 //   umm = (cm12 x12 + cm6 x6) / r^2
 // LJ_12_6_sigma_epsilon (potential_functions/LJ_12_6_sigma_epsilon.py:26-36):
 //   c = sigma^2, cu = 4eps(1, -1), cs = 24eps(2, -1), cm = 24eps(26, -7)
-// LJ_12_6 (potential_functions/LJ_12_6.py:71-78):
+// LJ_12_6 (potential_functions/LJ_12_6.py:34-41):
 //   c = 1, cu = (A12, A6), cs = (12 A12, 6 A6), cm = (156 A12, 42 A6)
 struct PairEntry {
     float c, cu12, cu6, cs12, cs6, cm12, cm6;

@@ -440,7 +440,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                         kin += 0.5f * m * v_mean * v_mean;
                         r[k] += vv[k] * a.dt;
                     }
-                } else {  // integrators/NVT.py:196-215
+                } else {  // integrators/NVT.py:83-102
                     const float factor = 0.5f * xi * a.dt;
                     const float plus = 1.0f / (1.0f + factor);
                     const float minus = 1.0f - factor;
@@ -540,12 +540,12 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
         __syncthreads();
         if (!eval) {
             const double time = ctrl->time_zero + (double)step * (double)a.dt;
-            if (INTEG == GDB_INTEGRATOR_NVT) {  // NVT.py:226-237
+            if (INTEG == GDB_INTEGRATOR_NVT) {  // NVT.py:113-124
                 const double T = target_temperature(a, time);
                 const double dev = 2.0 * stot[0] / ((double)a.dof * T) - 1.0;
                 xi = (float)((double)xi + (double)(a.dt * a.omega2) * dev);
             }
-            if (rank == 0 && tid == 0 && rec && step / a.every < a.nrows) {  // scalar_saver.py:274-288
+            if (rank == 0 && tid == 0 && rec && step / a.every < a.nrows) {  // scalar_saver.py:165-179
                 double *row = a.rows + (size_t)(step / a.every) * GDB_NUM_SCALARS;
                 row[GDB_SCALAR_U] = stot[1];
                 row[GDB_SCALAR_W] = stot[2];
@@ -553,7 +553,7 @@ __global__ void __launch_bounds__(CL_THREADS, 1) k_cluster_run(const ClusterJob 
                 row[GDB_SCALAR_K] = stot[0];
                 row[GDB_SCALAR_FSQ] = stot[4];
             }
-            if (reset && owner) {  // momentum_reset.py:379-393
+            if (reset && owner) {  // momentum_reset.py:64-78
                 v.x -= (float)(stot[5] / stot[8]);
                 v.y -= (float)(stot[6] / stot[8]);
                 v.z -= (float)(stot[7] / stot[8]);

@@ -4,8 +4,8 @@
 //   interactions/pair_potential.py:141-246   (forces, U, W, lapU)
 //   interactions/nblist.py:57-143            (N^2 list: check + build)
 //   interactions/nblist_linked_lists.py:84-218 (cell list: check, cells, build, clear)
-//   integrators/NVE.py:59-105, integrators/NVT.py:188-237
-//   runtime_actions/scalar_saver.py:270-304, runtime_actions/momentum_reset.py:372-408
+//   integrators/NVE.py:59-105, integrators/NVT.py:75-124
+//   runtime_actions/scalar_saver.py:161-197, runtime_actions/momentum_reset.py:44-103
 //   simulation/Simulation.py:306-346          (composed step loop)
 //
 // Design (see the layout notes in gdb_internal.cuh):
@@ -21,8 +21,10 @@
 //    unless the step kernel flagged a particle beyond skin/2.  Cell lists use a
 //    counting sort (histogram, scan, scatter, in-cell sort by user index) and
 //    physically reorder the particles by cell, so neighbour gathers hit L1/L2.
-//  * The launch sequence of a chunk of steps is captured once in a CUDA graph
-//    and replayed.
+//  * By default a timeblock is one launch of the persistent cooperative kernel
+//    k_run (md_kernels.cuh), or of the thread-block-cluster kernel for small
+//    systems (md_cluster.cu).  The fallback (GDB_PERSISTENT=0) captures the
+//    launch sequence of a chunk of steps once in a CUDA graph and replays it.
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdarg.h>
@@ -1020,7 +1022,7 @@ int gdb_get_thermostat_state(gdb_sim *h, float state[2]) {
     int rc = read_ctrl(h);
     if (rc) return rc;
     state[0] = h->h_ctrl->xi;
-    state[1] = 0.0f;  // the sum is consumed by every update, as NVT.py:236
+    state[1] = 0.0f;  // the sum is consumed by every update, as NVT.py:123
     return GDB_OK;
 }
 

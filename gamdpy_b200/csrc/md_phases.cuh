@@ -964,7 +964,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
             }
             a.rng[uidx] = st;
             a.lbeta[uidx] = make_float4(obk[0], obk[1], obk[2], 0.f);
-        } else {  // integrators/NVT.py:196-215
+        } else {  // integrators/NVT.py:83-102
             const float factor = 0.5f * xi * a.dt;
             const float plus = 1.0f / (1.0f + factor);
             const float minus = 1.0f - factor;
@@ -1060,8 +1060,8 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
 }
 
 // Fixed-order float64 sum of `nblocks` partial rows (blocks or rounds) and the
-// bookkeeping of a finished step (NVT.py:226-237, scalar_saver.py:274-288,
-// momentum_reset.py:379-393).  Run by one whole block.
+// bookkeeping of a finished step (NVT.py:113-124, scalar_saver.py:165-179,
+// momentum_reset.py:64-78).  Run by one whole block.
 template <int MODE>
 __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, double *s_red) {
     DevCtrl *ctrl = a.ctrl;

@@ -33,7 +33,7 @@ def _check_nonneg_int(name, value):
 
 class ScalarSaver(RuntimeAction):
     """Sums of per-particle scalars every ``steps_between_output`` steps
-    (runtime_actions/scalar_saver.py:9-313).  Output dataset
+    (runtime_actions/scalar_saver.py:9-206).  Output dataset
     ``scalars[block, save, column]`` float32 with attrs ``scalar_names`` and
     ``steps_between_output`` (scalar_saver.py:172-179)."""
 

@@ -4,8 +4,11 @@ get_default_sim.py).
 Same constructor, timeblock generator, status/summary strings and output
 layout as gamdpy.  Where gamdpy JIT-compiles and launches a numba kernel per
 timeblock (``integrate_self``, Simulation.py:271-282), this calls
-``gdb_sim_run`` once per timeblock: the library runs the steps as a CUDA-graph
-replay of fused force+integrate kernels and returns the block's device time.
+``gdb_sim_run`` once per timeblock: by default the library runs the whole
+timeblock (steps, neighbour-list rebuilds, thermostat) in one persistent
+cooperative kernel, or in one thread-block cluster for small systems; a
+CUDA-graph replay of standalone fused force+integrate kernels is the fallback
+(GDB_PERSISTENT=0).  It returns the block's device time.
 """
 import math
 import sys

@@ -142,8 +142,8 @@ int gdb_get_thermostat_state(gdb_sim *h, float state[2]);
 int gdb_set_thermostat_state(gdb_sim *h, const float state[2]);
 
 /* Runtime actions compiled into the step: ScalarSaver(steps_between_output)
- * (runtime_actions/scalar_saver.py:270-304) and MomentumReset(steps_between_reset)
- * (runtime_actions/momentum_reset.py:400-408); 0 disables. */
+ * (runtime_actions/scalar_saver.py:161-197) and MomentumReset(steps_between_reset)
+ * (runtime_actions/momentum_reset.py:84-103); 0 disables. */
 int gdb_set_runtime_actions(gdb_sim *h, int scalar_every, int momentum_every);
 
 /* ConfigurationSaver (runtime_actions/configuration_saver.py:21-141): keep
@@ -281,12 +281,16 @@ int gdb_batch_get_last_error(gdb_batch *b, char *buf, int n);
  * Inputs and outputs are the caller's DEVICE arrays: r_dev (n, 3) float32,
  * ff_dev (n,) float32 or NULL (all 1), n_vectors_dev (nq, 3) int32 with every
  * component in [-n_max, n_max], rho_re_dev / rho_im_dev (nq,) float64.  box is
- * a host array.  stream is a cudaStream_t (NULL = default stream); the call
- * waits for its work to finish.  Limits: nq <= 65536, n_max <= 48.
- * Scratch is one static device array of 0.5 MiB that every GPU loading the
- * library keeps until exit; it is shared by all calls, so calls that overlap
- * on the GPU race.  The first call on a device looks up the array's address
- * and should come before any stream capture. */
+ * a host array.  stream is a cudaStream_t (NULL = default stream).  Every
+ * call synchronizes `stream` before it returns: it reads back a flag that
+ * reports n-vector components outside [-n_max, n_max].  Limits: nq <= 65536,
+ * n_max <= 48.  Scratch is one static device array of 0.5 MiB that every GPU
+ * loading the library keeps until exit; it is shared by all calls on a
+ * device, so calls that overlap on the GPU (other streams, other host
+ * threads) race and must be serialized by the caller.  The first call on a
+ * device looks up the array's address and should come before any stream
+ * capture; the address is kept for the life of the process, so the device's
+ * primary context must not be reset (cudaDeviceReset) between calls. */
 int gdb_sq_compute_noalloc(int n, const float *r_dev, const float *ff_dev, const float box[3], int nq,
                            const int32_t *n_vectors_dev, int n_max, double *rho_re_dev, double *rho_im_dev,
                            void *stream);

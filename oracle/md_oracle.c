@@ -77,7 +77,7 @@ static void lj_sigma_epsilon(float dist, const float *p, float *u, float *s, flo
     *umm = 24.0f * epsilon * (26.0f * x12 - 7.0f * x6) * o2;
 }
 
-/* LJ_12_6.py:71-78: params (A12, A6, ...). */
+/* LJ_12_6.py:34-41: params (A12, A6, ...). */
 static void lj_12_6(float dist, const float *p, float *u, float *s, float *umm) {
     float A12 = p[0], A6 = p[1];
     float inv = 1.0f / dist;
@@ -437,7 +437,7 @@ void orc_set_langevin(uint64_t *states, float *old_beta, float alpha) {
     g_lv_alpha = alpha;
 }
 
-/* integrators/NVT.py:188-224 (step) and :226-237 (update_thermostat_state).
+/* integrators/NVT.py:75-111 (step) and :226-237 (update_thermostat_state).
  * state[0] = xi (float32), the kinetic-energy sum is returned in float64
  * (the reference accumulates it with float32 atomics into state[1]).
  * Returns sum_i K_i. */
@@ -471,7 +471,7 @@ double orc_nvt_step(int n, float *r, float *v, const float *f, const float *m, i
     return ksum;
 }
 
-/* NVT.py:231-236: ke_deviation = 2*sumK/(degrees*T) - 1 (float64 under
+/* NVT.py:119-123: ke_deviation = 2*sumK/(degrees*T) - 1 (float64 under
  * numba: degrees is an int64), xi += dt*omega2*ke_deviation stored float32. */
 float orc_nvt_thermostat_update(float xi, double ksum, float dt, float omega2, long long degrees, float T) {
     double ke_dev = 2.0 * ksum / ((double)degrees * (double)T) - 1.0;
@@ -479,7 +479,7 @@ float orc_nvt_thermostat_update(float xi, double ksum, float dt, float omega2, l
     return (float)nx;
 }
 
-/* runtime_actions/momentum_reset.py:372-393: v -= (sum m v)/(sum m). */
+/* runtime_actions/momentum_reset.py:57-78: v -= (sum m v)/(sum m). */
 void orc_momentum_reset(int n, float *v, const float *m) {
     double p[3] = {0, 0, 0}, M = 0;
     for (int i = 0; i < n; i++) {
@@ -497,8 +497,8 @@ void orc_momentum_reset(int n, float *v, const float *m) {
  * the kernel-launch form of :306-328): for step in 0..steps:
  *   neighbour-list check (nblist.py:57-86 / nblist_linked_lists.py:84-115)
  *   and rebuild; forces; if step < steps: integrate, then post-step actions
- *   ScalarSaver (scalar_saver.py:270-304) and MomentumReset
- *   (momentum_reset.py:400-408) in that order.
+ *   ScalarSaver (scalar_saver.py:161-197) and MomentumReset
+ *   (momentum_reset.py:84-103) in that order.
  *
  * integrator: 0 = NVE, 1 = NVT, 2 = NVT_Langevin (state from orc_set_langevin).
  * nvt_state[0] = xi (in/out).

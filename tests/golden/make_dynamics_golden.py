@@ -8,6 +8,8 @@ block frames (num_blocks, conf_per_block, 2, N, 3) float32 holding positions
 inside the box and image counts, ptype, attrs dt and simbox_initial.
 
 Run from the repository root:  python tests/golden/make_dynamics_golden.py
+(the reference's source tree is read from /root/reference; GAMDPY_REF
+overrides it).
 """
 import importlib.util
 import os
@@ -16,7 +18,7 @@ import types
 
 import numpy as np
 
-REF = "/root/reference/gamdpy/tools/calc_dynamics.py"
+REF = os.path.join(os.environ.get("GAMDPY_REF", "/root/reference"), "gamdpy", "tools", "calc_dynamics.py")
 
 
 class Trajectory(dict):

@@ -1,5 +1,7 @@
-"""Black-box probe: does numba.cuda (the compiler gamdpy's kernels go through)
-fuse ``dist_sq = dist_sq + dr_k * dr_k`` into a multiply-add on this GPU?
+"""Generator of the fixture numba_contraction.json: does numba.cuda (the
+compiler gamdpy's kernels go through) fuse ``dist_sq = dist_sq + dr_k * dr_k``
+into a multiply-add on this GPU?  The library's default distance form
+(fused accumulation, GDB_NBLIST_FMA=1) rests on the answer recorded there.
 
 gamdpy computes neighbour distances with that accumulation
 (gamdpy/simulation_boxes/orthorhombic.py:59-73) and numba passes no ``fma``
@@ -9,7 +11,7 @@ expression on random inputs and counts how often its results equal the
 unfused and the fused float32 evaluation.  It runs on a GPU machine; the
 result it prints is recorded in numba_contraction.json beside it.
 
-    python tests/golden/probe_numba_contraction.py [out.json]
+    python tests/golden/make_numba_contraction.py [out.json]
 """
 import json
 import sys

@@ -65,3 +65,7 @@ def test_reference_arm_under_torchrun_prints_one_line():
     d = json.loads(lines[0])
     assert d["impl"] == "reference" and d["n_gpus"] == 2 and d["value"] > 0
     assert d["cpu_baseline"]["kind"] == "port" and d["e2e"]["h2d_bytes_per_step"] == 0
+    # the same workload description as the GPU arm's line
+    sys.path.insert(0, ROOT)
+    import bench
+    assert d["config"] == bench.ka_config(4000)

@@ -65,3 +65,55 @@ def test_dynamics_needs_two_blocks():
     traj = Trajectory(d["block"][:2], d["ptype"], float(d["dt"]), d["simbox_initial"])
     with pytest.raises(Exception):
         gp.tools.calc_dynamics(traj, 1, qvalues=7.0)
+
+
+def _random_walk_frames(num_blocks, conf_per_block, n, seed):
+    rng = np.random.default_rng(seed)
+    box = np.array([5.0, 5.5, 6.0], np.float32)
+    steps = num_blocks * conf_per_block
+    walk = np.cumsum(rng.normal(0.0, 0.2, (steps, n, 3)), axis=0) + rng.uniform(-2, 2, (1, n, 3))
+    img = np.floor(walk / box + 0.5)
+    frames = np.zeros((num_blocks, conf_per_block, 2, n, 3), np.float32)
+    frames[:, :, 0] = (walk - img * box).astype(np.float32).reshape(num_blocks, conf_per_block, n, 3)
+    frames[:, :, 1] = img.reshape(num_blocks, conf_per_block, n, 3).astype(np.float32)
+    return frames, box
+
+
+def test_dynamics_more_pairs_than_one_grid_vs_oracle(oracle, monkeypatch):
+    """1025 blocks of 65 frames: 65 600 lags inside blocks, more than the
+    65 535 frame pairs one grid holds, plus the lags across blocks; equal to
+    the oracle, and bit-identical when the pairs go in chunks of 1000 and the
+    frames are staged three blocks at a time."""
+    frames, box = _random_walk_frames(1025, 65, 8, seed=11)
+    ptype = np.array([0, 1, 0, 0, 1, 0, 0, 0], np.int32)
+    traj = Trajectory(frames, ptype, 0.005, box)
+    res = gp.tools.calc_dynamics(traj, 0, qvalues=np.array([6.5, 7.5]))
+    ref = oracle.calc_dynamics(frames, ptype, box, 0.005, 0, qvalues=np.array([6.5, 7.5]))
+    assert np.array_equal(res["count"], ref["count"])
+    for k in ("msd", "Fs"):
+        np.testing.assert_allclose(res[k], ref[k], rtol=1e-6, atol=1e-9)
+    monkeypatch.setenv("GDB_DYN_PAIR_CHUNK", "1000")
+    monkeypatch.setenv("GDB_DYN_STAGE_BYTES", str(3 * 65 * 2 * 8 * 3 * 4))
+    small = gp.tools.calc_dynamics(traj, 0, qvalues=np.array([6.5, 7.5]))
+    for k in ("msd", "alpha2", "Fs"):
+        assert np.array_equal(small[k], res[k])
+
+
+def test_dynamics_type_without_particles_is_nan(oracle):
+    """A type below max(ptype) with no particles gives NaN columns, as the
+    reference's mean of an empty array; longer qvalues are cut to the types."""
+    frames, box = _random_walk_frames(6, 5, 12, seed=4)
+    ptype = np.zeros(12, np.int32)
+    ptype[::3] = 2  # type 1 has no particles
+    traj = Trajectory(frames, ptype, 0.005, box)
+    q = np.array([6.0, 7.0, 8.0, 9.0])
+    res = gp.tools.calc_dynamics(traj, 0, qvalues=q)
+    assert res["msd"].shape == (res["count"].shape[0], 3)
+    assert np.all(np.isnan(res["msd"][:, 1])) and np.all(np.isnan(res["Fs"][:, 1]))
+    with np.errstate(invalid="ignore", divide="ignore"):
+        import warnings
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            ref = oracle.calc_dynamics(frames, ptype, box, 0.005, 0, qvalues=q)
+    for k in ("msd", "Fs"):
+        np.testing.assert_allclose(res[k], ref[k], rtol=1e-6, atol=1e-9, equal_nan=True)
