@@ -56,7 +56,9 @@ def parse():
     p.add_argument("--steps", type=int, default=2000)
     p.add_argument("--warmup", type=int, default=200)
     p.add_argument("--n", "--particles", dest="n", type=int, default=1_048_576)
-    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--impl", default="b200", choices=["b200", "reference", "numba"],
+                   help="reference: the CPU port of the reference on the host cores; numba: gamdpy's own "
+                        "numba.cuda path from baseline/_ref on the same GPU, beside this library")
     p.add_argument("--block", type=int, default=500, help="steps per timeblock")
     p.add_argument("--profile", action="store_true",
                    help="only warm-up and timed steps (for ncu): no e2e, CPU baseline or clock sampling")
@@ -319,6 +321,118 @@ def run_reference_arm(args):
     barrier(pg)
     if pg is not None:
         pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# comparator: gamdpy's own numba.cuda path on the same GPU
+# ---------------------------------------------------------------------------
+GAMDPY_REF_DIR = os.path.join(ROOT, "baseline", "_ref")
+
+
+def _import_gamdpy_stock():
+    """gamdpy, unmodified, from baseline/_ref.  h5py and matplotlib are not
+    in this image: gamdpy imports them at module level
+    (simulation/Simulation.py:20, interactions/pair_potential.py:5) and, with
+    storage='memory', writes its output into an h5py.File; a dict with
+    ``attrs`` stands in for that file and an empty module for matplotlib."""
+    import types
+    h5 = types.ModuleType("h5py")
+
+    class File(dict):
+        def __init__(self, *a, **k):
+            super().__init__()
+            self.attrs = {}
+
+        def create_dataset(self, name, data=None, shape=None, dtype=None, **k):
+            self[name] = np.zeros(shape, dtype=dtype) if data is None else np.array(data, dtype=dtype)
+            return self[name]
+
+        def create_group(self, name):
+            self[name] = File()
+            return self[name]
+
+        def close(self):
+            pass
+
+    h5.File = File
+    sys.modules.setdefault("h5py", h5)
+    mpl = types.ModuleType("matplotlib")
+    mpl.pyplot = types.ModuleType("matplotlib.pyplot")
+    sys.modules.setdefault("matplotlib", mpl)
+    sys.modules.setdefault("matplotlib.pyplot", mpl.pyplot)
+    sys.path.insert(0, GAMDPY_REF_DIR)
+    import warnings
+    warnings.filterwarnings("ignore")
+    from numba import config
+    config.CUDA_LOW_OCCUPANCY_WARNINGS = False
+    import gamdpy
+    return gamdpy
+
+
+def gamdpy_numba_tps(rp, case, n, steps):
+    """TPS of gamdpy's Simulation on one of this bench's systems (the same
+    seeded input), its default compute plan with the workload's list kind
+    and skin, timed as benchmarks/benchmark_LJ.py:66-91: a first run of the
+    timeblock (JIT and warm-up), then a second whose CUDA-event block time
+    gives TPS."""
+    from gamdpy_b200 import workloads
+    if case == "lj2048":
+        src = workloads.lj_configuration([8, 8, 8], 0.973, 0.7, seed=0)
+        params = [1.0, 1.0, 2.5]
+        integ = rp.integrators.NVE(dt=0.005)
+        skin, nblist = 0.5, "N squared"
+    else:
+        src = workloads.ka_configuration(n, seed=1234)
+        params = [workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT]
+        integ = rp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005)
+        skin, nblist = 0.3, "linked lists"
+    conf = rp.Configuration(D=3)
+    conf["r"] = src["r"].copy()
+    conf.simbox = rp.Orthorhombic(3, np.asarray(src.simbox.lengths, np.float32))
+    conf.ptype[:] = src.ptype
+    conf["m"] = 1.0
+    conf["v"] = src["v"].copy()
+    pp = rp.PairPotential(rp.apply_shifted_force_cutoff(rp.LJ_12_6_sigma_epsilon), params=params, max_num_nbs=300)
+    plan = rp.get_default_compute_plan(conf)
+    plan["skin"] = np.float32(skin)
+    plan["nblist"] = nblist
+    sim = rp.Simulation(conf, pp, integ, [rp.MomentumReset(MOMENTUM_RESET_EVERY)], num_timeblocks=1,
+                        steps_per_timeblock=steps, compute_plan=plan, storage="memory", verbose=False)
+    for _ in sim.run_timeblocks():
+        pass
+    for _ in sim.run_timeblocks():
+        pass
+    tps = sim.last_num_blocks * sim.steps_per_block / np.sum(sim.timing_numba_blocks) * 1000
+    return {"case": case, "n": int(conf.N), "steps": steps, "tps": float(tps), "mats": float(tps * conf.N / 1e6),
+            "compute_plan": {k: (v.item() if hasattr(v, "item") else v) for k, v in sim.compute_plan.items()}}
+
+
+def run_numba_comparator(args):
+    """gamdpy's own numba.cuda path on this GPU, beside this library, on the
+    KA workload at N = 2048, 65 536 and --n, and on the LJ 2048 case."""
+    rank, world, local, pg = dist_setup(args)
+    if rank != 0:
+        barrier(pg)
+        return
+    if not os.path.isdir(os.path.join(GAMDPY_REF_DIR, "gamdpy")):
+        print(json.dumps({"impl": "gamdpy-numba-cuda", "unavailable": "gamdpy is not installed in baseline/_ref"}))
+        return
+    rp = _import_gamdpy_stock()
+    cases = [("lj2048", 2048, 10_000), ("ka", 2048, 10_000), ("ka", 65536, 2000), ("ka", args.n, 500)]
+    out = []
+    for case, n, steps in cases:
+        try:
+            g = gamdpy_numba_tps(rp, case, n, steps)
+        except Exception as e:  # record and go on with the other sizes
+            g = {"case": case, "n": n, "error": f"{type(e).__name__}: {e}"[:300]}
+        if "error" not in g:
+            b = measure_lj2048(local, steps, min(steps, 1000), 200) if case == "lj2048" else \
+                measure_ka(local, n, steps, min(steps, 500), 200)
+            g["b200_tps"] = b["tps"]
+            g["ratio_tps"] = b["tps"] / g["tps"]
+        out.append(g)
+        print(json.dumps({"impl": "gamdpy-numba-cuda", **g}), flush=True)
+    barrier(pg)
 
 
 def measure_batch(local, replicas, steps, block, warmup, autotune=False, seed=2024, e2e_blocks=0):
@@ -694,6 +808,9 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference_arm(args)
+        return
+    if args.impl == "numba":
+        run_numba_comparator(args)
         return
     if args.workload == "batch":
         run_batch(args)

@@ -52,6 +52,9 @@ SIGNATURES = {
     "gdb_upload_state": ([_P, _P, _P, _P, _P, _P], _i),
     "gdb_download_state": ([_P, _P, _P, _P, _P], _i),
     "gdb_download_scalars": ([_P, _P, _P, _P, _P, _P], _i),
+    "gdb_download_table": ([_P, _P, _P, _P, _i, _P], _i),
+    "gdb_host_alloc": ([ctypes.c_size_t, _P], _i),
+    "gdb_host_free": ([_P], _i),
     "gdb_set_pair_potential": ([_P, _i, _i, _i, _P, _i], _i),
     "gdb_set_nblist": ([_P, _i, _f, _i], _i),
     "gdb_set_plan": ([_P, _i, _i], _i),
@@ -163,6 +166,31 @@ def i32(a, shape=None):
     return a
 
 
+def pinned_empty(shape, dtype):
+    """A numpy array in page-locked host memory from gdb_host_alloc, freed
+    when the last view of it is gone; None when no GPU is available (the
+    caller then keeps ordinary numpy memory)."""
+    dtype = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dtype.itemsize
+    p = ctypes.c_void_p()
+    try:
+        if lib().gdb_host_alloc(ctypes.c_size_t(max(nbytes, 1)), ctypes.byref(p)) != GDB_OK or not p.value:
+            return None
+    except (RuntimeError, OSError):
+        return None
+    addr = p.value
+
+    def _free(_self, addr=addr):
+        try:
+            lib().gdb_host_free(ctypes.c_void_p(addr))
+        except Exception:
+            pass
+
+    owner_t = type("PinnedBytes", (ctypes.c_char * max(nbytes, 1),), {"__del__": _free})
+    owner = owner_t.from_address(addr)
+    return np.frombuffer(owner, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+
 class Sim:
     """Owner of one gdb_sim handle (device state of one configuration)."""
 
@@ -222,6 +250,26 @@ class Sim:
             if a is not None:
                 assert a.dtype == dt and a.shape == (n, 3) and a.flags.c_contiguous
         self.call("gdb_download_state", ptr(r), ptr(v), ptr(f), ptr(r_im))
+
+    def download_table(self, vectors, r_im, scalars, cols):
+        """Fill a Configuration's own arrays in place in one call: vectors
+        (3, n, 3) float32 r, v, f; r_im (n, 3) int32; scalars (n, nscal)
+        float32 with cols = the columns of U, W, lapU, K, Fsq, m (-1 absent).
+        Any array may be None."""
+        n = self.n
+        if vectors is not None:
+            assert vectors.dtype == np.float32 and vectors.shape == (3, n, 3) and vectors.flags.c_contiguous
+        if r_im is not None:
+            assert r_im.dtype == np.int32 and r_im.shape == (n, 3) and r_im.flags.c_contiguous
+        nscal = 0
+        c = None
+        if scalars is not None:
+            assert scalars.dtype == np.float32 and scalars.ndim == 2 and scalars.shape[0] == n
+            assert scalars.flags.c_contiguous
+            nscal = scalars.shape[1]
+            c = np.ascontiguousarray(cols, np.int32)
+            assert c.shape == (6,)
+        self.call("gdb_download_table", ptr(vectors), ptr(r_im), ptr(scalars), int(nscal), ptr(c))
 
     # --- configuration of the step ------------------------------------
     def set_pair_potential(self, kind, cutmode, table):

@@ -181,6 +181,27 @@ class Configuration:
         raise ValueError(f"Unknown key {key}. Vectors: {self.vector_columns}, Scalars: {self.scalar_columns}")
 
     # --- host <-> device (Configuration.py:227-243) ----------------------
+    def _attach(self, device):
+        """Attach to a simulation handle.  The vectors, scalars and image
+        arrays move into page-locked host memory (contents kept), so the
+        copies to and from the device run at DMA speed; as in gamdpy, whose
+        copy_to_host replaces these arrays (Configuration.py:236-243), views
+        taken before this point no longer follow the configuration."""
+        from . import _lib
+        self._device = device
+        for name, arr in (("vectors", self.vectors.array), ("scalars", self.scalars), ("r_im", self.r_im)):
+            if getattr(self, "_pinned_" + name, None) is arr:
+                continue
+            pinned = _lib.pinned_empty(arr.shape, arr.dtype)
+            if pinned is None:
+                return
+            pinned[...] = arr
+            if name == "vectors":
+                self.vectors.array = pinned
+            else:
+                setattr(self, name, pinned)
+            setattr(self, "_pinned_" + name, pinned)
+
     def copy_to_device(self):
         """Upload the full state to the attached simulation handle."""
         if self._device is None:
@@ -192,7 +213,14 @@ class Configuration:
         """Download r, v, f, images and the per-particle scalars."""
         if self._device is None:
             return
-        # straight into this configuration's arrays (and a kept scalar buffer)
+        va, sc, im = self.vectors.array, self.scalars, self.r_im
+        if (va.dtype == np.float32 and va.shape == (3, self.N, 3) and va.flags.c_contiguous and
+                self.vector_columns == ["r", "v", "f"] and sc.dtype == np.float32 and sc.flags.c_contiguous and
+                im.dtype == np.int32 and im.flags.c_contiguous and im.shape == (self.N, 3)):
+            # one call straight into this configuration's arrays
+            cols = [self.sid.get(k, -1) for k in ("U", "W", "lapU", "K", "Fsq", "m")]
+            self._device.download_table(va, im, sc, cols)
+            return
         vec = {k: self.vectors[k] for k in ("r", "v", "f")}
         im = self.r_im
         if all(a.dtype == np.float32 and a.flags.c_contiguous for a in vec.values()) and \

@@ -256,6 +256,38 @@ __global__ void k_unpack1(int n, const float *src, const int *orig, float *dst) 
     dst[orig[s]] = src[s];
 }
 
+// download of the whole state in gamdpy's host layouts, one pass: slot s ->
+// user index i = orig[s]; vec (3, n, 3) r, v, f; im (n, 3); sc (n, nscal) with
+// column cols[q] for U, W, lapU, K, Fsq and the mass (q = 0..5, -1 = absent)
+struct UnpackCols {
+    int c[6];
+};
+__global__ void k_unpack_all(int n, const float4 *pos, const float4 *vel, const float4 *frc, const int4 *img,
+                             const float *pscal, const int *orig, float *vec, int *im, float *sc, int nscal,
+                             UnpackCols cols) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const size_t i = (size_t)orig[s], N = (size_t)n;
+    if (vec) {
+        const float4 p = pos[s], v = vel[s], f = frc[s];
+        float *r = vec + 3 * i, *vv = vec + 3 * (N + i), *ff = vec + 3 * (2 * N + i);
+        r[0] = p.x, r[1] = p.y, r[2] = p.z;
+        vv[0] = v.x, vv[1] = v.y, vv[2] = v.z;
+        ff[0] = f.x, ff[1] = f.y, ff[2] = f.z;
+    }
+    if (im) {
+        const int4 g = img[s];
+        im[3 * i] = g.x, im[3 * i + 1] = g.y, im[3 * i + 2] = g.z;
+    }
+    if (sc) {
+        float *row = sc + i * nscal;
+#pragma unroll
+        for (int q = 0; q < 5; q++)
+            if (cols.c[q] >= 0) row[cols.c[q]] = pscal[q * N + s];
+        if (cols.c[5] >= 0) row[cols.c[5]] = vel[s].w;
+    }
+}
+
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
@@ -848,6 +880,50 @@ int gdb_download_state(gdb_sim *h, float *r, float *v, float *f, int32_t *r_im) 
     if (f && (rc = download_planes(h, h->frc, 0, f))) return rc;
     if (r_im && (rc = download_planes(h, h->img, 1, r_im))) return rc;
     CK(cudaStreamSynchronize(h->st));
+    return GDB_OK;
+}
+
+int gdb_download_table(gdb_sim *h, float *vectors, int32_t *r_im, float *scalars, int nscal, const int32_t cols[6]) {
+    if (!h) return set_err(h, GDB_ERR_ARG, "NULL handle");
+    if (!h->uploaded) return set_err(h, GDB_ERR_STATE, "state not uploaded");
+    if (scalars && (nscal < 1 || !cols)) return set_err(h, GDB_ERR_ARG, "gdb_download_table: bad scalar table");
+    UnpackCols uc;
+    for (int q = 0; q < 6; q++) {
+        uc.c[q] = scalars ? cols[q] : -1;
+        if (uc.c[q] >= nscal) return set_err(h, GDB_ERR_ARG, "gdb_download_table: column %d outside the table", uc.c[q]);
+    }
+    CK(cudaSetDevice(h->dev));
+    const size_t N = h->n;
+    const size_t bv = vectors ? 9 * N * sizeof(float) : 0, bi = r_im ? 3 * N * sizeof(int) : 0,
+                 bs = scalars ? N * nscal * sizeof(float) : 0;
+    if (bv + bi + bs == 0) return GDB_OK;
+    char *stage = nullptr;
+    CK(pool_alloc(&stage, bv + bi + bs, h->st));
+    float *dv = vectors ? (float *)stage : nullptr;
+    int *di = r_im ? (int *)(stage + bv) : nullptr;
+    float *ds = scalars ? (float *)(stage + bv + bi) : nullptr;
+    k_unpack_all<<<grid_for(h->n), GDB_BLOCK, 0, h->st>>>(h->n, h->pos[h->cur], h->vel, h->frc, h->img, h->pscal,
+                                                        h->orig, dv, di, ds, nscal, uc);
+    CKL();
+    if (vectors) CK(cudaMemcpyAsync(vectors, dv, bv, cudaMemcpyDeviceToHost, h->st));
+    if (r_im) CK(cudaMemcpyAsync(r_im, di, bi, cudaMemcpyDeviceToHost, h->st));
+    if (scalars) CK(cudaMemcpyAsync(scalars, ds, bs, cudaMemcpyDeviceToHost, h->st));
+    CK(cudaFreeAsync(stage, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    return GDB_OK;
+}
+
+int gdb_host_alloc(size_t bytes, void **out) {
+    gdb_sim *h = nullptr;
+    if (!out) return set_err(h, GDB_ERR_ARG, "gdb_host_alloc: NULL argument");
+    *out = nullptr;
+    CK(cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocPortable));
+    return GDB_OK;
+}
+
+int gdb_host_free(void *p) {
+    gdb_sim *h = nullptr;
+    if (p) CK(cudaFreeHost(p));
     return GDB_OK;
 }
 

@@ -816,118 +816,53 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
     }
 }
 
-// Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
-// only (MODE_EVAL).  A round is blockDim/TP consecutive particles.
-// Standalone launches (PERSIST false) take rounds g.b, g.b + g.nb, ... and
-// write one float64 partial row per block to partials[g.b].  The persistent
-// kernels (PERSIST true) hand rounds out through an atomic counter (blocks on
-// faster SMs take more) and write one row per round to partials[round], so
-// the fixed-order sum does not depend on which block ran which round.  Only
-// the sums the step needs are reduced: all of them on saved and reset steps,
-// the kinetic energy (NVT) otherwise.  Sets the rebuild flag when a particle
-// has moved more than skin/2 since the build.
-template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
-__device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
-                                  Span g = grid_span()) {
+// Everything a step does for particle i once its force is summed (shared by
+// the row and brick force phases): ConfigurationSaver frame, pending
+// momentum shift, per-particle scalars, the integrator update
+// (MODE_STEP) or the force store (MODE_EVAL), periodic wrap with images, the
+// skin check for the next step and this particle's share of the block sums.
+template <int INTEG, int MODE>
+__device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 pi, float4 v, float4 rr, float fx,
+                                                float fy, float fz, float u, float w, float l, bool rec, bool reset,
+                                                int step, bool shift_pending, float shx, float shy, float shz,
+                                                float xi, float4 *pos_next, double (&red)[NQ], bool &moved) {
     DevCtrl *ctrl = a.ctrl;
-    const float4 *pos = cur_pos(a, cur);
-    float4 *pos_next = cur_pos(a, cur ^ 1);
-    const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
-    const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
-    const int ppar = (step & 1) ^ 1;
-    const bool shift_pending = ctrl->pending[ppar] != 0;
-    float shx = 0.f, shy = 0.f, shz = 0.f;
-    if (shift_pending) {
-        shx = ctrl->shift[ppar][0];
-        shy = ctrl->shift[ppar][1];
-        shz = ctrl->shift[ppar][2];
-    }
-    const float xi = ctrl->xi;
     const size_t n = a.n;
-    const int per_block = blockDim.x / TP;
-    const int rounds_total = (a.n + per_block - 1) / per_block;
-    const bool full = rec || reset;
-    const bool needk = full || INTEG == GDB_INTEGRATOR_NVT;
-    double red[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) red[q] = 0.0;
-    bool moved = false;
-    __shared__ int s_round;
-    int round = g.b;
-    if (PERSIST) {
-        if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
-        __syncthreads();
-        round = s_round;
+    // ConfigurationSaver: frame taken before this step's integration
+    if (a.conf) {
+        const int si = conf_save_index(step);
+        if (si >= 0 && si < a.conf_per_block) {
+            const int4 im = a.img[i];
+            const size_t uidx = (size_t)a.orig[i];
+            float *fr = a.conf + (size_t)si * 2 * n * 3;
+            fr[3 * uidx] = pi.x;
+            fr[3 * uidx + 1] = pi.y;
+            fr[3 * uidx + 2] = pi.z;
+            fr += n * 3;
+            fr[3 * uidx] = (float)im.x;
+            fr[3 * uidx + 1] = (float)im.y;
+            fr[3 * uidx + 2] = (float)im.z;
+        }
     }
-    while (round < rounds_total) {
-        const int i = round * per_block + threadIdx.x / TP;
-        const int sub = threadIdx.x % TP;
-        const bool active = i < a.n;
-        float fx = 0.f, fy = 0.f, fz = 0.f, u = 0.f, w = 0.f, l = 0.f;
-        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
-        // the integrating lane's own state, loaded before the neighbour loop so
-        // its latency overlaps the gathers
-        float4 v = make_float4(0.f, 0.f, 0.f, 1.f), rr = v;
-        if (active && sub == 0) {
-            v = a.vel[i];
-            if (MODE == MODE_STEP) rr = a.rref[i];
-        }
-        if (active) {
-            pi = pos[i];
-            if (rec)
-                neighbour_loop<TP, NT, true, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
-            else
-                neighbour_loop<TP, NT, false, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
-        }
-        if (TP > 1) {
-#pragma unroll
-            for (int o = TP / 2; o > 0; o >>= 1) {
-                fx += __shfl_xor_sync(0xffffffffu, fx, o);
-                fy += __shfl_xor_sync(0xffffffffu, fy, o);
-                fz += __shfl_xor_sync(0xffffffffu, fz, o);
-                if (rec) {
-                    u += __shfl_xor_sync(0xffffffffu, u, o);
-                    w += __shfl_xor_sync(0xffffffffu, w, o);
-                    l += __shfl_xor_sync(0xffffffffu, l, o);
-                }
-            }
-        }
-        if (active && sub == 0) {
-        // ConfigurationSaver: frame taken before this step's integration
-        if (a.conf) {
-            const int si = conf_save_index(step);
-            if (si >= 0 && si < a.conf_per_block) {
-                const int4 im = a.img[i];
-                const size_t uidx = (size_t)a.orig[i];
-                float *fr = a.conf + (size_t)si * 2 * n * 3;
-                fr[3 * uidx] = pi.x;
-                fr[3 * uidx + 1] = pi.y;
-                fr[3 * uidx + 2] = pi.z;
-                fr += n * 3;
-                fr[3 * uidx] = (float)im.x;
-                fr[3 * uidx + 1] = (float)im.y;
-                fr[3 * uidx + 2] = (float)im.z;
-            }
-        }
-        if (shift_pending) {
-            v.x -= shx;
-            v.y -= shy;
-            v.z -= shz;
-        }
-        const float fsq = fx * fx + fy * fy + fz * fz;
-        if (rec) {
-            a.pscal[i] = u;
-            a.pscal[n + i] = w;
-            a.pscal[2 * n + i] = l;
-        }
-        red[1] += u;
-        red[2] += w;
-        red[3] += l;
-        red[4] += fsq;
-        if (MODE == MODE_EVAL) {
-            a.frc[i] = make_float4(fx, fy, fz, 0.f);
-            if (shift_pending) a.vel[i] = v;
-        } else {
+    if (shift_pending) {
+        v.x -= shx;
+        v.y -= shy;
+        v.z -= shz;
+    }
+    const float fsq = fx * fx + fy * fy + fz * fz;
+    if (rec) {
+        a.pscal[i] = u;
+        a.pscal[n + i] = w;
+        a.pscal[2 * n + i] = l;
+    }
+    red[1] += u;
+    red[2] += w;
+    red[3] += l;
+    red[4] += fsq;
+    if (MODE == MODE_EVAL) {
+        a.frc[i] = make_float4(fx, fy, fz, 0.f);
+        if (shift_pending) a.vel[i] = v;
+    } else {
         const float m = v.w;
         float kin = 0.f;
         float r[3] = {pi.x, pi.y, pi.z};
@@ -1015,8 +950,88 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
             red[7] += (double)m * vv[2];
             red[8] += m;
         }
-        }  // MODE_STEP
-        }  // integrating lane
+    }  // MODE_STEP
+}
+
+// Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
+// only (MODE_EVAL).  A round is blockDim/TP consecutive particles.
+// Standalone launches (PERSIST false) take rounds g.b, g.b + g.nb, ... and
+// write one float64 partial row per block to partials[g.b].  The persistent
+// kernels (PERSIST true) hand rounds out through an atomic counter (blocks on
+// faster SMs take more) and write one row per round to partials[round], so
+// the fixed-order sum does not depend on which block ran which round.  Only
+// the sums the step needs are reduced: all of them on saved and reset steps,
+// the kinetic energy (NVT) otherwise.  Sets the rebuild flag when a particle
+// has moved more than skin/2 since the build.
+template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
+__device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
+                                  Span g = grid_span()) {
+    DevCtrl *ctrl = a.ctrl;
+    const float4 *pos = cur_pos(a, cur);
+    float4 *pos_next = cur_pos(a, cur ^ 1);
+    const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
+    const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
+    const int ppar = (step & 1) ^ 1;
+    const bool shift_pending = ctrl->pending[ppar] != 0;
+    float shx = 0.f, shy = 0.f, shz = 0.f;
+    if (shift_pending) {
+        shx = ctrl->shift[ppar][0];
+        shy = ctrl->shift[ppar][1];
+        shz = ctrl->shift[ppar][2];
+    }
+    const float xi = ctrl->xi;
+    const size_t n = a.n;
+    const int per_block = blockDim.x / TP;
+    const int rounds_total = (a.n + per_block - 1) / per_block;
+    const bool full = rec || reset;
+    const bool needk = full || INTEG == GDB_INTEGRATOR_NVT;
+    double red[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) red[q] = 0.0;
+    bool moved = false;
+    __shared__ int s_round;
+    int round = g.b;
+    if (PERSIST) {
+        if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
+        __syncthreads();
+        round = s_round;
+    }
+    while (round < rounds_total) {
+        const int i = round * per_block + threadIdx.x / TP;
+        const int sub = threadIdx.x % TP;
+        const bool active = i < a.n;
+        float fx = 0.f, fy = 0.f, fz = 0.f, u = 0.f, w = 0.f, l = 0.f;
+        float4 pi = make_float4(0.f, 0.f, 0.f, 0.f);
+        // the integrating lane's own state, loaded before the neighbour loop so
+        // its latency overlaps the gathers
+        float4 v = make_float4(0.f, 0.f, 0.f, 1.f), rr = v;
+        if (active && sub == 0) {
+            v = a.vel[i];
+            if (MODE == MODE_STEP) rr = a.rref[i];
+        }
+        if (active) {
+            pi = pos[i];
+            if (rec)
+                neighbour_loop<TP, NT, true, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
+            else
+                neighbour_loop<TP, NT, false, NC>(a, pos, tab, nt, i, sub, pi, fx, fy, fz, u, w, l);
+        }
+        if (TP > 1) {
+#pragma unroll
+            for (int o = TP / 2; o > 0; o >>= 1) {
+                fx += __shfl_xor_sync(0xffffffffu, fx, o);
+                fy += __shfl_xor_sync(0xffffffffu, fy, o);
+                fz += __shfl_xor_sync(0xffffffffu, fz, o);
+                if (rec) {
+                    u += __shfl_xor_sync(0xffffffffu, u, o);
+                    w += __shfl_xor_sync(0xffffffffu, w, o);
+                    l += __shfl_xor_sync(0xffffffffu, l, o);
+                }
+            }
+        }
+        if (active && sub == 0)
+            finish_particle<INTEG, MODE>(a, i, pi, v, rr, fx, fy, fz, u, w, l, rec, reset, step, shift_pending, shx,
+                                         shy, shz, xi, pos_next, red, moved);
         if (PERSIST) {
             // this round's sums to partials[round]; the next round
             if (full) {

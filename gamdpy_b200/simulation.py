@@ -154,7 +154,7 @@ class Simulation:
         pp = self.interactions[0]
         table, _ = pp.table()
         self._sim = _lib.Sim(conf.N, table.shape[0], device)
-        conf._device = self._sim
+        conf._attach(self._sim)
         self._sim.set_box(conf.simbox.lengths)
         pp.configure_device(self._sim, conf, self.compute_plan)
         # gamdpy's tp heuristic targets its own launch shape; the library picks

@@ -103,6 +103,25 @@ int gdb_download_state(gdb_sim *h, float *r, float *v, float *f, int32_t *r_im);
  * gamdpy's columns (Configuration.py:109-131).  Any pointer may be NULL. */
 int gdb_download_scalars(gdb_sim *h, float *U, float *W, float *lapU, float *K, float *Fsq);
 
+/* The whole state in one call, in the host arrays of gamdpy's Configuration
+ * (Configuration.copy_to_host, configuration/Configuration.py:236-243):
+ * vectors is the (3, n, 3) float32 r, v, f column array (colarray.py:45),
+ * r_im (n, 3) int32, scalars the (n, nscal) float32 table whose columns
+ * cols[0..5] hold U, W, lapU, K, Fsq and the mass (-1 = column absent;
+ * Configuration.py:109-131).  One kernel unpacks every plane into device
+ * staging laid out as those arrays, then one copy per array; from pinned
+ * host memory (gdb_host_alloc) the copies run at DMA speed.  Any array may
+ * be NULL.  Synchronises the handle's stream. */
+int gdb_download_table(gdb_sim *h, float *vectors, int32_t *r_im, float *scalars, int nscal, const int32_t cols[6]);
+
+/* Page-locked host memory (cudaHostAlloc, portable across devices) for the
+ * host arrays of a Configuration attached to a device, so uploads and
+ * downloads copy without staging through pageable pages.  No counterpart in
+ * the reference, whose host arrays are numpy's (numba copies through its own
+ * staging).  gdb_host_free releases it. */
+int gdb_host_alloc(size_t bytes, void **out);
+int gdb_host_free(void *p);
+
 /* Pair potential table (PairPotential.convert_user_params,
  * interactions/pair_potential.py:23-51): params is ntypes*ntypes rows of
  * nparams float32 (row-major [i][j][p]); the last parameter is the cut. */

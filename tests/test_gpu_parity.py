@@ -347,6 +347,40 @@ def test_sq_vs_gamdpy_and_oracle(oracle):
     assert np.abs(raw["rho_q"][0] - d["ff_rho_q"]).max() < 2e-3 * max(1.0, np.abs(d["ff_rho_q"]).max())
 
 
+def test_rdf_and_sq_at_the_large_lj_geometry(oracle):
+    """The structure analysis of the large LJ workload (rho 0.84, r < 5 with
+    1000 bins, S(q) on the first 200 |n|^2 shells of the reference's
+    non-negative generator) on a box of its kind: 186 624 particles (FCC
+    36^3, +-0.1 jitter, 20 NVE steps) in L = 60.6, a grid of 12^3 cells of
+    edge >= 5 of which 1000 lie off the box faces (the plain-difference
+    shortcut).  Through the device-resident path of a running Simulation
+    (particles in cell order): counts bit-exact against the oracle's all
+    pairs; S(q) within 1e-4 of the float64 oracle."""
+    conf = workloads.lj_configuration([36, 36, 36], 0.84, 1.0, seed=5)
+    L = conf.simbox.lengths.astype(np.float32)
+    rng = np.random.default_rng(8)
+    r = conf["r"].astype(np.float64) + rng.uniform(-0.1, 0.1, (conf.N, 3))
+    r -= L * np.round(r / L)
+    conf["r"] = r.astype(np.float32)
+    plan = {"pb": 256, "tp": 1, "lanes": 0, "skin": 0.5, "UtilizeNIII": False, "gridsync": False,
+            "nblist": "linked lists"}
+    sim = gp.Simulation(conf, workloads.lj_pair_potential(max_num_nbs=200), gp.integrators.NVE(dt=0.004), [],
+                        num_timeblocks=1, steps_per_timeblock=20, compute_plan=plan, storage="memory")
+    for _ in sim.run_timeblocks():
+        pass
+    rdf = gp.CalculatorRadialDistribution(conf, bins=1000, r_max=5.0)
+    rdf.update()
+    got = rdf.rdf_list[-1]
+    ref = oracle.rdf(conf["r"], conf.ptype, L, 1000, fma=1, r_max=5.0)
+    assert ref.sum() > 3e8 and np.array_equal(got, ref.astype(np.float64))
+    sq = gp.CalculatorStructureFactor(conf)
+    sq.generate_q_vectors(2 * np.pi * np.sqrt(237.5) / float(L[0]))
+    assert len(sq.q_vectors) == 2219
+    sq.update()
+    ref64 = oracle.sq(conf["r"], sq.q_vectors)
+    assert np.abs(sq.list_of_rho_q[-1] - ref64).max() < 1e-4 * max(1.0, np.abs(ref64).max())
+
+
 def test_sq_negative_and_large_n_vectors(oracle):
     conf = workloads.ka_configuration(5000, seed=2)
     L = conf.simbox.lengths
