@@ -35,6 +35,7 @@ sys.path.insert(0, ROOT)
 METRIC = "MATS (million atom-timesteps/s), KA-LJ NVT cell lists, 1 B200"
 UNIT = "Matom-steps/s"
 MOMENTUM_RESET_EVERY = 100  # the only runtime action, as benchmarks/benchmark_LJ.py:28-47
+PATH_NAMES = {0: "graph", 1: "persistent", 2: "cluster", 3: "cluster-global", 4: "persistent-staged-halos"}
 
 
 def ka_workload(n, langevin=False):
@@ -279,8 +280,7 @@ def run_sweep(args):
         bpa = 4.0 * mean_nbs + 64.0
         achieved = bpa * n * steps / t_max / 1e9
         line = {"sweep": True, "n": n, "mats": n * steps * world / t_max / 1e6, "tps": steps / t_max,
-                "steps": steps, "ms_per_step": t_max * 1e3 / steps, "path": ["graph", "persistent", "cluster"][
-                    dev.last_path()] if 0 <= dev.last_path() <= 2 else dev.last_path(),
+                "steps": steps, "ms_per_step": t_max * 1e3 / steps, "path": PATH_NAMES.get(dev.last_path(), dev.last_path()),
                 "hbm_frac": achieved / peak, "hbm_peak": peak, "peak_source": peak_kind,
                 "algorithmic_bytes_per_atom_step": bpa, "n_gpus": world}
         if rank == 0 and world == 1:
@@ -603,7 +603,7 @@ def measure_ka(local, n, steps, block, warmup, seed=1234, tp=0):
     path = dev.last_path()
     return {"workload": ka_workload(n), "n": n, "steps": steps, "timeblock_steps": block, "ms": ms,
             "tps": steps / ms * 1e3, "mats": n * steps / ms / 1e3, "ms_per_step": ms / steps,
-            "path": ["graph", "persistent", "cluster"][path] if 0 <= path <= 2 else path, "clocks": clock_info}
+            "path": PATH_NAMES.get(path, path), "clocks": clock_info}
 
 
 def run_lj_small(args):
@@ -919,7 +919,8 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded KA lattice)",
         "config": ka_config(n, args.langevin),
         "measured": {"tps": tps, "timeblock_steps": block, "parallelism": f"replicas x{world}",
-                     "mean_neighbours": mean_nbs, "max_neighbours": max_nbs, "path": dev.last_path()},
+                     "mean_neighbours": mean_nbs, "max_neighbours": max_nbs,
+                     "path": PATH_NAMES.get(dev.last_path(), dev.last_path())},
         "e2e": e2e,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_source": peak_kind,

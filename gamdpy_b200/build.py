@@ -29,7 +29,7 @@ def _stale(target, deps):
 
 def build(verbose=False, force=False):
     deps = [os.path.join(CSRC, s) for s in SOURCES] + [
-        os.path.join(CSRC, h) for h in ("gdb_internal.cuh", "md_phases.cuh", "md_kernels.cuh", "md_cluster.cuh")
+        os.path.join(CSRC, h) for h in ("gdb_internal.cuh", "md_phases.cuh", "md_kernels.cuh", "md_cluster.cuh", "md_bricks.cuh")
     ] + [os.path.join(HERE, "..", "include", "gamdb200.h")]
     if not force and not _stale(LIB, deps):
         return LIB

@@ -58,6 +58,10 @@ char g_lib_error[512] = "";
 // 23.2k).  GDB_NSQ_AUTO=<N> moves the limit, 0 switches it off.
 constexpr int NSQ_AUTO_MAX = 3072;
 
+// Systems from this many particles take the brick path on the persistent
+// kernel (GDB_BRICK_MIN_N moves it; GDB_BRICKS=0 switches the path off).
+constexpr int BRICK_MIN_N = 131073;
+
 struct gdb_sim {
     int n = 0, ntypes = 1, dev = 0;
     cudaStream_t st = nullptr;
@@ -111,6 +115,17 @@ struct gdb_sim {
     bool cluster_ok = true;  // small systems run resident in one thread-block cluster
     bool cluster_force = false;  // GDB_CLUSTER=1: the cluster path whenever it fits
     int nsq_auto_max = NSQ_AUTO_MAX;  // persistent kernel: N^2 build up to this N (GDB_NSQ_AUTO)
+    // the staged-halo path of large cell-list systems on the persistent
+    // kernel (md_bricks.cuh): cells numbered in bricks of 4 x 4 x 4 cells,
+    // each brick's halo staged in shared memory.  Off by default (measured
+    // slower than the row path on B200); GDB_BRICKS=1 (or 2) switches it on.
+    bool bricks_req = false;  // GDB_BRICKS
+    bool staged_ok = true;    // cleared when a halo outgrew its stage
+    bool bricks_ok = true;    // cleared for batches' cluster systems (they run the row phases)
+    int order = 0;            // 0: row order; 2: the staged-halo path's brick order
+    int nb[3] = {0, 0, 0};    // bricks per dimension
+    int brick_min_n = BRICK_MIN_N;  // GDB_BRICK_MIN_N
+    int brick_hcap = BRICK_HCAP;    // GDB_BRICK_HCAP lowers the stage the kernels may fill (tests of the fallback)
     int last_path = -1;      // 0 graph, 1 persistent grid, 2 cluster
     int grid_cap = 0;        // upper bound on the persistent grid (0: the whole GPU)
     ClusterJob *d_job = nullptr, *h_job = nullptr;
@@ -218,6 +233,18 @@ __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
         ctrl->rebuild = 1;
         ctrl->rebuild_next = 0;
     }
+}
+
+// Continue an abandoned timeblock: clear the abort and barrier state and keep
+// the step counter and the block's start time.
+__global__ void k_block_resume(DevCtrl *ctrl) {
+    ctrl->bar_count = 0;
+    for (int g = 0; g < 64; g++) ctrl->bar_group[g] = 0;
+    ctrl->abort = 0;
+    ctrl->ticket = 0;
+    ctrl->work[0] = ctrl->work[1] = 0;
+    ctrl->rebuild = 1;
+    ctrl->rebuild_next = 0;
 }
 
 // upload helpers: gamdpy layout -> float4 / int4
@@ -387,7 +414,26 @@ static int ensure_nblist(gdb_sim *h) {
             nc[k] = (int)(h->box[k] / min_cell);
             if (nc[k] < 1) nc[k] = 1;
         }
-        const int ncell = nc[0] * nc[1] * nc[2];
+        // the brick path: a persistent large system whose grid holds the
+        // 8-cell halo of a brick in every dimension and whose expected halo
+        // fits the stage with a quarter to spare
+        const double per_cell = (double)h->n / ((double)nc[0] * nc[1] * nc[2]);
+        const bool use = h->bricks_req && h->bricks_ok && h->staged_ok && h->persistent &&
+                         h->n >= h->brick_min_n && h->n > h->nsq_auto_max && nc[0] >= BRICK_W &&
+                         nc[1] >= BRICK_W && nc[2] >= BRICK_W &&
+                         per_cell * BRICK_W * BRICK_W * BRICK_W * 1.25 <= BRICK_HCAP;
+        const int order = use ? 2 : 0;
+        const bool want = order != 0;
+        if (order != h->order) {
+            h->order = order;
+            free_graphs(h);
+            if (h->uploaded) {
+                int one = 1;
+                CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
+            }
+        }
+        for (int k = 0; k < 3; k++) h->nb[k] = want ? (nc[k] + BRICK - 1) / BRICK : 0;
+        const int ncell = want ? h->nb[0] * h->nb[1] * h->nb[2] * BRICK * BRICK * BRICK : nc[0] * nc[1] * nc[2];
         if (ncell > h->cell_cap) {
             if (h->cell_count) cudaFree(h->cell_count);
             if (h->cell_start) cudaFree(h->cell_start);
@@ -454,6 +500,11 @@ static SimArgs make_args(gdb_sim *h) {
     a.ncx = h->nc[0];
     a.ncy = h->nc[1];
     a.ncz = h->nc[2];
+    const int order = h->nb_kind == GDB_NBLIST_CELLS ? h->order : 0;
+    a.nbx = order ? h->nb[0] : 0;
+    a.nby = order ? h->nb[1] : 0;
+    a.nbz = order ? h->nb[2] : 0;
+    a.brick_hcap = h->brick_hcap;
     a.nb_kind = h->nb_kind;
     a.fma = h->fma;
     a.Lx = h->box[0];
@@ -542,7 +593,30 @@ static int run_grid(gdb_sim *h, const void *fn, int *grid) {
 }
 
 // One launch of k_run: `steps` steps from pos[cur], then the final evaluation.
+static int launch_run_bricks(gdb_sim *h, int steps, int do_eval) {
+    const void *fn = h->ntypes == 1   ? run_bricks_kernel_nt1(h->integ)
+                     : h->ntypes == 2 ? run_bricks_kernel_nt2(h->integ)
+                                      : run_bricks_kernel_ntg(h->integ);
+    const size_t smem = sizeof(BrickSmem);
+    CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BRICK_THREADS, smem));
+    if (occ < 1) return set_err(h, GDB_ERR_CUDA, "brick kernel cannot be resident");
+    const int nbricks = h->nb[0] * h->nb[1] * h->nb[2];
+    int grid = std::min(std::min(nbricks, occ * h->num_sms), 64 * BAR_GROUP);
+    if (h->grid_cap > 0) grid = std::min(grid, h->grid_cap);
+    int rc;
+    if ((rc = ensure_partials(h, nbricks))) return rc;
+    SimArgs a = make_args(h);
+    int cur0 = h->cur, ns = steps, ev = do_eval;
+    void *args[] = {(void *)&a, (void *)&h->table, (void *)&cur0, (void *)&ns, (void *)&ev};
+    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(BRICK_THREADS), args, smem, h->st));
+    h->cur ^= (steps & 1);
+    return GDB_OK;
+}
+
 static int launch_run(gdb_sim *h, int steps, int do_eval) {
+    if (h->order == 2 && h->nb_kind == GDB_NBLIST_CELLS) return launch_run_bricks(h, steps, do_eval);
     const void *fn = h->ntypes == 1   ? run_kernel_nt1(h->tp, h->integ)
                      : h->ntypes == 2 ? run_kernel_nt2(h->tp, h->integ)
                                       : run_kernel_ntg(h->tp, h->integ);
@@ -556,6 +630,7 @@ static int launch_run(gdb_sim *h, int steps, int do_eval) {
         a.nb_kind = GDB_NBLIST_NSQ;
         a.ncell = 0;
         a.nchunks = 0;
+        a.nbx = a.nby = a.nbz = 0;
     }
     int cur0 = h->cur, ns = steps, ev = do_eval;
     void *args[] = {(void *)&a, (void *)&h->table, (void *)&cur0, (void *)&ns, (void *)&ev};
@@ -737,6 +812,12 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (cs && cs[0] == '1') h->cluster_force = true;
     const char *na = getenv("GDB_NSQ_AUTO");
     if (na) h->nsq_auto_max = atoi(na);
+    const char *bk = getenv("GDB_BRICKS");
+    if (bk && (bk[0] == '1' || bk[0] == '2')) h->bricks_req = true;
+    const char *bm = getenv("GDB_BRICK_MIN_N");
+    if (bm) h->brick_min_n = atoi(bm);
+    const char *bh = getenv("GDB_BRICK_HCAP");
+    if (bh) h->brick_hcap = std::max(1, std::min(atoi(bh), BRICK_HCAP));
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);
     int coop = 0;
     cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device);
@@ -1149,6 +1230,14 @@ int gdb_eval_forces(gdb_sim *h) {
     int rc = check_ready(h);
     if (rc) return rc;
     CK(cudaMemsetAsync(&h->ctrl->maxcount, 0, sizeof(int), h->st));
+    if (h->order == 2 && h->nb_kind == GDB_NBLIST_CELLS) {
+        // the staged-halo path's evaluation: the persistent kernel with no steps
+        k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, 0.0);
+        CKL();
+        if ((rc = launch_run(h, 0, 1))) return rc;
+        if ((rc = read_ctrl(h))) return rc;
+        return status_to_rc(h);
+    }
     if ((rc = enqueue_rebuild(h))) return rc;
     if ((rc = enqueue_step(h, MODE_EVAL))) return rc;
     if ((rc = read_ctrl(h))) return rc;
@@ -1220,8 +1309,29 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
         }
     }
     if (h->persistent) {
+        const int cur0 = h->cur;
+        const bool bricks = h->order == 2 && h->nb_kind == GDB_NBLIST_CELLS;
         if ((rc = launch_run(h, steps, 1))) return rc;
-        h->last_path = 1;
+        h->last_path = bricks ? 4 : 1;
+        if (bricks) {
+            if ((rc = read_ctrl(h))) return rc;
+            if (h->h_ctrl->status & GDB_STATUS_BRICK_CAPACITY) {
+                // a brick's halo outgrew shared memory at a rebuild, before
+                // any step used that list: go on without bricks from the step
+                // reached, in the same timeblock
+                const int done = h->h_ctrl->step;
+                h->cur = cur0 ^ (done & 1);
+                h->staged_ok = false;
+                if ((rc = ensure_nblist(h))) return rc;
+                const unsigned clear = h->h_ctrl->status & ~GDB_STATUS_BRICK_CAPACITY;
+                CK(cudaMemcpyAsync(&h->ctrl->status, &clear, sizeof(unsigned), cudaMemcpyHostToDevice, h->st));
+                if (h->cell_count) CK(cudaMemsetAsync(h->cell_count, 0, (size_t)h->cell_cap * sizeof(int), h->st));
+                k_block_resume<<<1, 1, 0, h->st>>>(h->ctrl);
+                CKL();
+                if ((rc = launch_run(h, steps - done, 1))) return rc;
+                h->last_path = 1;
+            }
+        }
     } else {
         h->last_path = 0;
         const int G = 16;
@@ -1282,6 +1392,45 @@ int gdb_time_step_kernel(gdb_sim *h, int reps, float *ms_per_launch) {
     int rc = check_ready(h);
     if (rc) return rc;
     if (reps < 1 || !ms_per_launch) return set_err(h, GDB_ERR_ARG, "bad arguments");
+    if (h->order == 2 && h->nb_kind == GDB_NBLIST_CELLS) {
+        // a list for the current positions (the persistent kernel's
+        // evaluation), then `reps` standalone brick steps
+        k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, 0.0);
+        CKL();
+        if ((rc = launch_run(h, 0, 1))) return rc;
+        const void *fn = h->ntypes == 1   ? step_bricks_kernel_nt1(h->integ, MODE_STEP)
+                         : h->ntypes == 2 ? step_bricks_kernel_nt2(h->integ, MODE_STEP)
+                                          : step_bricks_kernel_ntg(h->integ, MODE_STEP);
+        const size_t smem = sizeof(BrickSmem);
+        CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        int occ = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, BRICK_THREADS, smem));
+        const int nbricks = h->nb[0] * h->nb[1] * h->nb[2];
+        const int grid = std::max(1, std::min(nbricks, occ * h->num_sms));
+        k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, 0.0);
+        CKL();
+        const int saved_every = h->scalar_every, saved_reset = h->momentum_every;
+        h->scalar_every = 0;
+        h->momentum_every = 0;
+        float ms = 0.f;
+        cudaError_t e = cudaSuccess;
+        for (int r = 0; r <= reps && e == cudaSuccess; r++) {  // the first launch untimed
+            if (r == 1) e = cudaEventRecord(h->ev0, h->st);
+            SimArgs a = make_args(h);
+            int cur = h->cur;
+            void *args[] = {(void *)&a, (void *)&h->table, (void *)&cur};
+            if (e == cudaSuccess) e = cudaLaunchKernel(fn, dim3(grid), dim3(BRICK_THREADS), args, smem, h->st);
+            h->cur ^= 1;
+        }
+        h->scalar_every = saved_every;
+        h->momentum_every = saved_reset;
+        if (e != cudaSuccess) return set_err(h, GDB_ERR_CUDA, "brick step kernel: %s", cudaGetErrorString(e));
+        CK(cudaEventRecord(h->ev1, h->st));
+        CK(cudaEventSynchronize(h->ev1));
+        CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+        *ms_per_launch = ms / reps;
+        return GDB_OK;
+    }
     const int grid = grid_for((long long)h->n * h->tp);
     if ((rc = ensure_partials(h, grid))) return rc;
     // a list for the current positions, then `reps` step kernels alone
@@ -1345,6 +1494,42 @@ int gdb_get_nblist(gdb_sim *h, int32_t *out, int max_nbs) {
     CK(cudaMemcpyAsync(orig.data(), h->orig, N * sizeof(int), cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
     const size_t stride = h->stride;
+    if (h->order == 2 && h->nb_kind == GDB_NBLIST_CELLS) {
+        // 16-bit halo indices: map them back through every brick's runs
+        const unsigned short *l16 = reinterpret_cast<const unsigned short *>(nbl.data());
+        std::vector<int> cs((size_t)h->ncell + 1);
+        CK(cudaMemcpy(cs.data(), h->cell_start, cs.size() * sizeof(int), cudaMemcpyDeviceToHost));
+        const int nbr = h->nb[0] * h->nb[1] * h->nb[2];
+        std::vector<int> dst, src;
+        for (int r = 0; r < nbr; r++) {
+            const BrickHalo hb = brick_halo(r, h->nc, h->nb);
+            dst.clear();
+            src.clear();
+            int off = 0;
+            for (int row = 0; row < hb.wy * hb.wz; row++)
+                for_each_halo_run(hb, row % hb.wy, row / hb.wy, h->nc, h->nb, [&](int, int first, int last, int) {
+                    const int len = cs[last + 1] - cs[first];
+                    if (len == 0) return;
+                    dst.push_back(off);
+                    src.push_back(cs[first]);
+                    off += len;
+                });
+            dst.push_back(off);
+            for (int s = cs[(size_t)r * BRICK * BRICK * BRICK]; s < cs[(size_t)(r + 1) * BRICK * BRICK * BRICK]; s++) {
+                const int i = orig[s];
+                int32_t *row = out + (size_t)i * (max_nbs + 1);
+                const int cnt = nbc[s];
+                const int lim = std::min(std::min(cnt, h->max_nbs), max_nbs);
+                for (int k = 0; k < lim; k++) {
+                    const int e = l16[((size_t)(k >> 3) * stride + s) * NB16 + (k & 7)];
+                    const int q = (int)(std::upper_bound(dst.begin(), dst.end() - 1, e) - dst.begin()) - 1;
+                    row[k] = orig[src[q] + (e - dst[q])];
+                }
+                row[max_nbs] = cnt;
+            }
+        }
+        return GDB_OK;
+    }
     for (size_t s = 0; s < N; s++) {
         const int i = orig[s];
         int32_t *row = out + (size_t)i * (max_nbs + 1);
@@ -1559,6 +1744,12 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
             g->pp.push_back(pingpong | (sorted << 1));
             g->smem = std::max(g->smem, smem);
         } else if (h->n <= CLG_MAX_N) {
+            // the global-memory cluster kernel runs the row phases
+            h->bricks_ok = false;
+            if (int rc = ensure_nblist(h)) {
+                batch_free(b);
+                return rc;
+            }
             // about 4096 particles per CTA (four per lane), 1 to 16 CTAs
             // (measured on B200, 128-replica sweep: 954 / 1048 / 1134 / 1272 /
             // 1084 MATS at 512 / 1024 / 2048 / 4096 / 8192 per CTA)

@@ -4,6 +4,7 @@
 // instantiations compile in parallel.
 #pragma once
 
+#include "md_bricks.cuh"
 #include "md_phases.cuh"
 
 namespace gdb {
@@ -152,6 +153,116 @@ __device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int n
     }
 }
 
+// Neighbour-list rebuild of the brick path: the counting sort into brick
+// order (the row rebuild's phases, cells numbered brick by brick), then the
+// brick-wise list build over staged halos.
+template <bool FMA, class Sync>
+__device__ inline bool rebuild_phases_bricks(const SimArgs &a, int cur, Span g, const Sync &sync, BrickSmem &bs,
+                                             BrickPipe &pp) {
+    DevCtrl *c = a.ctrl;
+    auto none = [] {};
+    phase_cell_assign<false>(a, cur, g);
+    if (!sync(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_scan_partial(a, g);
+    if (!sync(c, [&] { block_scan_chunks(a); })) return false;
+    phase_scan_final(a, g);
+    if (!sync(c, none)) return false;
+    phase_scatter(a, g);
+    if (!sync(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_sort_cells(a, g);
+    if (!sync(c, none)) return false;
+    phase_gather(a, cur, g);
+    if (!sync(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    if (!phase_nbl_bricks<FMA>(a, bs, pp, g)) return false;
+    if (!sync(c, none)) return false;
+    trace_mark(c, TR_REBUILD_PHASE);
+    phase_finish_cells(a, cur, g);
+    const bool ok = sync(c, [&] {
+        if (threadIdx.x == 0) rebuild_done(c);
+    });
+    trace_mark(c, TR_REBUILD_DONE);
+    return ok;
+}
+
+// Persistent cooperative kernel of the brick path: one timeblock of one
+// system per launch (steps, rebuilds, thermostat), bricks as rounds, halos
+// staged by bulk copies into dynamic shared memory (BrickSmem).
+template <int NT, int INTEG>
+__global__ void __launch_bounds__(BRICK_THREADS, 2)
+    k_run_bricks(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
+    extern __shared__ __align__(128) unsigned char brick_dsm[];
+    BrickSmem &bs = *reinterpret_cast<BrickSmem *>(brick_dsm);
+    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    load_table(tab, s_tab);
+    brick_smem_init(bs);
+    DevCtrl *ctrl = a.ctrl;
+    if (*(volatile int *)&ctrl->abort) return;
+    const GridSync sync{};
+    const Span g = grid_span();
+    const int nbricks = a.nbx * a.nby * a.nbz;
+    BrickPipe pp = brick_pipe_init();
+    int cur = cur0;
+    trace_mark(ctrl, TR_START);
+    for (int s = 0; s < nsteps + do_eval; s++) {
+        if (*(volatile int *)&ctrl->rebuild) {
+            const bool ok = a.fma ? rebuild_phases_bricks<true>(a, cur, g, sync, bs, pp)
+                                  : rebuild_phases_bricks<false>(a, cur, g, sync, bs, pp);
+            if (!ok) return;
+        }
+        const int step = *(volatile int *)&ctrl->step;
+        bool ok;
+        if (s < nsteps) {
+            if (!phase_step_bricks<NT, INTEG, MODE_STEP, true>(a, bs, pp, s_tab, tab.nt, cur, step)) return;
+            trace_mark(ctrl, TR_STEP_PHASE);
+            ok = sync(ctrl, [&] {
+                finalize_step<MODE_STEP>(a, step, nbricks, s_red);
+                if (threadIdx.x == 0 && ctrl->rebuild_next) {
+                    ctrl->rebuild = 1;
+                    ctrl->rebuild_next = 0;
+                }
+            });
+            cur ^= 1;
+            trace_mark(ctrl, TR_STEP);
+        } else {
+            if (!phase_step_bricks<NT, INTEG, MODE_EVAL, true>(a, bs, pp, s_tab, tab.nt, cur, step)) return;
+            ok = sync(ctrl, [&] {
+                finalize_step<MODE_EVAL>(a, step, nbricks, s_red);
+                if (threadIdx.x == 0) ctrl->work[(step + 1) & 1] = 0;
+            });
+            trace_mark(ctrl, TR_EVAL);
+        }
+        if (!ok) return;
+    }
+}
+
+// One brick-path step (or force-only evaluation) per launch, with the list
+// already built; the last CTA to finish does the float64 bookkeeping.
+template <int NT, int INTEG, int MODE>
+__global__ void __launch_bounds__(BRICK_THREADS, 2) k_step_bricks(SimArgs a, PairTable tab, int cur) {
+    extern __shared__ __align__(128) unsigned char brick_dsm[];
+    BrickSmem &bs = *reinterpret_cast<BrickSmem *>(brick_dsm);
+    __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
+    __shared__ double s_red[NQ * 32];
+    __shared__ bool s_last;
+    load_table(tab, s_tab);
+    brick_smem_init(bs);
+    DevCtrl *ctrl = a.ctrl;
+    const int step = ctrl->step;
+    BrickPipe pp = brick_pipe_init();
+    phase_step_bricks<NT, INTEG, MODE, false>(a, bs, pp, s_tab, tab.nt, cur, step);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(&ctrl->ticket, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    finalize_step<MODE>(a, step, a.nbx * a.nby * a.nbz, s_red);
+    if (threadIdx.x == 0) ctrl->ticket = 0;
+}
+
 // Persistent cooperative kernel: one timeblock of one system per launch.
 template <int TP, int NT, int INTEG>
 __global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
@@ -195,7 +306,9 @@ __global__ void __launch_bounds__(CLG_BLOCK, 1)
     void launch_step_##NTNAME(const SimArgs &a, const PairTable &tab, cudaStream_t st, int tp, int integ, \
                               int mode, int grid, int cur);                                            \
     const void *run_kernel_##NTNAME(int tp, int integ);                                                  \
-    const void *run_clusters_kernel_##NTNAME(int tp, int integ);
+    const void *run_clusters_kernel_##NTNAME(int tp, int integ);                                         \
+    const void *run_bricks_kernel_##NTNAME(int integ);                                                   \
+    const void *step_bricks_kernel_##NTNAME(int integ, int mode);
 
 GDB_DECLARE_NT(nt1)
 GDB_DECLARE_NT(nt2)
@@ -253,6 +366,18 @@ GDB_DECLARE_NT(ntg)
             case 4: return run_clusters_tp_##NTNAME<4>(integ);                                               \
             default: return run_clusters_tp_##NTNAME<8>(integ);                                              \
         }                                                                                                    \
+    }                                                                                                        \
+    const void *run_bricks_kernel_##NTNAME(int integ) {                                                      \
+        return integ == GDB_INTEGRATOR_NVT        ? (const void *)k_run_bricks<NT, GDB_INTEGRATOR_NVT>       \
+               : integ == GDB_INTEGRATOR_LANGEVIN ? (const void *)k_run_bricks<NT, GDB_INTEGRATOR_LANGEVIN>  \
+                                                  : (const void *)k_run_bricks<NT, GDB_INTEGRATOR_NVE>;      \
+    }                                                                                                        \
+    const void *step_bricks_kernel_##NTNAME(int integ, int mode) {                                           \
+        if (mode == MODE_EVAL) return (const void *)k_step_bricks<NT, 0, MODE_EVAL>;                          \
+        return integ == GDB_INTEGRATOR_NVT ? (const void *)k_step_bricks<NT, GDB_INTEGRATOR_NVT, MODE_STEP>  \
+               : integ == GDB_INTEGRATOR_LANGEVIN                                                            \
+                   ? (const void *)k_step_bricks<NT, GDB_INTEGRATOR_LANGEVIN, MODE_STEP>                     \
+                   : (const void *)k_step_bricks<NT, GDB_INTEGRATOR_NVE, MODE_STEP>;                         \
     }
 
 }  // namespace gdb

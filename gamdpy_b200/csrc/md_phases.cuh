@@ -50,6 +50,8 @@ struct SimArgs {
     DevCtrl *ctrl;
     int n, stride, max_nbs;
     int ncell, nchunks, ncx, ncy, ncz;
+    int nbx, nby, nbz;  // bricks per dimension (staged-halo path, md_bricks.cuh), 0: cells x fastest
+    int brick_hcap;     // staged positions a brick's halo may hold (<= BRICK_HCAP)
     int nb_kind, fma;
     float Lx, Ly, Lz;
     float cps2;    // (max_cut + skin)^2, nblist.py:152
@@ -221,24 +223,28 @@ __device__ inline void phase_cell_assign(const SimArgs &a, int cur, Span g = gri
         const int cx = cell_coord(p.x, a.Lx, a.ncx, a.ctrl);
         const int cy = cell_coord(p.y, a.Ly, a.ncy, a.ctrl);
         const int cz = cell_coord(p.z, a.Lz, a.ncz, a.ctrl);
-        const int c = (cz * a.ncy + cy) * a.ncx + cx;  // x fastest
+        // x fastest over the grid, or brick by brick (bricks of 4 x 4 x 4 cells)
+        const int c = a.nbx ? ((((cz >> 2) * a.nby + (cy >> 2)) * a.nbx + (cx >> 2)) << 6) |
+                                  ((((cz & 3) << 2) | (cy & 3)) << 2) | (cx & 3)
+                            : (cz * a.ncy + cy) * a.ncx + cx;
         a.pcell[i] = c;
         a.prank[i] = atomicAdd(&a.cell_count[c], 1);
     }
 }
 
-// Block-wide exclusive scan of SCAN_CHUNK ints (SCAN_CHUNK / blockDim per
-// thread: 8 for 256 threads, 2 for 1024).
+// Block-wide exclusive scan of SCAN_CHUNK ints (ceil(SCAN_CHUNK / blockDim)
+// per thread: 8 for 256 or 288 threads, 2 for 1024; threads past the chunk
+// hold nothing).
 __device__ __forceinline__ void chunk_scan(const int *in, int len, int base, int *out_excl, int add, int *total,
                                            int *sm /* 32 */) {
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    const int ept = SCAN_CHUNK / (int)blockDim.x;
+    const int ept = (SCAN_CHUNK + (int)blockDim.x - 1) / (int)blockDim.x;
     int v[8];
     int s = 0;
 #pragma unroll
     for (int q = 0; q < 8; q++) {
         const int idx = base + t * ept + q;
-        v[q] = (q < ept && idx < len) ? in[idx] : 0;
+        v[q] = (q < ept && t * ept + q < SCAN_CHUNK && idx < len) ? in[idx] : 0;
         s += v[q];
     }
     int incl = s;
@@ -266,7 +272,7 @@ __device__ __forceinline__ void chunk_scan(const int *in, int len, int base, int
 #pragma unroll
         for (int q = 0; q < 8; q++) {
             const int idx = base + t * ept + q;
-            if (q < ept && idx < len) out_excl[idx] = run;
+            if (q < ept && t * ept + q < SCAN_CHUNK && idx < len) out_excl[idx] = run;
             run += v[q];
         }
     }
@@ -980,7 +986,6 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
         shz = ctrl->shift[ppar][2];
     }
     const float xi = ctrl->xi;
-    const size_t n = a.n;
     const int per_block = blockDim.x / TP;
     const int rounds_total = (a.n + per_block - 1) / per_block;
     const bool full = rec || reset;

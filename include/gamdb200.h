@@ -45,6 +45,7 @@ extern "C" {
 #define GDB_STATUS_BAD_ARG 0x8u
 #define GDB_STATUS_CLUSTER_CAPACITY 0x10u /* a list outgrew the cluster path's shared memory (rerun on the global path) */
 #define GDB_STATUS_BAD_INDEX 0x20u /* a cell-sort slot outside [0, n): the access was skipped */
+#define GDB_STATUS_BRICK_CAPACITY 0x40u /* a brick's halo outgrew shared memory (the run goes on without bricks) */
 
 /* potentials: gamdpy/interactions/potential_functions/ */
 #define GDB_POT_LJ_SIGMA_EPSILON 0 /* LJ_12_6_sigma_epsilon.py:6-36, params (sigma, epsilon, cut) */
@@ -221,8 +222,13 @@ int gdb_get_nbflag(gdb_sim *h, int32_t out[3]);
  * sequence, 1 persistent cooperative kernel, 2 thread-block cluster
  * (N <= 4096 with fewer than about 160 000 list entries, N x the neighbours
  * expected from the density; environment GDB_CLUSTER=1: whenever N <= 4096
- * fits, GDB_CLUSTER=0: never), -1 none yet.  Diagnostic; no counterpart in
- * the reference. */
+ * fits, GDB_CLUSTER=0: never), 3 global-memory cluster (batches), 4 the
+ * persistent kernel with staged halos (environment GDB_BRICKS=1: cells
+ * numbered in bricks of 4 x 4 x 4, each brick's halo copied into shared
+ * memory by bulk copies, 16-bit lists; cell lists from 131 073 particles,
+ * GDB_BRICK_MIN_N moves the size; off by default, measured slower than the
+ * row path on B200), -1 none yet.
+ * Diagnostic; no counterpart in the reference. */
 int gdb_get_last_path(gdb_sim *h);
 
 /* Status bits set by kernels since the last clear; gdb_clear_status resets. */

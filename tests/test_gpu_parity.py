@@ -112,8 +112,10 @@ def test_cell_build_paths_vs_oracle(oracle, n, face):
 
 @pytest.mark.parametrize("n", [200000])
 def test_thread_per_particle_build_vs_oracle(oracle, n, monkeypatch):
-    """Large systems build a thread per particle (standalone chain and
-    persistent kernel); the sets must still equal the oracle's cell build."""
+    """Large systems off the brick path build a thread per particle
+    (standalone chain and persistent kernel); the sets must still equal the
+    oracle's cell build."""
+    monkeypatch.setenv("GDB_BRICKS", "0")
     conf = workloads.ka_configuration(n, seed=13, jitter=0.2)
     L = conf.simbox.lengths
     table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
@@ -372,7 +374,7 @@ def test_rdf_and_sq_at_the_large_lj_geometry(oracle):
     rdf.update()
     got = rdf.rdf_list[-1]
     ref = oracle.rdf(conf["r"], conf.ptype, L, 1000, fma=1, r_max=5.0)
-    assert ref.sum() > 3e8 and np.array_equal(got, ref.astype(np.float64))
+    assert ref.sum() > 5e7 and np.array_equal(got, ref.astype(np.float64))
     sq = gp.CalculatorStructureFactor(conf)
     sq.generate_q_vectors(2 * np.pi * np.sqrt(237.5) / float(L[0]))
     assert len(sq.q_vectors) == 2219
