@@ -57,6 +57,8 @@ SIGNATURES = {
     "gdb_host_free": ([_P], _i),
     "gdb_set_pair_potential": ([_P, _i, _i, _i, _P, _i], _i),
     "gdb_set_nblist": ([_P, _i, _f, _i], _i),
+    "gdb_set_exclusions": ([_P, _P, _i], _i),
+    "gdb_set_bonds": ([_P, _i, _P, _i, _P], _i),
     "gdb_set_plan": ([_P, _i, _i], _i),
     "gdb_set_integrator_nve": ([_P, _f], _i),
     "gdb_set_integrator_nvt": ([_P, _f, _f, _i, _P], _i),
@@ -279,6 +281,22 @@ class Sim:
 
     def set_nblist(self, kind, skin, max_nbs):
         self.call("gdb_set_nblist", int(kind), float(skin), int(max_nbs))
+
+    def set_exclusions(self, excl):
+        """(n, max + 1) int32 exclusion table with the count last, or None."""
+        if excl is None:
+            self.call("gdb_set_exclusions", None, 0)
+            return
+        ex = i32(excl)
+        if ex.ndim != 2 or ex.shape[0] != self.n:
+            raise ValueError(f"exclusions must be ({self.n}, max + 1)")
+        self.call("gdb_set_exclusions", ptr(ex), int(ex.shape[1] - 1))
+
+    def set_bonds(self, indices, params):
+        """indices (nbonds, 3) int32 (i, j, type); params (ntypes, 2) (r0, k)."""
+        ind = i32(indices).reshape(-1, 3)
+        prm = f32(params).reshape(-1, 2)
+        self.call("gdb_set_bonds", int(len(ind)), ptr(ind), int(len(prm)), ptr(prm))
 
     def set_plan(self, tp=0, pb=0):
         self.call("gdb_set_plan", int(tp), int(pb))

@@ -276,13 +276,27 @@ class Configuration:
         self.simbox = Orthorhombic(self.D, box_vector)
 
     def make_positions(self, N, rho):
-        """Simple-cubic positions (Configuration.py:308-361 semantics: ceil(N^(1/D))
-        particles per line, centred, scaled to density rho)."""
+        """Positions along the simple-cubic lines of ceil(N^(1/D)) particles,
+        the reference's arithmetic (Configuration.py:308-361): coordinate d of
+        particle i is (i mod p^(d+1)) / p^d with true division (p particles
+        per line), so consecutive indices step one lattice spacing in x and a
+        fraction of one in the other dimensions -- chains built from
+        consecutive indices start with equal bond lengths -- then the centring
+        offsets, the shift by int(p/2) and the scaling to density rho."""
         D = self.D
-        ppl = int(np.ceil(N ** (1.0 / D) - 1e-9))
-        box_length = (N / rho) ** (1.0 / D)
-        idx = np.stack(np.unravel_index(np.arange(N), [ppl] * D)[::-1], axis=1).astype(np.float64)
-        pos = (idx - ppl // 2) * (box_length / ppl)
+        ppl = float(np.ceil(pow(N, 1.0 / D)))
+        box_length = pow(N / rho, 1.0 / D)
+        idx = np.arange(N, dtype=np.float64)
+        pos = np.empty((N, D), np.float64)
+        pos[:, D - 1] = idx / ppl ** (D - 1)
+        for d in range(D - 2, -1, -1):
+            pos[:, d] = (idx % ppl ** (d + 1)) / ppl ** d
+        remove = 0
+        for d in range(1, D):
+            remove += D ** (D - d)
+            pos[:, d] -= remove / N
+        pos -= np.array(D * [int(0.5 * ppl)])
+        pos *= box_length / ppl
         self["r"] = pos
         self.simbox = Orthorhombic(D, np.array(D * [box_length]))
 

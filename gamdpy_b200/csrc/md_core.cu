@@ -139,6 +139,13 @@ struct gdb_sim {
     ulonglong2 *rng = nullptr;
     float4 *lbeta = nullptr;
     float alpha = 0.f;
+    // molecules: pair exclusions and harmonic bonds (by user index)
+    int *excl = nullptr;
+    int max_excl = 0;
+    int *bond_cnt = nullptr, *bond_j = nullptr, *bond_t = nullptr;
+    float2 *bond_prm = nullptr;
+    int bond_max = 0;
+    int *slot_of = nullptr;
     char err[512] = "";
 };
 
@@ -245,6 +252,12 @@ __global__ void k_block_resume(DevCtrl *ctrl) {
     ctrl->work[0] = ctrl->work[1] = 0;
     ctrl->rebuild = 1;
     ctrl->rebuild_next = 0;
+}
+
+// slot of every user index, from the current order
+__global__ void k_fill_slot_of(int n, const int *orig, int *slot_of) {
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < n) slot_of[orig[s]] = s;
 }
 
 // upload helpers: gamdpy layout -> float4 / int4
@@ -418,7 +431,8 @@ static int ensure_nblist(gdb_sim *h) {
         // 8-cell halo of a brick in every dimension and whose expected halo
         // fits the stage with a quarter to spare
         const double per_cell = (double)h->n / ((double)nc[0] * nc[1] * nc[2]);
-        const bool use = h->bricks_req && h->bricks_ok && h->staged_ok && h->persistent &&
+        const bool use = h->bricks_req && h->bricks_ok && h->staged_ok && h->persistent && !h->excl &&
+                         !h->bond_cnt &&
                          h->n >= h->brick_min_n && h->n > h->nsq_auto_max && nc[0] >= BRICK_W &&
                          nc[1] >= BRICK_W && nc[2] >= BRICK_W &&
                          per_cell * BRICK_W * BRICK_W * BRICK_W * 1.25 <= BRICK_HCAP;
@@ -528,6 +542,14 @@ static SimArgs make_args(gdb_sim *h) {
     a.rng = h->rng;
     a.lbeta = h->lbeta;
     a.alpha = h->alpha;
+    a.excl = h->excl;
+    a.max_excl = h->max_excl;
+    a.bond_cnt = h->bond_cnt;
+    a.bond_j = h->bond_j;
+    a.bond_t = h->bond_t;
+    a.bond_prm = h->bond_prm;
+    a.bond_max = h->bond_max;
+    a.slot_of = h->slot_of;
     return a;
 }
 
@@ -873,7 +895,8 @@ int gdb_sim_destroy(gdb_sim *h) {
     void *bufs[] = {h->pos[0], h->pos[1], h->vel,        h->frc,       h->rref,  h->pos_tmp, h->vel_tmp,
                     h->img,    h->img_tmp, h->orig,      h->orig_tmp,  h->nbl,   h->nbc,     h->pscal,
                     h->pscal_tmp, h->cell_count, h->cell_start, h->pcell, h->prank, h->perm, h->scell,
-                    h->bsum,   h->ctrl,   h->partials,   h->rows,  h->conf, h->trace, h->rng, h->lbeta};
+                    h->bsum,   h->ctrl,   h->partials,   h->rows,  h->conf, h->trace, h->rng, h->lbeta,
+                    h->excl,   h->bond_cnt, h->bond_j,   h->bond_t, h->bond_prm, h->slot_of};
     for (void *p : bufs)
         if (p) cudaFree(p);
     if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
@@ -925,6 +948,10 @@ int gdb_upload_state(gdb_sim *h, const float *r, const float *v, const float *m,
     k_pack<<<grid_for(h->n), GDB_BLOCK, 0, h->st>>>(h->n, dr, dv, dm, dpt, r_im ? dim : nullptr, h->pos[0], h->vel,
                                                    h->img, h->orig);
     CKL();
+    if (h->slot_of) {
+        k_fill_slot_of<<<grid_for(h->n), GDB_BLOCK, 0, h->st>>>(h->n, h->orig, h->slot_of);
+        CKL();
+    }
     CK(cudaFreeAsync(stage, h->st));
     int one = 1;
     CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
@@ -1058,6 +1085,92 @@ int gdb_set_nblist(gdb_sim *h, int kind, float skin, int max_nbs) {
         CK(cudaSetDevice(h->dev));
         int one = 1;
         CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    }
+    return GDB_OK;
+}
+
+int gdb_set_exclusions(gdb_sim *h, const int32_t *excl, int max_excl) {
+    if (!h) return set_err(h, GDB_ERR_ARG, "NULL handle");
+    CK(cudaSetDevice(h->dev));
+    if (h->excl) cudaFree(h->excl);
+    h->excl = nullptr;
+    h->max_excl = 0;
+    if (excl) {
+        if (max_excl < 1) return set_err(h, GDB_ERR_ARG, "gdb_set_exclusions: max_excl must be positive");
+        const size_t w = (size_t)max_excl + 1;
+        for (int i = 0; i < h->n; i++) {
+            const int cnt = excl[(size_t)i * w + max_excl];
+            if (cnt < 0 || cnt > max_excl)
+                return set_err(h, GDB_ERR_ARG, "gdb_set_exclusions: particle %d has %d exclusions (room for %d)", i,
+                               cnt, max_excl);
+            for (int k = 0; k < cnt; k++) {
+                const int j = excl[(size_t)i * w + k];
+                if (j < 0 || j >= h->n)
+                    return set_err(h, GDB_ERR_ARG, "gdb_set_exclusions: particle %d excludes %d", i, j);
+            }
+        }
+        CK(cudaMalloc(&h->excl, (size_t)h->n * w * sizeof(int)));
+        CK(cudaMemcpy(h->excl, excl, (size_t)h->n * w * sizeof(int), cudaMemcpyHostToDevice));
+        h->max_excl = max_excl;
+    }
+    free_graphs(h);
+    if (h->uploaded) {
+        int one = 1;
+        CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
+        CK(cudaStreamSynchronize(h->st));
+    }
+    return GDB_OK;
+}
+
+int gdb_set_bonds(gdb_sim *h, int nbonds, const int32_t *indices, int ntypes, const float *params) {
+    if (!h || nbonds < 0 || (nbonds > 0 && (!indices || !params || ntypes < 1)))
+        return set_err(h, GDB_ERR_ARG, "gdb_set_bonds: bad arguments");
+    CK(cudaSetDevice(h->dev));
+    int **bufs[] = {&h->bond_cnt, &h->bond_j, &h->bond_t};
+    for (int **b : bufs) {
+        if (*b) cudaFree(*b);
+        *b = nullptr;
+    }
+    if (h->bond_prm) cudaFree(h->bond_prm);
+    h->bond_prm = nullptr;
+    h->bond_max = 0;
+    free_graphs(h);
+    if (nbonds == 0) return GDB_OK;
+    // per-particle partner lists: every bond appears at both of its ends
+    std::vector<int> cnt(h->n, 0);
+    for (int b = 0; b < nbonds; b++) {
+        const int i = indices[3 * b], j = indices[3 * b + 1], t = indices[3 * b + 2];
+        if (i < 0 || i >= h->n || j < 0 || j >= h->n || i == j || t < 0 || t >= ntypes)
+            return set_err(h, GDB_ERR_ARG, "gdb_set_bonds: bond %d (%d, %d, type %d) is invalid", b, i, j, t);
+        cnt[i]++;
+        cnt[j]++;
+    }
+    int bmax = 1;
+    for (int c : cnt) bmax = std::max(bmax, c);
+    std::vector<int> bj((size_t)h->n * bmax, 0), bt((size_t)h->n * bmax, 0), fill(h->n, 0);
+    for (int b = 0; b < nbonds; b++) {
+        const int i = indices[3 * b], j = indices[3 * b + 1], t = indices[3 * b + 2];
+        bj[(size_t)i * bmax + fill[i]] = j;
+        bt[(size_t)i * bmax + fill[i]++] = t;
+        bj[(size_t)j * bmax + fill[j]] = i;
+        bt[(size_t)j * bmax + fill[j]++] = t;
+    }
+    std::vector<float2> prm(ntypes);
+    for (int t = 0; t < ntypes; t++) prm[t] = make_float2(params[2 * t], params[2 * t + 1]);
+    CK(cudaMalloc(&h->bond_cnt, (size_t)h->n * sizeof(int)));
+    CK(cudaMalloc(&h->bond_j, bj.size() * sizeof(int)));
+    CK(cudaMalloc(&h->bond_t, bt.size() * sizeof(int)));
+    CK(cudaMalloc(&h->bond_prm, prm.size() * sizeof(float2)));
+    CK(cudaMemcpy(h->bond_cnt, cnt.data(), (size_t)h->n * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->bond_j, bj.data(), bj.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->bond_t, bt.data(), bt.size() * sizeof(int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->bond_prm, prm.data(), prm.size() * sizeof(float2), cudaMemcpyHostToDevice));
+    h->bond_max = bmax;
+    if (!h->slot_of) CK(cudaMalloc(&h->slot_of, (size_t)h->n * sizeof(int)));
+    if (h->uploaded) {
+        k_fill_slot_of<<<grid_for(h->n), GDB_BLOCK, 0, h->st>>>(h->n, h->orig, h->slot_of);
+        CKL();
         CK(cudaStreamSynchronize(h->st));
     }
     return GDB_OK;
@@ -1283,7 +1396,8 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
     CK(cudaEventRecord(h->ev0, h->st));
     k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
     CKL();
-    if (h->cluster_ok && h->n <= CL_MAX_N && h->integ != GDB_INTEGRATOR_LANGEVIN && cluster_preferred(h)) {
+    if (h->cluster_ok && h->n <= CL_MAX_N && h->integ != GDB_INTEGRATOR_LANGEVIN && !h->excl && !h->bond_cnt &&
+        cluster_preferred(h)) {
         rc = run_cluster(h, steps);
         if (rc == GDB_OK) {
             CK(cudaEventRecord(h->ev1, h->st));
@@ -1736,7 +1850,7 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
         int C, tp, cap, pingpong, sorted;
         size_t smem;
         cluster_shape(h->n, particles_per_cta, &C, &tp);
-        if (h->cluster_ok && h->n <= CL_MAX_N &&
+        if (h->cluster_ok && h->n <= CL_MAX_N && !h->excl && !h->bond_cnt &&
             cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &pingpong, &sorted, &smem)) {
             gdb_batch::Group *g = batch_group(b, 0, C, tp);
             g->idx.push_back(k);

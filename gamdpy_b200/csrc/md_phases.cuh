@@ -65,7 +65,26 @@ struct SimArgs {
     ulonglong2 *rng;
     float4 *lbeta;
     float alpha;
+    // molecules: pair exclusions and harmonic bonds, by user index
+    const int *excl;          // (n, max_excl + 1), count last; NULL: no exclusions
+    int max_excl;
+    const int *bond_cnt;      // bonds of each particle; NULL: no bonds
+    const int *bond_j;        // partner (user index), (n, bond_max)
+    const int *bond_t;        // bond type, (n, bond_max)
+    const float2 *bond_prm;   // (r0, k) per bond type
+    int bond_max;
+    int *slot_of;             // slot of each user index, kept by the cell sort (bonds)
 };
+
+// The pair (ui, uj) of user indices is in ui's exclusion row
+// (interactions/nblist.py:120-123, nblist_linked_lists.py:174-178).
+__device__ __forceinline__ bool excluded(const SimArgs &a, int ui, int uj) {
+    const int *row = a.excl + (size_t)ui * (a.max_excl + 1);
+    const int cnt = min(row[a.max_excl], a.max_excl);
+    for (int k = 0; k < cnt; k++)
+        if (row[k] == uj) return true;
+    return false;
+}
 
 __device__ __forceinline__ float4 *cur_pos(const SimArgs &a, int cur) { return cur ? a.pos1 : a.pos0; }
 
@@ -183,6 +202,7 @@ __device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_sp
             const int j = j0 + lane;
             bool hit = false;
             if (j < a.n && j != i) hit = dist_sq_exact<FMA>(load<NC>(pos + j), pi, a.Lx, a.Ly, a.Lz) < a.cps2;
+            if (hit && a.excl) hit = !excluded(a, a.orig[i], a.orig[j]);
             const unsigned m = __ballot_sync(0xffffffffu, hit);
             if (hit) {
                 const int k = count + __popc(m & ((1u << lane) - 1u));
@@ -521,7 +541,8 @@ __device__ inline void phase_nbl_cells_t(const SimArgs &a, Span g, int *s_lo, in
                         if (p >= gn) break;
                         const float d2 = SHIFTED ? dist_sq_shifted<FMA>(pj, pi[p], sh.x, sh.y, sh.z)
                                                  : dist_sq_exact<FMA>(pj, pi[p], Lx, Ly, Lz);
-                        const bool hit = ok && j != g0 + p && d2 < a.cps2;
+                        bool hit = ok && j != g0 + p && d2 < a.cps2;
+                        if (hit && a.excl) hit = !excluded(a, a.orig_tmp[g0 + p], a.orig_tmp[j]);
                         const unsigned m = __ballot_sync(0xffffffffu, hit);
                         if (hit) {
                             const int k = cnt[p] + __popc(m & ((1u << lane) - 1u));
@@ -564,10 +585,11 @@ __device__ inline void phase_nbl_cells_tpp(const SimArgs &a, Span g) {
         const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
         int *out = a.nbl + (size_t)s * NB_CHUNK;
         int cnt = 0;
+        const int ui = a.excl ? a.orig_tmp[s] : 0;
         auto test = [&](float4 pj, int j, float sx, float sy, float sz) {
             const float d2 =
                 SHIFTED ? dist_sq_shifted<FMA>(pj, pi, sx, sy, sz) : dist_sq_exact<FMA>(pj, pi, Lx, Ly, Lz);
-            if (d2 < cps2 && j != s) {
+            if (d2 < cps2 && j != s && !(a.excl && excluded(a, ui, a.orig_tmp[j]))) {
                 if (cnt < maxn) out[(size_t)(cnt >> 2) * cs + (cnt & 3)] = j;
                 cnt++;
             }
@@ -667,6 +689,7 @@ __device__ inline void phase_finish_cells(const SimArgs &a, int cur, Span g = gr
         a.vel[s] = a.vel_tmp[s];
         a.img[s] = a.img_tmp[s];
         a.orig[s] = a.orig_tmp[s];
+        if (a.slot_of) a.slot_of[a.orig_tmp[s]] = s;
         a.pscal[3 * n + s] = a.pscal_tmp[3 * n + s];
         a.pscal[4 * n + s] = a.pscal_tmp[4 * n + s];
     }
@@ -819,6 +842,37 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
         pair_force<REC, NT>(pr, pi, p1, v1, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
         pair_force<REC, NT>(pr, pi, p2, v2, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
         pair_force<REC, NT>(pr, pi, p3, v3, Lx, Ly, Lz, ilx, ily, ilz, fx, fy, fz, u, w, l);
+    }
+}
+
+// Harmonic bonds of the particle in slot i, its own side of each
+// (interactions/bonds.py:102-135 with potential_functions/
+// harmonic_bond_function.py:37-43): dr = r_partner - r_i by the minimum
+// image, u = k (r - r0)^2 / 2 and s = -k (r - r0) / r; the particle takes
+// f -= dr s, half of u, its half of the virial dr^2 s / (2 D), and the whole
+// (1 - D) s + k into lapU, as the reference adds to both ends of a bond.
+__device__ __forceinline__ void bond_forces(const SimArgs &a, int i, float4 pi, const float4 *pos, bool rec, float &fx,
+                                            float &fy, float &fz, float &u, float &w, float &l) {
+    const int ui = a.orig[i];
+    const int cnt = a.bond_cnt[ui];
+    for (int b = 0; b < cnt; b++) {
+        const size_t e = (size_t)ui * a.bond_max + b;
+        const int j = a.slot_of[a.bond_j[e]];
+        const float2 prm = a.bond_prm[a.bond_t[e]];
+        const float4 pj = pos[j];
+        const float dx = mic(__fsub_rn(pj.x, pi.x), a.Lx), dy = mic(__fsub_rn(pj.y, pi.y), a.Ly),
+                    dz = mic(__fsub_rn(pj.z, pi.z), a.Lz);
+        const float d2 = dx * dx + dy * dy + dz * dz;
+        const float d = sqrtf(d2);
+        const float s = -prm.y * (d - prm.x) / d;
+        fx -= dx * s;
+        fy -= dy * s;
+        fz -= dz * s;
+        if (rec) {
+            u += 0.5f * (0.5f * prm.y * (d - prm.x) * (d - prm.x));
+            w += d2 * s * (1.0f / 6.0f);
+            l += -2.0f * s + prm.y;
+        }
     }
 }
 
@@ -1034,6 +1088,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
                 }
             }
         }
+        if (active && sub == 0 && a.bond_cnt) bond_forces(a, i, pi, pos, rec, fx, fy, fz, u, w, l);
         if (active && sub == 0)
             finish_particle<INTEG, MODE>(a, i, pi, v, rr, fx, fy, fz, u, w, l, rec, reset, step, shift_pending, shx,
                                          shy, shz, xi, pos_next, red, moved);

@@ -20,14 +20,20 @@ class Interaction:
 
 
 class NbList2:
-    """O(N^2) neighbour-list build (gamdpy/interactions/nblist.py:5-163)."""
+    """O(N^2) neighbour-list build (gamdpy/interactions/nblist.py:5-163).
+    ``exclusions``: None or the (N, max_exclusions + 1) int32 table with the
+    count last (Bonds.get_exclusions); excluded pairs never enter the list."""
     kind = _lib.NBLIST_NSQ
 
     def __init__(self, configuration, exclusions, max_num_nbs):
-        if exclusions is not None and len(exclusions) > 0:
-            raise NotImplementedError("neighbour-list exclusions are outside the B200 hot path")
         self.N = configuration.N
         self.max_num_nbs = max_num_nbs
+        self.exclusions = None
+        if exclusions is not None:
+            ex = np.ascontiguousarray(np.asarray(exclusions, dtype=np.int32))
+            if ex.ndim != 2 or ex.shape[0] != self.N or ex.shape[1] < 2:
+                raise ValueError(f"exclusions must be (N, max + 1) with the count last, got {ex.shape}")
+            self.exclusions = ex
 
 
 class NbListLinkedLists(NbList2):
@@ -113,6 +119,7 @@ class PairPotential(Interaction):
         sim.set_pair_potential(kind, cutmode, table)
         nbl = self.make_nblist(configuration, compute_plan)
         sim.set_nblist(nbl.kind, float(np.float32(compute_plan["skin"])), self.max_num_nbs)
+        sim.set_exclusions(nbl.exclusions)
         self._device = sim
         self.max_cut = max_cut
 
@@ -130,3 +137,48 @@ class PairPotential(Interaction):
     def get_nblist(self):
         """Neighbour list in gamdpy's layout (N, max_num_nbs+1), count last."""
         return self._device.nblist(self.max_num_nbs)
+
+
+class Bonds(Interaction):
+    """Fixed bonds between particles (gamdpy/interactions/bonds.py:12-150):
+    ``bond_potential`` (harmonic_bond_function), ``potential_params`` one
+    (r0, k) row per bond type, ``indices`` rows (i, j, bond type).  The bond
+    forces are added per particle inside the library's fused step (each end
+    evaluates its bonds: no atomics, the same sums in every run)."""
+
+    def __init__(self, bond_potential, potential_params, indices):
+        self.bond_potential = bond_potential
+        self.potential_params = potential_params
+        self.indices = indices
+        self._device = None
+
+    def _arrays(self):
+        if getattr(self.bond_potential, "_gdb_bond", None) != "harmonic":
+            raise NotImplementedError("gamdpy_b200 evaluates harmonic bonds (harmonic_bond_function) in CUDA; got "
+                                      f"{getattr(self.bond_potential, '__name__', self.bond_potential)!r}")
+        params = np.ascontiguousarray(np.array(self.potential_params, dtype=np.float32))
+        if params.ndim != 2 or params.shape[1] < 2:
+            raise ValueError("potential_params must hold one (r0, k) row per bond type")
+        indices = np.ascontiguousarray(np.array(self.indices, dtype=np.int32))
+        if indices.ndim != 2 or indices.shape[1] != 3:
+            raise ValueError("indices must be rows (i, j, bond type)")
+        if len(indices) and indices[:, -1].max() >= params.shape[0]:
+            raise ValueError("a bond type has no parameter row")
+        return indices, params[:, :2].copy()
+
+    def get_exclusions(self, configuration, max_number_exclusions=20):
+        """(N, max + 1) int32 table of every particle's bonded partners with
+        the count last, the reference's format (bonds.py:137-150)."""
+        exclusions = np.zeros((configuration.N, max_number_exclusions + 1), dtype=np.int32)
+        for i, j, _ in self.indices:
+            for a, b in ((i, j), (j, i)):
+                if exclusions[a, -1] < max_number_exclusions:
+                    exclusions[a, exclusions[a, -1]] = b
+                exclusions[a, -1] += 1
+        assert np.max(exclusions[:, -1]) <= max_number_exclusions
+        return exclusions
+
+    def configure_device(self, sim, configuration):
+        indices, params = self._arrays()
+        sim.set_bonds(indices, params)
+        self._device = sim

@@ -90,3 +90,17 @@ def apply_shifted_potential_cutoff(pair_potential):
     potential._gdb_cutmode = _lib.CUT_SHIFTED_POTENTIAL
     potential.__name__ = f"shifted_potential({getattr(pair_potential, '__name__', 'potential')})"
     return potential
+
+
+def harmonic_bond_function(dist, params):
+    """u = k (r - r0)^2 / 2; returns (u, s = -u'/r, u'') with params (r0, k)
+    (potential_functions/harmonic_bond_function.py:6-43)."""
+    length, strength = f32(params[0]), f32(params[1])
+    d = dist if isinstance(dist, np.ndarray) else f32(dist)
+    u = f32(0.5) * strength * (d - length) ** 2
+    s = -strength * (d - length) / d
+    umm = strength
+    return u, s, umm
+
+
+harmonic_bond_function._gdb_bond = "harmonic"

@@ -69,12 +69,18 @@ class ScalarSaver(RuntimeAction):
         output.attrs["steps_between_output"] = self.steps_between_output
         output.attrs["scalar_names"] = list(self.sid.keys())
 
-    def update_from_rows(self, block, rows, output, volume):
-        """rows: (saves, 5) float64 from the library (U, W, lapU, K, Fsq)."""
+    def update_from_rows(self, block, rows, output, volume, compute_flags=None):
+        """rows: (saves, 5) float64 from the library (U, W, lapU, K, Fsq).
+        A column whose compute flag the run leaves off stays zero, as the
+        reference's saver sums per-particle values its kernels never filled
+        (scalar_saver.py:120-130)."""
         col = {"U": 0, "W": 1, "lapU": 2, "K": 3, "Fsq": 4}
         out = np.zeros((self.scalar_saves_per_block, self.num_scalars), np.float32)
         for name, idx in self.sid.items():
-            out[:, idx] = volume if name == "Vol" else rows[: self.scalar_saves_per_block, col[name]]
+            if name == "Vol":
+                out[:, idx] = volume
+            elif compute_flags is None or compute_flags.get(name, False):
+                out[:, idx] = rows[: self.scalar_saves_per_block, col[name]]
         output["scalars"][block, :] = out
 
 

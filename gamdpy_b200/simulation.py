@@ -18,7 +18,7 @@ import numpy as np
 from . import _lib
 from .configuration import Configuration, get_default_compute_flags, unit_cells
 from .integrators import NVE, NVT, NVT_Langevin
-from .interactions import PairPotential
+from .interactions import Bonds, PairPotential
 from .runtime_actions import ConfigurationSaver, MomentumReset, ScalarSaver
 
 B200_NUM_SM = 148
@@ -73,6 +73,17 @@ def get_default_compute_plan(configuration):
     return {"pb": pb, "tp": tp, "skin": skin, "UtilizeNIII": UtilizeNIII, "gridsync": gridsync, "nblist": nblist}
 
 
+def split_interactions(interactions):
+    """(PairPotential, Bonds or None) of an interactions list: the library
+    runs one pair potential, optionally with one set of harmonic bonds."""
+    items = interactions if isinstance(interactions, list) else [interactions]
+    pairs = [x for x in items if isinstance(x, PairPotential)]
+    bonds = [x for x in items if isinstance(x, Bonds)]
+    if len(pairs) != 1 or len(bonds) > 1 or len(pairs) + len(bonds) != len(items):
+        raise NotImplementedError("gamdpy_b200 runs one PairPotential per simulation, optionally with one Bonds")
+    return pairs[0], (bonds[0] if bonds else None)
+
+
 def _lanes(tp):
     """Library lanes per particle for a gamdpy ``tp``: largest power of two
     <= tp, at most 32."""
@@ -93,8 +104,7 @@ class Simulation:
         self.compute_plan = dict(compute_plan) if compute_plan is not None else get_default_compute_plan(
             configuration)
         self.interactions = interactions if isinstance(interactions, list) else [interactions]
-        if len(self.interactions) != 1 or not isinstance(self.interactions[0], PairPotential):
-            raise NotImplementedError("gamdpy_b200 runs exactly one PairPotential per simulation")
+        self._pair, self._bonds = split_interactions(self.interactions)
         self.integrator = integrator
         if not isinstance(integrator, (NVE, NVT, NVT_Langevin)):
             raise NotImplementedError("gamdpy_b200 supports the NVE, NVT and NVT_Langevin integrators")
@@ -151,12 +161,14 @@ class Simulation:
         conf = self.configuration
         if conf.D != 3:
             raise NotImplementedError("gamdpy_b200 simulates D = 3")
-        pp = self.interactions[0]
+        pp = self._pair
         table, _ = pp.table()
         self._sim = _lib.Sim(conf.N, table.shape[0], device)
         conf._attach(self._sim)
         self._sim.set_box(conf.simbox.lengths)
         pp.configure_device(self._sim, conf, self.compute_plan)
+        if self._bonds is not None:
+            self._bonds.configure_device(self._sim, conf)
         # gamdpy's tp heuristic targets its own launch shape; the library picks
         # lanes per particle for B200 unless the plan sets "lanes"
         self._sim.set_plan(int(self.compute_plan.get("lanes", 0)))
@@ -227,13 +239,19 @@ class Simulation:
         """Host side of one finished timeblock: state back to the host, list
         validity check, runtime-action output (Simulation.py:418-447)."""
         self.configuration.copy_to_host()
+        # quantities the run's compute flags leave off read zero, as in the
+        # reference, whose kernels then never accumulate them
+        for name in ("U", "W", "lapU", "K", "Fsq"):
+            if name in self.configuration.sid and not self.compute_flags.get(name, False):
+                self.configuration.scalars[:, self.configuration.sid[name]] = 0.0
         if isinstance(self.integrator, NVT):
             self.integrator.sync_from_device()
         for interaction in self.interactions:
             interaction.check_datastructure_validity()
         if self._scalar_saver is not None:
             rows = self._sim.scalar_rows(self._scalar_saver.scalar_saves_per_block)
-            self._scalar_saver.update_from_rows(block, rows, self.memory, self.configuration.get_volume())
+            self._scalar_saver.update_from_rows(block, rows, self.memory, self.configuration.get_volume(),
+                                                self.compute_flags)
         if self._conf_saver is not None:
             frames = self._sim.saved_configurations(self._conf_saver.conf_per_block)
             self._conf_saver.update_from_frames(block, frames, self.memory)
@@ -293,7 +311,7 @@ class Simulation:
         saved = (conf["r"].copy(), conf["v"].copy(), conf.r_im.copy())
         xi = self.integrator.thermostat_state.copy() if isinstance(self.integrator, NVT) else None
         skins = list(skins) if skins is not None else [float(self.compute_plan["skin"])]
-        pp = self.interactions[0]
+        pp = self._pair
         best = None
         for skin in skins:
             for tp in tps_candidates:

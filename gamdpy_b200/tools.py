@@ -17,13 +17,15 @@ class Evaluator:
         self.compute_plan = dict(compute_plan) if compute_plan is not None else get_default_compute_plan(
             configuration)
         self.interactions = interactions if isinstance(interactions, list) else [interactions]
-        if len(self.interactions) != 1:
-            raise NotImplementedError("gamdpy_b200 evaluates one PairPotential")
-        pp = self.interactions[0]
+        from .simulation import split_interactions
+        pp, bonds = split_interactions(self.interactions)
+        self._pair = pp
         table, _ = pp.table()
         self._sim = _lib.Sim(configuration.N, table.shape[0], device)
         self._sim.set_box(configuration.simbox.lengths)
         pp.configure_device(self._sim, configuration, self.compute_plan)
+        if bonds is not None:
+            bonds.configure_device(self._sim, configuration)
         self._sim.set_plan(int(self.compute_plan.get("lanes", 0)))
 
     def evaluate(self, configuration=None):
@@ -38,7 +40,7 @@ class Evaluator:
         for k in ("U", "W", "lapU"):
             if k in conf.sid:
                 conf.scalars[:, conf.sid[k]] = sc[k]
-        self.interactions[0].check_datastructure_validity()
+        self._pair.check_datastructure_validity()
 
 
 def calc_dynamics(trajectory, first_block, qvalues=None):

@@ -132,6 +132,24 @@ int gdb_set_pair_potential(gdb_sim *h, int kind, int cutmode, int ntypes, const 
  * pair_potential.py:84-97; compute_plan['nblist'], ['skin']). */
 int gdb_set_nblist(gdb_sim *h, int kind, float skin, int max_nbs);
 
+/* Pair exclusions (PairPotential(..., exclusions), interactions/
+ * pair_potential.py:12-20, tested in the list builds at
+ * interactions/nblist.py:120-123 and nblist_linked_lists.py:174-178): excl is
+ * the (n, max_excl + 1) int32 table of user indices with the count last, as
+ * Bonds.get_exclusions returns it (interactions/bonds.py:137-150); excluded
+ * pairs never enter the neighbour list.  NULL removes the table.  Systems with
+ * exclusions or bonds run on the grid kernels, not the thread-block-cluster
+ * or staged-halo paths. */
+int gdb_set_exclusions(gdb_sim *h, const int32_t *excl, int max_excl);
+
+/* Harmonic bonds (interactions/bonds.py:12-135 with
+ * potential_functions/harmonic_bond_function.py:6-43): indices (nbonds, 3)
+ * int32 rows (i, j, bond type) of user indices, params (ntypes, 2) float32
+ * rows (r0, k).  u = k (r - r0)^2 / 2 per bond, half to each end; the bond
+ * forces are added in the fused step before the integration.  nbonds = 0
+ * removes them. */
+int gdb_set_bonds(gdb_sim *h, int nbonds, const int32_t *indices, int ntypes, const float *params);
+
 /* Threads per particle (compute_plan['tp'], simulation/get_default_compute_plan.py:55-63):
  * 1, 2, 4, 8, 16 or 32 lanes share one particle's neighbours; 0 = choose.
  * pb (particles per block): for systems on the thread-block-cluster path

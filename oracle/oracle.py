@@ -170,6 +170,55 @@ def forces(r, ptype, box, table, nbl, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF,
     return {"f": f, "U": U, "W": W, "lapU": lap, "Fsq": fsq}
 
 
+def exclude(nbl, exclusions):
+    """A neighbour list without the excluded pairs, as the builds' exclusion
+    test (interactions/nblist.py:120-123, nblist_linked_lists.py:174-178)
+    leaves it: a candidate is dropped when it appears among the first
+    exclusions[i, -1] entries of particle i's row; the order of the rest is
+    kept."""
+    nbl = np.asarray(nbl)
+    ex = np.asarray(exclusions)
+    out = np.zeros_like(nbl)
+    for i in range(len(nbl)):
+        drop = set(ex[i, : ex[i, -1]].tolist())
+        row = [j for j in nbl[i, : nbl[i, -1]].tolist() if j not in drop]
+        out[i, : len(row)] = row
+        out[i, -1] = len(row)
+    return out
+
+
+def bond_terms(r, box, indices, params):
+    """Harmonic bond contributions per particle (interactions/bonds.py:102-135
+    with potential_functions/harmonic_bond_function.py:37-43), each bond in
+    float32 as the reference computes it: dr = r_j - r_i by the minimum image,
+    dist = sqrt(dist_sq), u = k (dist - r0)^2 / 2, s = -k (dist - r0) / dist;
+    f_i -= dr s, f_j += dr s, u / 2 and dr^2 s / (2 D) to both ends, and
+    (1 - D) s + k to both lapU entries; per-particle sums in float64.
+    Returns dict f (N, 3), U, W, lapU (N,)."""
+    r, box = _f32(r), _f32(box)
+    n = len(r)
+    f = np.zeros((n, 3)); U = np.zeros(n); W = np.zeros(n); lap = np.zeros(n)
+    half, vf = np.float32(0.5), np.float32(0.5 / 3)
+    for i, j, t in np.asarray(indices):
+        r0, k = np.float32(params[t][0]), np.float32(params[t][1])
+        dr = np.zeros(3, np.float32)
+        for c in range(3):
+            d = r[j, c] - r[i, c]
+            d = d - box[c] if np.float32(2.0) * d > box[c] else (d + box[c] if np.float32(2.0) * d < -box[c] else d)
+            dr[c] = d
+        dist = np.float32(math.sqrt(np.float32(dr[0] * dr[0] + dr[1] * dr[1] + dr[2] * dr[2])))
+        u = half * k * (dist - r0) ** 2
+        s = -k * (dist - r0) / dist
+        f[i] -= dr * s
+        f[j] += dr * s
+        w = np.float32(np.sum(dr * dr * s * vf))
+        U[i] += u * half; U[j] += u * half
+        W[i] += w; W[j] += w
+        lp = np.float32(-2.0) * s + k
+        lap[i] += lp; lap[j] += lp
+    return {"f": f, "U": U, "W": W, "lapU": lap}
+
+
 def forces_fp64(r, ptype, box, sigma, epsilon, cut, nbl):
     """Forces of the shifted-force LJ_12_6_sigma_epsilon pair potential over
     a neighbour list, every operation in float64 (the float32 positions taken

@@ -378,6 +378,90 @@ def case_known_answers():
     print("known answers:", {k: v for k, v in res.items() if v.size < 5})
 
 
+# --------------------------------------------------------------------------
+# case: molecules -- harmonic bonds (interactions/bonds.py) with the bonded
+# pairs excluded from the pair potential's neighbour list, as the reference's
+# examples/LJchain.py sets them up: chains of 10 beads on gamdpy's simple
+# cubic positions, two bond types (r0, k) alternating along the chains
+# --------------------------------------------------------------------------
+CHAIN_BONDS = [[1.0, 3000.0], [1.1, 2000.0]]
+
+
+class _KernelCuda:
+    """The running simulated kernel's cuda module.  The reference's bond
+    calculator (interactions/bonds.py:102-135) is compiled with numba.njit,
+    so under the simulator its ``cuda`` global is the module-level API, which
+    has no per-thread local arrays; this proxy hands it the kernel's own."""
+
+    def __getattr__(self, name):
+        from numba import cuda
+        from numba.cuda.simulator.kernel import _get_kernel_context
+        ctx = _get_kernel_context()
+        return getattr(ctx if ctx is not None else cuda, name)
+
+
+def chain_system(gp, n, rho, seed):
+    import gamdpy.interactions.bonds as bonds_module
+    bonds_module.cuda = _KernelCuda()
+    conf = gp.Configuration(D=3, compute_flags={"lapU": True, "Fsq": True})
+    conf.make_positions(N=n, rho=rho)
+    conf["m"] = 1.0
+    conf.randomize_velocities(temperature=1.0, seed=seed)
+    indices = [[i, i + 1, i % 2] for i in range(n - 1) if i % 10 != 9]
+    bonds = gp.Bonds(gp.harmonic_bond_function, CHAIN_BONDS, indices)
+    excl = bonds.get_exclusions(conf)
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon), params=[1.0, 1.0, 2.5],
+                          exclusions=excl, max_num_nbs=300)
+    return conf, bonds, excl, pp, np.array(indices, np.int32)
+
+
+def chain_eval_case(name, n, nblist_kind):
+    gp = _import_gamdpy_cached()
+    conf, bonds, excl, pp, indices = chain_system(gp, n, 1.0, seed=4)
+    cp = plan(nblist_kind, 0.5)
+    flags = gp.get_default_compute_flags()
+    flags.update({"lapU": True, "Fsq": True})
+    kernel, iparams = gp.add_interactions_list(conf, [pp, bonds], compute_plan=cp, compute_flags=flags)
+    conf.copy_to_device()
+    t0 = time.time()
+    kernel(0, conf.d_vectors, conf.d_scalars, conf.d_ptype, conf.simbox.d_data, iparams)
+    conf.copy_to_host()
+    nbl = pp.nblist.d_nblist.copy_to_host()
+    counts, flat = sorted_csr(nbl)
+    print(f"{name}: {time.time() - t0:.1f}s  N={n} mean nbs={counts.mean():.2f}")
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), r=conf["r"], box=conf.simbox.lengths, v=conf["v"],
+                        bond_indices=indices, bond_params=np.array(CHAIN_BONDS, np.float32), exclusions=excl,
+                        nblist=nblist_kind, skin=np.float32(0.5), nb_counts=counts, nb_flat=flat, f=conf["f"],
+                        U=conf["U"], W=conf["W"], lapU=conf["lapU"])
+
+
+def case_chain200_bonds():
+    chain_eval_case("chain200_bonds", 200, "N squared")
+
+
+def case_chain1200_cells():
+    chain_eval_case("chain1200_cells", 1200, "linked lists")
+
+
+def case_chain200_nve():
+    """8 NVE steps (dt 0.002) of the chain system through Simulation with
+    [PairPotential, Bonds], ScalarSaver every 2 steps."""
+    gp = _import_gamdpy_cached()
+    conf, bonds, excl, pp, indices = chain_system(gp, 200, 1.0, seed=4)
+    r0, v0 = conf["r"].copy(), conf["v"].copy()
+    t0 = time.time()
+    sim = gp.Simulation(conf, [pp, bonds], gp.integrators.NVE(dt=0.002), [gp.ScalarSaver(2)], num_timeblocks=1,
+                        steps_per_timeblock=8, compute_plan=plan("N squared", 0.5), storage="memory", timing=False)
+    for _ in sim.run_timeblocks():
+        pass
+    print(f"chain200_nve: {time.time() - t0:.1f}s")
+    np.savez_compressed(os.path.join(HERE, "chain200_nve.npz"), r0=r0, v0=v0, box=conf.simbox.lengths,
+                        bond_indices=indices, bond_params=np.array(CHAIN_BONDS, np.float32), exclusions=excl,
+                        dt=np.float32(0.002), steps=8, every=2, r=conf["r"], v=conf["v"], f=conf["f"],
+                        r_im=conf.r_im, U=conf["U"], W=conf["W"], scalars=sim.output["scalars"],
+                        scalar_names=np.array(sim.output.attrs["scalar_names"]))
+
+
 # cases that must see compiled numba (no simulator) run with simulator=False
 NO_SIMULATOR = {"known_answers", "rdf_typed"}
 
@@ -401,6 +485,9 @@ CASES = {
     "rdf_typed": case_rdf_typed,
     "rdf": case_rdf,
     "sq": case_sq,
+    "chain200_bonds": case_chain200_bonds,
+    "chain1200_cells": case_chain1200_cells,
+    "chain200_nve": case_chain200_nve,
 }
 
 if __name__ == "__main__":

@@ -123,3 +123,25 @@ def test_workload_builders():
     assert (c.ptype == 1).sum() == 2048 // 5
     assert np.all(np.abs(c["r"]) <= c.simbox.lengths / 2 + 1e-6)
     assert abs(np.sum(c["v"] ** 2) / (3 * (c.N - 1)) - 0.45) < 1e-4
+
+
+def test_make_positions_equals_gamdpy():
+    """Configuration.make_positions reproduces gamdpy's positions (the chain
+    fixture was made with them) bit for bit."""
+    d = golden("chain200_bonds")
+    c = gp.Configuration(D=3)
+    c.make_positions(N=200, rho=1.0)
+    assert np.array_equal(c["r"], d["r"])
+    assert np.array_equal(c.simbox.lengths, d["box"])
+
+
+def test_bond_exclusions_equal_gamdpy():
+    """Bonds.get_exclusions builds gamdpy's (N, 21) table (bonds.py:137-150)."""
+    d = golden("chain200_bonds")
+    c = gp.Configuration(D=3)
+    c.make_positions(N=200, rho=1.0)
+    bonds = gp.Bonds(gp.harmonic_bond_function, d["bond_params"].tolist(), d["bond_indices"].tolist())
+    assert np.array_equal(bonds.get_exclusions(c), d["exclusions"])
+    u, s, umm = gp.harmonic_bond_function(np.float32(1.2), [1.0, 3000.0])
+    assert np.isclose(u, 0.5 * 3000 * 0.2 ** 2, rtol=1e-6) and np.isclose(s, -3000 * 0.2 / 1.2, rtol=1e-6)
+    assert umm == 3000.0

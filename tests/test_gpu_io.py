@@ -17,7 +17,7 @@ def _sim(n=4000, flags=None):
     plan = {"pb": 64, "tp": 1, "lanes": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
             "nblist": "linked lists"}
     sim = gp.Simulation(conf, workloads.ka_pair_potential(), gp.integrators.NVT(temperature=0.45, tau=0.2, dt=0.005),
-                        [gp.ScalarSaver(8)], num_timeblocks=2, steps_per_timeblock=32, compute_plan=plan,
+                        [gp.ScalarSaver(8, flags)], num_timeblocks=2, steps_per_timeblock=32, compute_plan=plan,
                         storage="memory")
     return conf, sim
 

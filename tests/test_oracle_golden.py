@@ -181,3 +181,23 @@ def test_calc_dynamics_restatement_vs_gamdpy(oracle, tag):
     np.testing.assert_allclose(res["times"], d[f"{tag}_times"], rtol=1e-12)
     for k in ("msd", "alpha2", "Fs"):
         np.testing.assert_allclose(res[k], d[f"{tag}_{k}"], rtol=1e-12, atol=1e-12)
+
+
+def test_oracle_molecules_vs_gamdpy(oracle):
+    """The oracle's exclusion filter and bond terms against gamdpy's chain
+    fixture: the N^2 list without the bonded pairs equals gamdpy's list, and
+    pair forces on it plus the bond terms equal gamdpy's forces and energies."""
+    d = golden("chain200_bonds")
+    r, box = d["r"], d["box"]
+    full, _ = oracle.nblist_nsq(r, box, float(np.float32(2.5) + np.float32(0.5)), 300, fma=0)
+    nbl = oracle.exclude(full, d["exclusions"])
+    counts = nbl[:, -1]
+    flat = np.concatenate([np.sort(nbl[i, : counts[i]]) for i in range(len(nbl))])
+    assert np.array_equal(counts, d["nb_counts"]) and np.array_equal(flat, d["nb_flat"])
+    table = oracle.param_table([np.float32(1.0), np.float32(1.0), np.float32(2.5)])
+    pair = oracle.forces(r, np.zeros(len(r), np.int32), box, table, nbl, fma=0)
+    bond = oracle.bond_terms(r, box, d["bond_indices"], d["bond_params"])
+    for k in ("f", "U", "W", "lapU"):
+        got = np.asarray(pair[k], np.float64) + bond[k]
+        ref = d[k].astype(np.float64)
+        assert np.sqrt(np.mean((got - ref) ** 2) / np.mean(ref ** 2)) < 1e-5, k
