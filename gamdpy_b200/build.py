@@ -27,17 +27,33 @@ def _stale(target, deps):
     return any(os.path.getmtime(d) > t for d in deps)
 
 
+def _includes(path, seen=None):
+    """The file and every local header it includes, recursively."""
+    seen = set() if seen is None else seen
+    path = os.path.normpath(path)
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith("#include \""):
+                _includes(os.path.join(os.path.dirname(path), line.split('"')[1]), seen)
+    return seen
+
+
 def build(verbose=False, force=False):
-    deps = [os.path.join(CSRC, s) for s in SOURCES] + [
-        os.path.join(CSRC, h) for h in ("gdb_internal.cuh", "md_phases.cuh", "md_kernels.cuh", "md_cluster.cuh", "md_bricks.cuh")
-    ] + [os.path.join(HERE, "..", "include", "gamdb200.h")]
-    if not force and not _stale(LIB, deps):
-        return LIB
+    """Compile the translation units whose sources or included headers are
+    newer than their objects (all of them with force), then link."""
     objs, cmds = [], []
     for src in SOURCES:
+        path = os.path.join(CSRC, src)
         obj = os.path.join(CSRC, src.replace(".cu", ".o"))
-        cmds.append([NVCC, *ARCH, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+        if force or _stale(obj, _includes(path)):
+            cmds.append([NVCC, *ARCH, *FLAGS, "-c", path, "-o", obj])
+    if not cmds and not _stale(LIB, objs):
+        return LIB
     # translation units compile in parallel
     procs = []
     for cmd in cmds:
