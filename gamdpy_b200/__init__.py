@@ -3,7 +3,7 @@
 Drop-in for the part of gamdpy's API that runs the simulation hot path --
 pair-potential forces/virial/energy over N^2 or cell neighbour lists (with
 exclusions, plus harmonic bonds for molecules), the NVE,
-NVT (Nose-Hoover) and NVT_Langevin steps, ScalarSaver / MomentumReset /
+NVT (Nose-Hoover), NVT_Langevin and NPT_Atomic steps, ScalarSaver / MomentumReset /
 ConfigurationSaver, and the RDF and S(q) calculators.  The compute path is the hand-written
 sm_100a CUDA library libgamdb200.so (include/gamdb200.h), called through
 ctypes.  There is no CPU fallback: operations raise if the library is missing.

@@ -36,7 +36,7 @@ INTEGRATOR_NVE = 0
 INTEGRATOR_NVT = 1
 TFUNC_CONSTANT = 0
 TFUNC_RAMP = 1
-NUM_SCALARS = 5  # U, W, lapU, K, Fsq
+NUM_SCALARS = 6  # U, W, lapU, K, Fsq, Vol (NPT_Atomic runs)
 
 # every exported entry point with its argument types (order as in gamdb200.h)
 _P = ctypes.c_void_p
@@ -46,6 +46,7 @@ _d = ctypes.c_double
 SIGNATURES = {
     "gdb_version": ([], _i),
     "gdb_device_count": ([_P], _i),
+    "gdb_device_name": ([_i, ctypes.c_char_p, _i], _i),
     "gdb_sim_create": ([_i, _i, _i, _P], _i),
     "gdb_sim_destroy": ([_P], _i),
     "gdb_set_box": ([_P, _P], _i),
@@ -67,6 +68,7 @@ SIGNATURES = {
     "gdb_set_runtime_actions": ([_P, _i, _i], _i),
     "gdb_set_configuration_saver": ([_P, _i], _i),
     "gdb_get_saved_configurations": ([_P, _P, _i], _i),
+    "gdb_get_saved_boxes": ([_P, _P, _i], _i),
     "gdb_eval_forces": ([_P], _i),
     "gdb_sim_run": ([_P, _d, _i, _P], _i),
     "gdb_set_trace": ([_P, _i], _i),
@@ -84,12 +86,17 @@ SIGNATURES = {
     "gdb_sq_update": ([_P, _i, _P, _P, _P, _P], _i),
     "gdb_set_integrator_langevin": ([_P, _f, _f, ctypes.c_uint64, _i, _P], _i),
     "gdb_get_langevin_state": ([_P, _P, _P], _i),
+    "gdb_set_integrator_npt": ([_P, _f, _f, _f, _i, _P, _i, _P], _i),
+    "gdb_get_npt_state": ([_P, _P, _P], _i),
+    "gdb_set_npt_state": ([_P, _P, _P], _i),
+    "gdb_get_box": ([_P, _P], _i),
     "gdb_calc_dynamics": ([_i, _i, _i, _P, _P, _i, _P, _i, _P, _i, _P, _P, _P, _P], _i),
     "gdb_last_analysis_ms": ([_P, _P], _i),
     "gdb_rdf_compute": ([_i, _P, _P, _P, _i, _i, _d, _P], _i),
     "gdb_sq_compute": ([_i, _P, _P, _P, _i, _P, _P, _P], _i),
     "gdb_sq_compute_noalloc": ([_i, _P, _P, _P, _i, _P, _i, _P, _P, _P], _i),
     "gdb_batch_create": ([_P, _i, _i, _P], _i),
+    "gdb_batch_create_ex": ([_P, _i, _i, _i, _i, _P], _i),
     "gdb_batch_run": ([_P, _d, _i, _P], _i),
     "gdb_batch_destroy": ([_P], _i),
     "gdb_batch_get_last_error": ([_P, ctypes.c_char_p, _i], _i),
@@ -193,6 +200,12 @@ def pinned_empty(shape, dtype):
     return np.frombuffer(owner, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
 
 
+def device_name(device=0):
+    buf = ctypes.create_string_buffer(256)
+    check(lib().gdb_device_name(int(device), buf, 256), None, "gdb_device_name")
+    return buf.value.decode()
+
+
 class Sim:
     """Owner of one gdb_sim handle (device state of one configuration)."""
 
@@ -201,6 +214,7 @@ class Sim:
         check(lib().gdb_sim_create(int(n), int(ntypes), int(device), ctypes.byref(self.h)), None,
               "gdb_sim_create")
         self.n, self.ntypes = int(n), int(ntypes)
+        self.device = int(device)
 
     def __del__(self):
         try:
@@ -313,6 +327,29 @@ class Sim:
         self.call("gdb_set_integrator_langevin", float(dt), float(alpha), int(seed) & 0xFFFFFFFFFFFFFFFF, int(tfunc),
                   ptr(tp))
 
+    def set_npt(self, dt, mass_t, mass_p, tfunc, tparams, pfunc, pparams):
+        tp = f32(np.resize(np.asarray(tparams, np.float32), 4))
+        pp = f32(np.resize(np.asarray(pparams, np.float32), 4))
+        self.call("gdb_set_integrator_npt", float(dt), float(mass_t), float(mass_p), int(tfunc), ptr(tp), int(pfunc),
+                  ptr(pp))
+
+    def npt_state(self):
+        """(thermostat_state (2,), barostat_state (3,)) float32."""
+        ts = np.zeros(2, np.float32)
+        bs = np.zeros(3, np.float32)
+        self.call("gdb_get_npt_state", ptr(ts), ptr(bs))
+        return ts, bs
+
+    def set_npt_state(self, ts, bs):
+        ts = f32(ts, (2,))
+        bs = f32(bs, (3,))
+        self.call("gdb_set_npt_state", ptr(ts), ptr(bs))
+
+    def box(self):
+        b = np.zeros(3, np.float32)
+        self.call("gdb_get_box", ptr(b))
+        return b
+
     def langevin_state(self):
         """(states (n, 2) uint64, old_beta (n, 3) float32) in user order."""
         st = np.zeros((self.n, 2), np.uint64)
@@ -334,6 +371,11 @@ class Sim:
 
     def set_configuration_saver(self, conf_per_block):
         self.call("gdb_set_configuration_saver", int(conf_per_block))
+
+    def saved_boxes(self, conf_per_block):
+        out = np.zeros((conf_per_block, 3), np.float32)
+        self.call("gdb_get_saved_boxes", ptr(out), int(conf_per_block))
+        return out
 
     def saved_configurations(self, conf_per_block):
         out = np.zeros((conf_per_block, 2, self.n, 3), np.float32)
@@ -466,11 +508,12 @@ def sq_compute(r, box, n_vectors, ff=None):
 class BatchHandle:
     """Owner of one gdb_batch handle: several Sim handles advanced together."""
 
-    def __init__(self, sims, particles_per_cta=0):
+    def __init__(self, sims, particles_per_cta=0, clg_particles_per_cta=0, clg_tp=0):
         self.sims = list(sims)
         arr = (ctypes.c_void_p * len(self.sims))(*[s.h.value for s in self.sims])
         self.h = ctypes.c_void_p()
-        rc = lib().gdb_batch_create(arr, len(self.sims), int(particles_per_cta), ctypes.byref(self.h))
+        rc = lib().gdb_batch_create_ex(arr, len(self.sims), int(particles_per_cta), int(clg_particles_per_cta),
+                                       int(clg_tp), ctypes.byref(self.h))
         if rc != GDB_OK:
             buf = ctypes.create_string_buffer(512)
             lib().gdb_batch_get_last_error(None, buf, 512)

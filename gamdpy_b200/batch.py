@@ -25,13 +25,16 @@ class SimulationBatch:
 
     All simulations need the same device, number of particle types,
     integrator kind, ``steps_per_timeblock`` and ``dt`` (the timeblock's start
-    time is shared).  ``particles_per_cta`` shapes the clusters (about that
-    many particles per CTA, at most 256, up to 16 CTAs per system; 0 = the
-    single-system default, so every system gives the same bits as alone);
-    ``autotune`` picks it by timing.
+    time is shared).  ``particles_per_cta`` shapes the shared-memory clusters
+    of systems up to 4096 particles (about that many particles per CTA, at
+    most 256, up to 16 CTAs per system; 0 = the single-system default, so
+    every system gives the same bits as alone); ``clg_particles_per_cta`` and
+    ``clg_tp`` the global-memory clusters of larger systems (particles per
+    1024-thread CTA, 0 = fit one wave; lanes per particle, 0 = 1).
+    ``autotune`` picks all three by timing.
     """
 
-    def __init__(self, simulations, particles_per_cta=0):
+    def __init__(self, simulations, particles_per_cta=0, clg_particles_per_cta=0, clg_tp=0):
         self.simulations = list(simulations)
         if not self.simulations:
             raise ValueError("SimulationBatch needs at least one Simulation")
@@ -46,8 +49,19 @@ class SimulationBatch:
         self.dt = s0.dt
         self.num_blocks = min(s.num_blocks for s in self.simulations)
         self.particles_per_cta = int(particles_per_cta)
-        self._batch = _lib.BatchHandle([s._sim for s in self.simulations], self.particles_per_cta)
+        self.clg_particles_per_cta = int(clg_particles_per_cta)
+        self.clg_tp = int(clg_tp)
+        self._batch = self._handle()
         self.timing_blocks = None
+
+    def _handle(self):
+        return _lib.BatchHandle([s._sim for s in self.simulations], self.particles_per_cta,
+                                self.clg_particles_per_cta, self.clg_tp)
+
+    @property
+    def shape(self):
+        """(particles_per_cta, clg_particles_per_cta, clg_tp) of the handle."""
+        return self.particles_per_cta, self.clg_particles_per_cta, self.clg_tp
 
     @property
     def num_particles(self):
@@ -105,34 +119,55 @@ class SimulationBatch:
                 f"Steps : {len(self.timing_blocks)} * {self.steps_per_block}  TPS: {tps:.3e}  "
                 f"atom-steps/s: {tps * self.num_particles:.3e}\n")
 
-    def autotune(self, candidates=(64, 96, 128, 192, 256), steps=None, verbose=False):
-        """Pick ``particles_per_cta`` by timing short batched runs; the
-        configurations and thermostat states are restored afterwards."""
+    def autotune(self, candidates=(0, 64, 128, 192, 256), clg_candidates=(0, 2048, 4096, 8192),
+                 clg_tps=(1, 2, 4), steps=None, verbose=False):
+        """Pick the batch's shape by timing short batched runs, one axis at a
+        time (shared-memory clusters' particles per CTA, then the
+        global-memory clusters' particles per CTA, then their lanes per
+        particle), each axis kept at its best before the next.  The
+        configurations and thermostat states are restored afterwards.
+        Returns the chosen (particles_per_cta, clg_particles_per_cta, clg_tp)."""
         steps = steps or min(self.steps_per_block, 256)
         saved = []
         for s in self.simulations:
             c = s.configuration
-            xi = s.integrator.thermostat_state.copy() if isinstance(s.integrator, NVT) else None
+            # the device's xi: the host copy is behind it until a block ends
+            xi = s._sim.thermostat_state() if isinstance(s.integrator, NVT) else None
             saved.append((c["r"].copy(), c["v"].copy(), c.r_im.copy(), xi))
-        best = None
-        for ppc in candidates:
-            self._batch = _lib.BatchHandle([s._sim for s in self.simulations], int(ppc))
-            for s in self.simulations:
-                s.configuration.copy_to_device()
+
+        def restore():
+            for s, (r, v, rim, xi) in zip(self.simulations, saved):
+                c = s.configuration
+                c["r"], c["v"] = r, v
+                c.r_im[:] = rim
+                if xi is not None:
+                    s.integrator.thermostat_state[:] = xi
+                    s._sim.set_thermostat_state(xi)
+                c.copy_to_device()
+
+        def timed(shape):
+            self.particles_per_cta, self.clg_particles_per_cta, self.clg_tp = shape
+            self._batch = self._handle()
+            restore()
             self.integrate_self(0.0, steps)
             ms = self.integrate_self(0.0, steps)
             if verbose:
-                print(f"autotune: particles_per_cta={ppc}: {steps / ms * 1000:.1f} TPS")
-            if best is None or ms < best[0]:
-                best = (ms, ppc)
-        self.particles_per_cta = best[1]
-        self._batch = _lib.BatchHandle([s._sim for s in self.simulations], self.particles_per_cta)
-        for s, (r, v, rim, xi) in zip(self.simulations, saved):
-            c = s.configuration
-            c["r"], c["v"] = r, v
-            c.r_im[:] = rim
-            if xi is not None:
-                s.integrator.thermostat_state[:] = xi
-                s._sim.set_thermostat_state(xi)
-            c.copy_to_device()
-        return self.particles_per_cta
+                print(f"autotune: shape={shape}: {steps / ms * 1000:.1f} TPS")
+            return ms
+
+        best = (self.particles_per_cta, self.clg_particles_per_cta, self.clg_tp)
+        best_ms = timed(best)
+        for axis, cands in ((0, candidates), (1, clg_candidates), (2, clg_tps)):
+            for c in cands:
+                shape = list(best)
+                shape[axis] = int(c)
+                shape = tuple(shape)
+                if shape == best:
+                    continue
+                ms = timed(shape)
+                if ms < best_ms:
+                    best, best_ms = shape, ms
+        self.particles_per_cta, self.clg_particles_per_cta, self.clg_tp = best
+        self._batch = self._handle()
+        restore()
+        return best

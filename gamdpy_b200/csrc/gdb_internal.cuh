@@ -62,6 +62,10 @@ struct DevCtrl {
     int pending[2];    // momentum shift pending, by step parity
     float shift[2][4]; // momentum shift vector, by step parity
     float xi;          // Nose-Hoover friction (NVT.thermostat_state[0])
+    float npt_ts0;     // NPT_Atomic: thermostat state p_xi/Q
+    float npt_bs0;     // NPT_Atomic: barostat state p_eps/W
+    float npt_vol;     // NPT_Atomic: volume (barostat_state[2])
+    float box[3];      // current box lengths (changed by NPT_Atomic steps)
     float sumK;        // last kinetic-energy sum (float copy, NVT.thermostat_state[1] analogue)
     double time_zero;  // simulated time at the start of the timeblock
     double evalU, evalW;  // sums of the last force-only evaluation

@@ -57,6 +57,9 @@ char g_lib_error[512] = "";
 // N^2 build: N 2048 56.6k vs 70.9k, N 4096 46.0k vs 43.0k, N 8192 38.2k vs
 // 23.2k).  GDB_NSQ_AUTO=<N> moves the limit, 0 switches it off.
 constexpr int NSQ_AUTO_MAX = 3072;
+// persistent N^2 builds stage the positions in shared memory up to this N
+// (48 KiB, the default dynamic limit)
+constexpr int NSQ_SMEM_MAX = 3072;
 
 // Systems from this many particles take the brick path on the persistent
 // kernel (GDB_BRICK_MIN_N moves it; GDB_BRICKS=0 switches the path off).
@@ -87,6 +90,10 @@ struct gdb_sim {
     float dt = 0.005f, tau = 0.2f, omega2 = 0;
     int tfunc = 0;
     float tparams[4] = {0, 0, 0, 0};
+    // NPT_Atomic: masses without the temperature factor, target pressure
+    float npt_mass_t = 0.f, npt_mass_p = 0.f;
+    int pfunc = 0;
+    float pparams[4] = {0, 0, 0, 0};
     int scalar_every = 0, momentum_every = 0;
     // device buffers
     float4 *pos[2] = {nullptr, nullptr}, *vel = nullptr, *frc = nullptr, *rref = nullptr;
@@ -432,6 +439,7 @@ static int ensure_nblist(gdb_sim *h) {
         // fits the stage with a quarter to spare
         const double per_cell = (double)h->n / ((double)nc[0] * nc[1] * nc[2]);
         const bool use = h->bricks_req && h->bricks_ok && h->staged_ok && h->persistent && !h->excl &&
+                         h->integ != GDB_INTEGRATOR_NPT &&
                          !h->bond_cnt &&
                          h->n >= h->brick_min_n && h->n > h->nsq_auto_max && nc[0] >= BRICK_W &&
                          nc[1] >= BRICK_W && nc[2] >= BRICK_W &&
@@ -480,6 +488,7 @@ static int ensure_partials(gdb_sim *h, int nblocks) {
 
 static SimArgs make_args(gdb_sim *h) {
     SimArgs a;
+    a.nsq_smem = 0;
     a.pos0 = h->pos[0];
     a.pos1 = h->pos[1];
     a.vel = h->vel;
@@ -505,6 +514,7 @@ static SimArgs make_args(gdb_sim *h) {
     a.partials = h->partials;
     a.rows = h->rows;
     a.conf = h->conf;
+    a.conf_box = h->conf ? h->conf + (size_t)h->conf_per_block * 2 * h->n * 3 : nullptr;
     a.ctrl = h->ctrl;
     a.n = h->n;
     a.stride = h->stride;
@@ -535,6 +545,27 @@ static SimArgs make_args(gdb_sim *h) {
     a.tp1 = h->tparams[1];
     a.tp2 = h->tparams[2];
     a.tp3 = h->tparams[3];
+    a.npt_mass_t = h->npt_mass_t;
+    a.npt_mass_p = h->npt_mass_p;
+    a.pfunc = h->pfunc;
+    a.pp0 = h->pparams[0];
+    a.pp1 = h->pparams[1];
+    a.pp2 = h->pparams[2];
+    a.pp3 = h->pparams[3];
+    a.min_cell = (h->max_cut + h->skin) / 2.0f;  // nblist_linked_lists.py:36
+    a.ncx_max = h->nc[0];
+    a.ncy_max = h->nc[1];
+    a.ncz_max = h->nc[2];
+    if (h->integ == GDB_INTEGRATOR_NPT && h->nb_kind == GDB_NBLIST_CELLS && a.ncell > 0) {
+        // the grid of the current box, within the allocated one
+        int nc[3];
+        for (int k = 0; k < 3; k++) nc[k] = std::min(h->nc[k], std::max(1, (int)(h->box[k] / a.min_cell)));
+        a.ncx = nc[0];
+        a.ncy = nc[1];
+        a.ncz = nc[2];
+        a.ncell = nc[0] * nc[1] * nc[2];
+        a.nchunks = (a.ncell + SCAN_CHUNK - 1) / SCAN_CHUNK;
+    }
     a.every = h->scalar_every;
     a.reset_every = h->momentum_every;
     a.nrows = h->rows ? h->rows_cap : 0;
@@ -604,9 +635,9 @@ static int enqueue_step(gdb_sim *h, int mode) {
 }
 
 // Grid of the persistent kernel: every block resident (cooperative launch).
-static int run_grid(gdb_sim *h, const void *fn, int *grid) {
+static int run_grid(gdb_sim *h, const void *fn, int *grid, size_t dsmem = 0) {
     int occ = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GDB_BLOCK, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, fn, GDB_BLOCK, dsmem));
     if (occ < 1) return set_err(h, GDB_ERR_CUDA, "persistent kernel cannot be resident");
     const int needed = grid_for((long long)h->n * h->tp);
     *grid = std::min(std::min(needed, occ * h->num_sms), 64 * BAR_GROUP);
@@ -642,10 +673,6 @@ static int launch_run(gdb_sim *h, int steps, int do_eval) {
     const void *fn = h->ntypes == 1   ? run_kernel_nt1(h->tp, h->integ)
                      : h->ntypes == 2 ? run_kernel_nt2(h->tp, h->integ)
                                       : run_kernel_ntg(h->tp, h->integ);
-    int grid = 0;
-    int rc = run_grid(h, fn, &grid);
-    if (rc) return rc;
-    if ((rc = ensure_partials(h, grid))) return rc;
     SimArgs a = make_args(h);
     if (a.nb_kind == GDB_NBLIST_CELLS && h->n <= h->nsq_auto_max) {
         // same neighbour sets as the cell build (in another order), one phase
@@ -654,9 +681,18 @@ static int launch_run(gdb_sim *h, int steps, int do_eval) {
         a.nchunks = 0;
         a.nbx = a.nby = a.nbz = 0;
     }
+    // small N^2 systems: every block stages the positions for the list build
+    const size_t dsmem = (a.nb_kind == GDB_NBLIST_NSQ && h->n <= NSQ_SMEM_MAX) ? (size_t)h->n * sizeof(float4) : 0;
+    a.nsq_smem = dsmem > 0;
+    // static plus dynamic shared memory above 48 KiB needs the opt-in
+    if (dsmem > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+    int grid = 0;
+    int rc = run_grid(h, fn, &grid, dsmem);
+    if (rc) return rc;
+    if ((rc = ensure_partials(h, grid))) return rc;
     int cur0 = h->cur, ns = steps, ev = do_eval;
     void *args[] = {(void *)&a, (void *)&h->table, (void *)&cur0, (void *)&ns, (void *)&ev};
-    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(GDB_BLOCK), args, 0, h->st));
+    CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(GDB_BLOCK), args, dsmem, h->st));
     h->cur ^= (steps & 1);
     return GDB_OK;
 }
@@ -813,6 +849,15 @@ int gdb_device_count(int *count) {
     return GDB_OK;
 }
 
+int gdb_device_name(int device, char *buf, int n) {
+    gdb_sim *h = nullptr;
+    if (!buf || n < 1) return set_err(h, GDB_ERR_ARG, "gdb_device_name: bad arguments");
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    snprintf(buf, (size_t)n, "%s", prop.name);
+    return GDB_OK;
+}
+
 int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     gdb_sim *h = nullptr;
     if (!out || n < 1 || ntypes < 1 || ntypes > GDB_MAX_TYPES)
@@ -915,12 +960,13 @@ int gdb_set_box(gdb_sim *h, const float lengths[3]) {
         if (!(lengths[k] > 0.f)) return set_err(h, GDB_ERR_ARG, "gdb_set_box: non-positive length");
     memcpy(h->box, lengths, sizeof(h->box));
     free_graphs(h);
+    CK(cudaSetDevice(h->dev));
+    CK(cudaMemcpyAsync(h->ctrl->box, h->box, sizeof(h->box), cudaMemcpyHostToDevice, h->st));
     if (h->uploaded) {
-        CK(cudaSetDevice(h->dev));
         int one = 1;
         CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
-        CK(cudaStreamSynchronize(h->st));
     }
+    CK(cudaStreamSynchronize(h->st));
     return GDB_OK;
 }
 
@@ -955,6 +1001,7 @@ int gdb_upload_state(gdb_sim *h, const float *r, const float *v, const float *m,
     CK(cudaFreeAsync(stage, h->st));
     int one = 1;
     CK(cudaMemcpyAsync(&h->ctrl->rebuild, &one, sizeof(int), cudaMemcpyHostToDevice, h->st));
+    CK(cudaMemcpyAsync(h->ctrl->box, h->box, sizeof(h->box), cudaMemcpyHostToDevice, h->st));
     CK(cudaStreamSynchronize(h->st));
     h->uploaded = true;
     return GDB_OK;
@@ -1304,6 +1351,69 @@ int gdb_set_thermostat_state(gdb_sim *h, const float state[2]) {
     return GDB_OK;
 }
 
+int gdb_set_integrator_npt(gdb_sim *h, float dt, float mass_t, float mass_p, int tfunc, const float *tparams,
+                           int pfunc, const float *pparams) {
+    if (!h || !(dt > 0.f) || !(mass_t > 0.f) || !(mass_p > 0.f) || !tparams || !pparams)
+        return set_err(h, GDB_ERR_ARG, "gdb_set_integrator_npt: bad arguments");
+    if (tfunc != GDB_TFUNC_CONSTANT && tfunc != GDB_TFUNC_RAMP)
+        return set_err(h, GDB_ERR_UNSUPPORTED, "unsupported temperature function %d", tfunc);
+    if (pfunc != GDB_TFUNC_CONSTANT && pfunc != GDB_TFUNC_RAMP)
+        return set_err(h, GDB_ERR_UNSUPPORTED, "unsupported pressure function %d", pfunc);
+    if (!h->persistent)
+        return set_err(h, GDB_ERR_UNSUPPORTED, "NPT_Atomic runs on the persistent kernel (cooperative launch)");
+    h->integ = GDB_INTEGRATOR_NPT;
+    h->dt = dt;
+    h->npt_mass_t = mass_t;
+    h->npt_mass_p = mass_p;
+    h->tfunc = tfunc;
+    h->pfunc = pfunc;
+    const int nt_ = tfunc == GDB_TFUNC_RAMP ? 4 : 1, np_ = pfunc == GDB_TFUNC_RAMP ? 4 : 1;
+    for (int k = 0; k < 4; k++) {
+        h->tparams[k] = k < nt_ ? tparams[k] : 0.f;
+        h->pparams[k] = k < np_ ? pparams[k] : 0.f;
+    }
+    free_graphs(h);
+    // state as a new NPT_Atomic: zeros, the volume of the box (NPT_Atomic.py:35-36, 49)
+    const float ts[2] = {0.f, 0.f};
+    const float bs[3] = {0.f, 0.f, h->box[0] * h->box[1] * h->box[2]};
+    return gdb_set_npt_state(h, ts, bs);
+}
+
+int gdb_get_npt_state(gdb_sim *h, float ts[2], float bs[3]) {
+    if (!h) return set_err(h, GDB_ERR_ARG, "NULL handle");
+    CK(cudaSetDevice(h->dev));
+    int rc = read_ctrl(h);
+    if (rc) return rc;
+    if (ts) {
+        ts[0] = h->h_ctrl->npt_ts0;
+        ts[1] = 0.f;
+    }
+    if (bs) {
+        bs[0] = h->h_ctrl->npt_bs0;
+        bs[1] = 0.f;
+        bs[2] = h->h_ctrl->npt_vol;
+    }
+    return GDB_OK;
+}
+
+int gdb_set_npt_state(gdb_sim *h, const float ts[2], const float bs[3]) {
+    if (!h) return set_err(h, GDB_ERR_ARG, "NULL handle");
+    CK(cudaSetDevice(h->dev));
+    if (ts) CK(cudaMemcpyAsync(&h->ctrl->npt_ts0, &ts[0], sizeof(float), cudaMemcpyHostToDevice, h->st));
+    if (bs) {
+        CK(cudaMemcpyAsync(&h->ctrl->npt_bs0, &bs[0], sizeof(float), cudaMemcpyHostToDevice, h->st));
+        CK(cudaMemcpyAsync(&h->ctrl->npt_vol, &bs[2], sizeof(float), cudaMemcpyHostToDevice, h->st));
+    }
+    CK(cudaStreamSynchronize(h->st));
+    return GDB_OK;
+}
+
+int gdb_get_box(gdb_sim *h, float lengths[3]) {
+    if (!h || !lengths) return set_err(h, GDB_ERR_ARG, "NULL argument");
+    memcpy(lengths, h->box, sizeof(h->box));
+    return GDB_OK;
+}
+
 int gdb_set_runtime_actions(gdb_sim *h, int scalar_every, int momentum_every) {
     if (!h || scalar_every < 0 || momentum_every < 0) return set_err(h, GDB_ERR_ARG, "bad runtime actions");
     h->scalar_every = scalar_every;
@@ -1319,7 +1429,8 @@ int gdb_set_configuration_saver(gdb_sim *h, int conf_per_block) {
     h->conf = nullptr;
     h->conf_per_block = 0;
     if (conf_per_block > 0) {
-        const size_t bytes = (size_t)conf_per_block * 2 * h->n * 3 * sizeof(float);
+        // frames, then one box row (4 floats) per frame
+        const size_t bytes = ((size_t)conf_per_block * 2 * h->n * 3 + (size_t)conf_per_block * 4) * sizeof(float);
         CK(cudaMalloc(&h->conf, bytes));
         CK(cudaMemset(h->conf, 0, bytes));
         h->conf_per_block = conf_per_block;
@@ -1336,6 +1447,24 @@ int gdb_get_saved_configurations(gdb_sim *h, float *out, int conf_per_block) {
     const size_t bytes = (size_t)conf_per_block * 2 * h->n * 3 * sizeof(float);
     CK(cudaMemcpyAsync(out, h->conf, bytes, cudaMemcpyDeviceToHost, h->st));
     CK(cudaStreamSynchronize(h->st));
+    return GDB_OK;
+}
+
+int gdb_get_saved_boxes(gdb_sim *h, float *out, int conf_per_block) {
+    if (!h || !out) return set_err(h, GDB_ERR_ARG, "NULL argument");
+    if (conf_per_block != h->conf_per_block || !h->conf)
+        return set_err(h, GDB_ERR_STATE, "configuration saver holds %d frames", h->conf_per_block);
+    if (h->integ != GDB_INTEGRATOR_NPT) {
+        // a box that no step changes
+        for (int k = 0; k < conf_per_block; k++) memcpy(out + 3 * k, h->box, 3 * sizeof(float));
+        return GDB_OK;
+    }
+    CK(cudaSetDevice(h->dev));
+    std::vector<float> rows((size_t)conf_per_block * 4);
+    CK(cudaMemcpyAsync(rows.data(), h->conf + (size_t)conf_per_block * 2 * h->n * 3, rows.size() * sizeof(float),
+                       cudaMemcpyDeviceToHost, h->st));
+    CK(cudaStreamSynchronize(h->st));
+    for (int k = 0; k < conf_per_block; k++) memcpy(out + 3 * k, rows.data() + 4 * k, 3 * sizeof(float));
     return GDB_OK;
 }
 
@@ -1396,8 +1525,8 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
     CK(cudaEventRecord(h->ev0, h->st));
     k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);
     CKL();
-    if (h->cluster_ok && h->n <= CL_MAX_N && h->integ != GDB_INTEGRATOR_LANGEVIN && !h->excl && !h->bond_cnt &&
-        cluster_preferred(h)) {
+    if (h->cluster_ok && h->n <= CL_MAX_N && h->integ != GDB_INTEGRATOR_LANGEVIN && h->integ != GDB_INTEGRATOR_NPT &&
+        !h->excl && !h->bond_cnt && cluster_preferred(h)) {
         rc = run_cluster(h, steps);
         if (rc == GDB_OK) {
             CK(cudaEventRecord(h->ev1, h->st));
@@ -1466,6 +1595,7 @@ int gdb_sim_run(gdb_sim *h, double time_zero, int steps, float *ms) {
     }
     CK(cudaEventRecord(h->ev1, h->st));
     if ((rc = read_ctrl(h))) return rc;
+    if (h->integ == GDB_INTEGRATOR_NPT) memcpy(h->box, h->h_ctrl->box, sizeof(h->box));  // the box the run left
     if (ms) CK(cudaEventElapsedTime(ms, h->ev0, h->ev1));
     return status_to_rc(h);
 }
@@ -1720,6 +1850,7 @@ struct gdb_batch {
     std::vector<int> solo;  // too large for a cluster
     int dev = 0, ntypes = 1, integ = 0;
     int clg_tp = 1;
+    int clg_ppc = 4096;  // particles per CTA of the global-memory clusters
     cudaStream_t st = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     char err[512] = "";
@@ -1803,9 +1934,17 @@ static cudaError_t launch_run_clusters(const void *fn, const ClusterRunJob *d_jo
 extern "C" {
 
 int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb_batch **out) {
+    return gdb_batch_create_ex(sims, count, particles_per_cta, 0, 0, out);
+}
+
+int gdb_batch_create_ex(gdb_sim *const *sims, int count, int particles_per_cta, int clg_particles_per_cta,
+                        int clg_tp, gdb_batch **out) {
     gdb_batch *b = nullptr;
-    if (!sims || count < 1 || !out) return bset(b, GDB_ERR_ARG, "gdb_batch_create: bad arguments");
+    if (!sims || count < 1 || !out || clg_particles_per_cta < 0 || clg_tp < 0 ||
+        (clg_tp != 0 && clg_tp != 1 && clg_tp != 2 && clg_tp != 4 && clg_tp != 8))
+        return bset(b, GDB_ERR_ARG, "gdb_batch_create: bad arguments");
     b = new gdb_batch();
+    if (clg_tp > 0) b->clg_tp = clg_tp;
     b->sims.assign(sims, sims + count);
     b->dev = sims[0]->dev;
     b->ntypes = sims[0]->ntypes;
@@ -1820,6 +1959,10 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
         if (h->integ == GDB_INTEGRATOR_LANGEVIN) {
             batch_free(b);
             return bset(nullptr, GDB_ERR_UNSUPPORTED, "gdb_batch_create: Langevin systems run one at a time");
+        }
+        if (h->integ == GDB_INTEGRATOR_NPT) {
+            batch_free(b);
+            return bset(nullptr, GDB_ERR_UNSUPPORTED, "gdb_batch_create: NPT_Atomic systems run one at a time");
         }
         for (int q = 0; q < k; q++)
             if (sims[q] == h) {
@@ -1843,6 +1986,9 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
     std::vector<int> order(count);
     for (int k = 0; k < count; k++) order[k] = k;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return sims[x]->n > sims[y]->n; });
+    // which systems fit a shared-memory cluster
+    std::vector<char> in_smem(count, 0);
+    long long p_smem = 0, p_glob = 0;
     for (int k : order) {
         gdb_sim *h = sims[k];
         int nc[3];
@@ -1850,7 +1996,41 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
         int C, tp, cap, pingpong, sorted;
         size_t smem;
         cluster_shape(h->n, particles_per_cta, &C, &tp);
-        if (h->cluster_ok && h->n <= CL_MAX_N && !h->excl && !h->bond_cnt &&
+        in_smem[k] = h->cluster_ok && h->n <= CL_MAX_N && !h->excl && !h->bond_cnt &&
+                     cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &pingpong, &sorted, &smem);
+        if (in_smem[k])
+            p_smem += h->n;
+        else if (h->n <= CLG_MAX_N)
+            p_glob += h->n;
+    }
+    // particles per CTA of the global-memory clusters: given, or the smallest
+    // (from 4096, in steps of 1.25x) whose CTAs (one per SM, 1 to 16 a system)
+    // fit the SMs left for them by the shared-memory clusters' share of the
+    // particles, so that the launch is one wave
+    if (clg_particles_per_cta > 0) {
+        b->clg_ppc = std::max(256, clg_particles_per_cta);
+    } else if (p_glob > 0) {
+        const int sms = std::max(1, sims[0]->num_sms);
+        const int budget = std::max(1, (int)((double)sms * (double)p_glob / (double)(p_glob + p_smem)));
+        int ppc = 4096;
+        for (int it = 0; it < 40; it++) {
+            long long ctas = 0;
+            for (int k : order)
+                if (!in_smem[k] && sims[k]->n <= CLG_MAX_N)
+                    ctas += std::min(16, (sims[k]->n + ppc - 1) / ppc);
+            if (ctas <= budget || ppc >= CLG_MAX_N) break;
+            ppc = (int)(ppc * 1.25);
+        }
+        b->clg_ppc = ppc;
+    }
+    for (int k : order) {
+        gdb_sim *h = sims[k];
+        int nc[3];
+        cluster_grid_of(h, nc);
+        int C, tp, cap, pingpong, sorted;
+        size_t smem;
+        cluster_shape(h->n, particles_per_cta, &C, &tp);
+        if (in_smem[k] &&
             cluster_plan(h->n, C, nc[0] * nc[1] * nc[2], h->max_nbs, &cap, &pingpong, &sorted, &smem)) {
             gdb_batch::Group *g = batch_group(b, 0, C, tp);
             g->idx.push_back(k);
@@ -1864,11 +2044,8 @@ int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb
                 batch_free(b);
                 return rc;
             }
-            // about 4096 particles per CTA (four per lane), 1 to 16 CTAs
-            // (measured on B200, 128-replica sweep: 954 / 1048 / 1134 / 1272 /
-            // 1084 MATS at 512 / 1024 / 2048 / 4096 / 8192 per CTA)
-            int c = 1;
-            while (c < 16 && h->n > c * 4096) c *= 2;
+            // about clg_ppc particles per CTA, 1 to 16 CTAs
+            const int c = std::max(1, std::min(16, (h->n + b->clg_ppc - 1) / b->clg_ppc));
             gdb_batch::Group *g = batch_group(b, 1, c, b->clg_tp);
             g->idx.push_back(k);
             g->cap.push_back(0);
@@ -1911,7 +2088,10 @@ int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms) {
             free_graphs(h);
         }
         if (rows > 0) BCK(cudaMemsetAsync(h->rows, 0, (size_t)rows * GDB_NUM_SCALARS * sizeof(double), h->st));
-        if ((rc = ensure_partials(h, std::max(grid_for((long long)h->n * h->tp), 16))))
+        // one partial row per round of the global-memory clusters too
+        // (rounds of CLG_BLOCK / clg_tp particles)
+        if ((rc = ensure_partials(h, std::max(std::max(grid_for((long long)h->n * h->tp), 16),
+                                              grid_for((long long)h->n * b->clg_tp, CLG_BLOCK)))))
             return bset(b, rc, "%s", h->err);
         BCK(cudaMemsetAsync(&h->ctrl->maxcount, 0, sizeof(int), h->st));
         k_block_begin<<<1, 1, 0, h->st>>>(h->ctrl, time_zero);

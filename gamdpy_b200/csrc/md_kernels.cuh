@@ -73,11 +73,12 @@ struct ClusterSync {
 // Neighbour-list rebuild by the blocks of span g: the phases of the
 // standalone chain with a synchronisation between them.
 template <bool FMA, int WPB, class Sync>
-__device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const Sync &sync, NbScratch<WPB> &scr) {
+__device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const Sync &sync, NbScratch<WPB> &scr,
+                                      float4 *spos) {
     DevCtrl *c = a.ctrl;
     auto none = [] {};
     if (a.nb_kind == GDB_NBLIST_NSQ) {
-        phase_nbl_nsq<FMA, false>(a, cur, g);
+        phase_nbl_nsq<FMA, false>(a, cur, g, spos);
         const bool ok = sync(c, [&] {
             if (threadIdx.x == 0) rebuild_done(c);
         });
@@ -113,18 +114,42 @@ __device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const S
 // `nsteps` steps starting from pos[cur0], then (if do_eval) the force-only
 // evaluation of the final state -- one timeblock of
 // simulation/Simulation.py:306-328 -- by the blocks of span g.
+// NPT_Atomic changes the box every step: the box of the step (ctrl->box,
+// written by the previous step's bookkeeping), and at a list build the cell
+// grid of that box as nblist_linked_lists.py:36-39 computes it, within the
+// allocated grid.
+__device__ __forceinline__ void npt_refresh_box(SimArgs &a) {
+    a.Lx = *(volatile float *)&a.ctrl->box[0];
+    a.Ly = *(volatile float *)&a.ctrl->box[1];
+    a.Lz = *(volatile float *)&a.ctrl->box[2];
+}
+__device__ __forceinline__ void npt_cell_grid(SimArgs &a) {
+    if (a.nb_kind != GDB_NBLIST_CELLS) return;
+    a.ncx = min(a.ncx_max, max(1, (int)(a.Lx / a.min_cell)));
+    a.ncy = min(a.ncy_max, max(1, (int)(a.Ly / a.min_cell)));
+    a.ncz = min(a.ncz_max, max(1, (int)(a.Lz / a.min_cell)));
+    a.ncell = a.ncx * a.ncy * a.ncz;
+    a.nchunks = (a.ncell + SCAN_CHUNK - 1) / SCAN_CHUNK;
+}
+
 template <int TP, int NT, int INTEG, int WPB, class Sync>
-__device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int nt, int cur0, int nsteps, int do_eval,
-                                 Span g, const Sync &sync, double *s_red) {
+__device__ inline void run_steps(const SimArgs &a0, const PairEntry *s_tab, int nt, int cur0, int nsteps, int do_eval,
+                                 Span g, const Sync &sync, double *s_red, float4 *spos = nullptr) {
     __shared__ NbScratch<WPB> scr;
+    // NPT_Atomic: a copy of the arguments follows the box
+    SimArgs a_npt;
+    if (INTEG == GDB_INTEGRATOR_NPT) a_npt = a0;
+    const SimArgs &a = INTEG == GDB_INTEGRATOR_NPT ? a_npt : a0;
     DevCtrl *ctrl = a.ctrl;
     int cur = cur0;
     const int rounds = (a.n + (int)blockDim.x / TP - 1) / ((int)blockDim.x / TP);  // partial rows per step
     trace_mark(ctrl, TR_START);
     for (int s = 0; s < nsteps + do_eval; s++) {
+        if (INTEG == GDB_INTEGRATOR_NPT) npt_refresh_box(a_npt);
         if (*(volatile int *)&ctrl->rebuild) {
-            const bool ok =
-                a.fma ? rebuild_phases<true>(a, cur, g, sync, scr) : rebuild_phases<false>(a, cur, g, sync, scr);
+            if (INTEG == GDB_INTEGRATOR_NPT) npt_cell_grid(a_npt);
+            const bool ok = a.fma ? rebuild_phases<true>(a, cur, g, sync, scr, spos)
+                                  : rebuild_phases<false>(a, cur, g, sync, scr, spos);
             if (!ok) return;
         }
         const int step = *(volatile int *)&ctrl->step;
@@ -133,7 +158,7 @@ __device__ inline void run_steps(const SimArgs &a, const PairEntry *s_tab, int n
             phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g);
             trace_mark(ctrl, TR_STEP_PHASE);
             ok = sync(ctrl, [&] {
-                finalize_step<MODE_STEP>(a, step, rounds, s_red);
+                finalize_step<MODE_STEP, INTEG>(a, step, rounds, s_red);
                 if (threadIdx.x == 0 && ctrl->rebuild_next) {
                     ctrl->rebuild = 1;
                     ctrl->rebuild_next = 0;
@@ -264,14 +289,18 @@ __global__ void __launch_bounds__(BRICK_THREADS, 2) k_step_bricks(SimArgs a, Pai
 }
 
 // Persistent cooperative kernel: one timeblock of one system per launch.
+// Small N^2-list systems stage their positions for the list build in dynamic
+// shared memory (a.nsq_smem, n float4 per block).
 template <int TP, int NT, int INTEG>
 __global__ void __launch_bounds__(GDB_BLOCK, GDB_RUN_MINBLOCKS(TP)) k_run(SimArgs a, PairTable tab, int cur0, int nsteps, int do_eval) {
+    extern __shared__ float4 run_dsm[];
     __shared__ PairEntry s_tab[GDB_MAX_TYPES * GDB_MAX_TYPES];
     __shared__ double s_red[NQ * 32];
     load_table(tab, s_tab);
     // a block that starts after others abandoned a barrier does no work
     if (*(volatile int *)&a.ctrl->abort) return;
-    run_steps<TP, NT, INTEG, GDB_BLOCK / 32>(a, s_tab, tab.nt, cur0, nsteps, do_eval, grid_span(), GridSync{}, s_red);
+    run_steps<TP, NT, INTEG, GDB_BLOCK / 32>(a, s_tab, tab.nt, cur0, nsteps, do_eval, grid_span(), GridSync{}, s_red,
+                                             a.nsq_smem ? run_dsm : nullptr);
 }
 
 // One system per thread-block cluster, state in global memory: a batch of
@@ -342,6 +371,7 @@ GDB_DECLARE_NT(ntg)
     static const void *run_tp_##NTNAME(int integ) {                                                          \
         return integ == GDB_INTEGRATOR_NVT        ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVT>          \
                : integ == GDB_INTEGRATOR_LANGEVIN ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_LANGEVIN>     \
+               : integ == GDB_INTEGRATOR_NPT      ? (const void *)k_run<TP, NT, GDB_INTEGRATOR_NPT>          \
                                                   : (const void *)k_run<TP, NT, GDB_INTEGRATOR_NVE>;         \
     }                                                                                                        \
     const void *run_kernel_##NTNAME(int tp, int integ) {                                                     \

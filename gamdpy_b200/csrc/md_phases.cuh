@@ -47,12 +47,14 @@ struct SimArgs {
     int *cell_count, *cell_start, *pcell, *prank, *perm, *scell, *bsum;
     double *partials, *rows;
     float *conf;
+    float *conf_box;  // ConfigurationSaver: the box of each frame (4 floats a frame)
     DevCtrl *ctrl;
     int n, stride, max_nbs;
     int ncell, nchunks, ncx, ncy, ncz;
     int nbx, nby, nbz;  // bricks per dimension (staged-halo path, md_bricks.cuh), 0: cells x fastest
     int brick_hcap;     // staged positions a brick's halo may hold (<= BRICK_HCAP)
     int nb_kind, fma;
+    int nsq_smem;  // persistent N^2 build stages all positions in dynamic shared memory
     float Lx, Ly, Lz;
     float cps2;    // (max_cut + skin)^2, nblist.py:152
     float skin2q;  // skin*skin*0.25, orthorhombic.py:131
@@ -60,6 +62,13 @@ struct SimArgs {
     long long dof;  // N*D - D (NVT.py:35)
     int tfunc;
     float tp0, tp1, tp2, tp3;
+    // NPT_Atomic: masses without the temperature factor, target pressure
+    // function, and the cell grid the box may use (recomputed per build)
+    float npt_mass_t, npt_mass_p;
+    int pfunc;
+    float pp0, pp1, pp2, pp3;
+    float min_cell;
+    int ncx_max, ncy_max, ncz_max;
     int every, reset_every, nrows, conf_per_block;
     // NVT_Langevin: generator (s0, s1) and previous random force per user index
     ulonglong2 *rng;
@@ -190,25 +199,43 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
 
 // N^2 build (interactions/nblist.py:88-143): one warp per particle, lanes
 // stride over j, ballot + popc append hits in ascending j (deterministic).
+// With `spos` (shared memory for all n positions) the block first copies the
+// positions there, so the candidate loads are shared-memory loads; four
+// candidates per lane are loaded before they are tested.
 template <bool FMA, bool NC>
-__device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_span()) {
+__device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_span(), float4 *spos = nullptr) {
     const float4 *pos = cur_pos(a, cur);
+    const float4 *src = pos;
+    if (spos) {
+        for (int k = threadIdx.x; k < a.n; k += blockDim.x) spos[k] = pos[k];
+        __syncthreads();
+        src = spos;
+    }
     const int lane = threadIdx.x & 31;
     const int warps = (g.nb * (int)blockDim.x) >> 5;
     for (int i = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; i < a.n; i += warps) {
-        const float4 pi = load<NC>(pos + i);
+        const float4 pi = spos ? src[i] : load<NC>(pos + i);
         int count = 0;
-        for (int j0 = 0; j0 < a.n; j0 += 32) {
-            const int j = j0 + lane;
-            bool hit = false;
-            if (j < a.n && j != i) hit = dist_sq_exact<FMA>(load<NC>(pos + j), pi, a.Lx, a.Ly, a.Lz) < a.cps2;
-            if (hit && a.excl) hit = !excluded(a, a.orig[i], a.orig[j]);
-            const unsigned m = __ballot_sync(0xffffffffu, hit);
-            if (hit) {
-                const int k = count + __popc(m & ((1u << lane) - 1u));
-                if (k < a.max_nbs) a.nbl[nbl_index(i, k, a.stride)] = j;
+        for (int j0 = 0; j0 < a.n; j0 += 128) {
+            float4 q[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = j0 + 32 * u + lane;
+                q[u] = j < a.n ? (spos ? src[j] : load<NC>(pos + j)) : pi;
             }
-            count += __popc(m);
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int j = j0 + 32 * u + lane;
+                bool hit = false;
+                if (j < a.n && j != i) hit = dist_sq_exact<FMA>(q[u], pi, a.Lx, a.Ly, a.Lz) < a.cps2;
+                if (hit && a.excl) hit = !excluded(a, a.orig[i], a.orig[j]);
+                const unsigned m = __ballot_sync(0xffffffffu, hit);
+                if (hit) {
+                    const int k = count + __popc(m & ((1u << lane) - 1u));
+                    if (k < a.max_nbs) a.nbl[nbl_index(i, k, a.stride)] = j;
+                }
+                count += __popc(m);
+            }
         }
         if (lane == 0) {
             a.nbc[i] = count;
@@ -714,6 +741,39 @@ __device__ __forceinline__ double target_temperature(const SimArgs &a, double t)
     return a.tp0;
 }
 
+// Target pressure of NPT_Atomic: the same constant / ramp forms.
+__device__ __forceinline__ double target_pressure(const SimArgs &a, double t) {
+    if (a.pfunc == GDB_TFUNC_RAMP) {
+        if (t < a.pp1) return a.pp0;
+        if (t < a.pp3) return a.pp0 + (t - a.pp1) * ((double)(a.pp2 - a.pp0) / (double)(a.pp3 - a.pp1));
+        return a.pp2;
+    }
+    return a.pp0;
+}
+
+// Per-step constants of NPT_Atomic's particle update (integrators/
+// NPT_Atomic.py:108-113, with numba's typing: factor in float64, plus, minus
+// and rfactor in float32) and the box scaling of scale_box (:168-181): every
+// coordinate times sf = (1 + dt D bs0)^(1/3), the box lengths too.
+struct NptStep {
+    float plus, minus, rfactor;
+    double sf;
+    float Lx, Ly, Lz;  // box after the scaling
+};
+__device__ __forceinline__ NptStep npt_step_consts(const SimArgs &a, const DevCtrl *ctrl) {
+    NptStep ns;
+    const float ts0 = ctrl->npt_ts0, bs0 = ctrl->npt_bs0;
+    const double factor = (double)(0.5f * a.dt) * ((1.0 + 3.0 / (double)a.dof) * (double)bs0 + (double)ts0);
+    ns.plus = 1.0f / (float)(1.0 + factor);
+    ns.minus = (float)(1.0 - factor);
+    ns.rfactor = bs0 * a.dt;
+    ns.sf = pow(1.0 + (double)a.dt * 3.0 * (double)bs0, 1.0 / 3.0);
+    ns.Lx = (float)((double)a.Lx * ns.sf);
+    ns.Ly = (float)((double)a.Ly * ns.sf);
+    ns.Lz = (float)((double)a.Lz * ns.sf);
+    return ns;
+}
+
 // numba.cuda.random's generator, the one of integrators/NVT_Langevin.py:105:
 // xoroshiro128+ with the (55, 14, 36) update, uniform float32 =
 // float32((x >> 11) 2^-53), normal = first Box-Muller value of two draws.
@@ -885,7 +945,8 @@ template <int INTEG, int MODE>
 __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 pi, float4 v, float4 rr, float fx,
                                                 float fy, float fz, float u, float w, float l, bool rec, bool reset,
                                                 int step, bool shift_pending, float shx, float shy, float shz,
-                                                float xi, float4 *pos_next, double (&red)[NQ], bool &moved) {
+                                                float xi, float4 *pos_next, double (&red)[NQ], bool &moved,
+                                                const NptStep *ns = nullptr) {
     DevCtrl *ctrl = a.ctrl;
     const size_t n = a.n;
     // ConfigurationSaver: frame taken before this step's integration
@@ -902,6 +963,11 @@ __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 
             fr[3 * uidx] = (float)im.x;
             fr[3 * uidx + 1] = (float)im.y;
             fr[3 * uidx + 2] = (float)im.z;
+            if (uidx == 0 && a.conf_box) {  // include_simbox (configuration_saver.py:137-139)
+                a.conf_box[4 * si] = a.Lx;
+                a.conf_box[4 * si + 1] = a.Ly;
+                a.conf_box[4 * si + 2] = a.Lz;
+            }
         }
     }
     if (shift_pending) {
@@ -959,6 +1025,13 @@ __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 
             }
             a.rng[uidx] = st;
             a.lbeta[uidx] = make_float4(obk[0], obk[1], obk[2], 0.f);
+        } else if (INTEG == GDB_INTEGRATOR_NPT) {  // integrators/NPT_Atomic.py:118-127
+#pragma unroll
+            for (int k = 0; k < 3; k++) {
+                vv[k] = ns->plus * (ns->minus * vv[k] + ff[k] / m * a.dt);
+                kin += 0.5f * m * vv[k] * vv[k];
+                r[k] += vv[k] * a.dt + ns->rfactor * r[k];
+            }
         } else {  // integrators/NVT.py:83-102
             const float factor = 0.5f * xi * a.dt;
             const float plus = 1.0f / (1.0f + factor);
@@ -994,6 +1067,10 @@ __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 
             im.z += dimg[2];
             a.img[i] = im;
         }
+        if (INTEG == GDB_INTEGRATOR_NPT) {  // scale_box, after the wrap in the step's box
+#pragma unroll
+            for (int k = 0; k < 3; k++) r[k] = (float)(ns->sf * (double)r[k]);
+        }
         if (!(fabsf(r[0]) <= L[0] && fabsf(r[1]) <= L[1] && fabsf(r[2]) <= L[2]))
             atomicOr(&ctrl->status, GDB_STATUS_NAN);
         const float4 pn = make_float4(r[0], r[1], r[2], pi.w);
@@ -1001,8 +1078,11 @@ __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 
         a.vel[i] = make_float4(vv[0], vv[1], vv[2], m);
         a.pscal[3 * n + i] = kin;
         a.pscal[4 * n + i] = fsq;
-        // skin check for the next step (nblist.py:57-86)
-        moved |= dist_sq_exact<false>(pn, rr, a.Lx, a.Ly, a.Lz) > a.skin2q;
+        // skin check for the next step (nblist.py:57-86), in the next step's box
+        if (INTEG == GDB_INTEGRATOR_NPT)
+            moved |= dist_sq_exact<false>(pn, rr, ns->Lx, ns->Ly, ns->Lz) > a.skin2q;
+        else
+            moved |= dist_sq_exact<false>(pn, rr, a.Lx, a.Ly, a.Lz) > a.skin2q;
         red[0] += kin;
         if (reset) {
             red[5] += (double)m * vv[0];
@@ -1029,7 +1109,8 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
     DevCtrl *ctrl = a.ctrl;
     const float4 *pos = cur_pos(a, cur);
     float4 *pos_next = cur_pos(a, cur ^ 1);
-    const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
+    // NPT_Atomic reads every particle's virial every step (NPT_Atomic.py:115)
+    const bool rec = MODE == MODE_EVAL || INTEG == GDB_INTEGRATOR_NPT || (a.every > 0 && step % a.every == 0);
     const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
     const int ppar = (step & 1) ^ 1;
     const bool shift_pending = ctrl->pending[ppar] != 0;
@@ -1040,6 +1121,8 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
         shz = ctrl->shift[ppar][2];
     }
     const float xi = ctrl->xi;
+    NptStep ns;
+    if (INTEG == GDB_INTEGRATOR_NPT && MODE == MODE_STEP) ns = npt_step_consts(a, ctrl);
     const int per_block = blockDim.x / TP;
     const int rounds_total = (a.n + per_block - 1) / per_block;
     const bool full = rec || reset;
@@ -1050,7 +1133,10 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
     bool moved = false;
     __shared__ int s_round;
     int round = g.b;
-    if (PERSIST) {
+    // the persistent kernels hand out rounds through a counter unless every
+    // block has at most one (small systems: two atomics less per step)
+    const bool dynamic = PERSIST && rounds_total > g.nb;
+    if (dynamic) {
         if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
         __syncthreads();
         round = s_round;
@@ -1091,7 +1177,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
         if (active && sub == 0 && a.bond_cnt) bond_forces(a, i, pi, pos, rec, fx, fy, fz, u, w, l);
         if (active && sub == 0)
             finish_particle<INTEG, MODE>(a, i, pi, v, rr, fx, fy, fz, u, w, l, rec, reset, step, shift_pending, shx,
-                                         shy, shz, xi, pos_next, red, moved);
+                                         shy, shz, xi, pos_next, red, moved, &ns);
         if (PERSIST) {
             // this round's sums to partials[round]; the next round
             if (full) {
@@ -1107,10 +1193,15 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
             }
 #pragma unroll
             for (int q = 0; q < NQ; q++) red[q] = 0.0;
-            __syncthreads();  // every thread has read s_round
-            if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
-            __syncthreads();
-            round = s_round;
+            if (dynamic) {
+                __syncthreads();  // every thread has read s_round
+                if (threadIdx.x == 0) s_round = (int)atomicAdd(&ctrl->work[step & 1], 1u);
+                __syncthreads();
+                round = s_round;
+            } else {
+                __syncthreads();  // s_red is free again
+                round = rounds_total;
+            }
         } else {
             round += g.nb;
         }
@@ -1137,13 +1228,14 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
 // Fixed-order float64 sum of `nblocks` partial rows (blocks or rounds) and the
 // bookkeeping of a finished step (NVT.py:113-124, scalar_saver.py:165-179,
 // momentum_reset.py:64-78).  Run by one whole block.
-template <int MODE>
+template <int MODE, int INTEG = GDB_INTEGRATOR_NVE>
 __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, double *s_red) {
     DevCtrl *ctrl = a.ctrl;
     const bool rec = MODE == MODE_EVAL || (a.every > 0 && step % a.every == 0);
     const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
     const int par = step & 1, ppar = par ^ 1;
-    const bool full = rec || reset;
+    const bool npt = INTEG == GDB_INTEGRATOR_NPT && MODE == MODE_STEP;
+    const bool full = rec || reset || npt;
     const bool needk = full || a.omega2 > 0.f;
     double tot[NQ];
 #pragma unroll
@@ -1163,7 +1255,35 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
     if (threadIdx.x == 0) {
         if (MODE == MODE_STEP) {
             const double time = ctrl->time_zero + (double)step * (double)a.dt;
-            if (a.omega2 > 0.f) {
+            if (npt) {
+                // update_thermostat_barostat_state (integrators/NPT_Atomic.py:
+                // 138-166) with numba's typing; the float32 accumulators
+                // thermostat_state[1] and barostat_state[1] are the float64
+                // sums of K and W rounded to float32
+                const float ts1 = (float)tot[0], bs1 = (float)tot[2];
+                const float bs0 = ctrl->npt_bs0;
+                const long long deg = a.dof;
+                const double temperature = 2.0 * (double)ts1 / (double)deg;
+                const double sf3 = 1.0 + (double)a.dt * 3.0 * (double)bs0;
+                const double mass_t = (double)a.npt_mass_t * temperature;
+                const double mass_p = (double)a.npt_mass_p * temperature;
+                const float vol = (float)((double)ctrl->npt_vol * sf3);
+                ctrl->npt_vol = vol;
+                const double sf = pow(sf3, 1.0 / 3.0);
+                ctrl->box[0] = (float)((double)ctrl->box[0] * sf);
+                ctrl->box[1] = (float)((double)ctrl->box[1] * sf);
+                ctrl->box[2] = (float)((double)ctrl->box[2] * sf);
+                const double T_target = target_temperature(a, time);
+                const double P_target = target_pressure(a, time);
+                const double p_inst = (temperature * (double)a.n + (double)bs1) / (double)vol;
+                const double ke_dev =
+                    ((double)(2.0f * ts1) + (double)(bs0 * bs0) * mass_p) / ((double)(deg + 1) * T_target) - 1.0;
+                const double p_dev = 3.0 * ((double)vol * (p_inst - P_target) + (double)(0.5f * ts1) / (double)deg);
+                const float ts0 = (float)((double)ctrl->npt_ts0 +
+                                          (double)a.dt * ke_dev * (double)(deg + 1) * T_target / mass_t);
+                ctrl->npt_ts0 = ts0;
+                ctrl->npt_bs0 = (float)((double)bs0 + (double)a.dt * (p_dev / mass_p + (double)(ts0 * bs0)));
+            } else if (a.omega2 > 0.f) {
                 const double T = target_temperature(a, time);
                 const double dev = 2.0 * tot[0] / ((double)a.dof * T) - 1.0;
                 ctrl->xi = (float)((double)ctrl->xi + (double)(a.dt * a.omega2) * dev);
@@ -1176,6 +1296,12 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
                 row[GDB_SCALAR_LAPU] = tot[3];
                 row[GDB_SCALAR_K] = tot[0];
                 row[GDB_SCALAR_FSQ] = tot[4];
+                if (npt) {  // the saver reads the box the step left (scalar_saver.py:195)
+                    float vol = ctrl->box[0];
+                    vol *= ctrl->box[1];
+                    vol *= ctrl->box[2];
+                    row[GDB_SCALAR_VOL] = vol;
+                }
             }
             if (reset) {
                 ctrl->shift[par][0] = (float)(tot[5] / tot[8]);

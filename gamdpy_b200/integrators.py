@@ -1,4 +1,5 @@
-"""Integrators (gamdpy/integrators/NVE.py, NVT.py, NVT_Langevin.py).
+"""Integrators (gamdpy/integrators/NVE.py, NVT.py, NVT_Langevin.py,
+NPT_Atomic.py).
 
 The step itself runs fused with the force evaluation in libgamdb200's step
 kernel; these classes carry the parameters with gamdpy's names and
@@ -112,3 +113,63 @@ class NVT_Langevin(Integrator):
     def configure_device(self, sim, configuration):
         kind, tparams = self._tfunc()
         sim.set_langevin(np.float32(self.dt), np.float32(self.alpha), int(self.seed), kind, tparams)
+
+
+class NPT_Atomic(Integrator):
+    """Constant N, P, T for atomic systems (integrators/NPT_Atomic.py:9-213):
+    leap-frog with the Martyna-Tobias-Klein thermostat and barostat
+    (Mol. Phys. 87, 1117 (1996)).  ``thermostat_state`` = (p_xi/Q, 0) and
+    ``barostat_state`` = (p_eps/W, 0, volume), float32 as in the reference
+    (the second entries are the reference's accumulators, zero between
+    steps).  ``temperature`` and ``pressure`` are numbers or functions of
+    time from make_function_constant / make_function_ramp.  The step, the box
+    scaling and the state update run fused in the persistent kernel; the box
+    lengths of the configuration follow the run."""
+
+    def __init__(self, temperature, tau: float, pressure, tau_p: float, dt: float) -> None:
+        self.temperature = temperature
+        self.tau = tau
+        self.pressure = pressure
+        self.tau_p = tau_p
+        self.dt = dt
+        self.thermostat_state = np.zeros(2, dtype=np.float32)
+        self.barostat_state = np.zeros(3, dtype=np.float32)
+        self._device = None
+
+    def _masses(self, configuration):
+        # NPT_Atomic.py:43-48 (numpy float32 arithmetic)
+        degrees = configuration.N * configuration.D - configuration.D
+        factor = np.float32(1. / (4 * np.pi * np.pi))
+        mass_t = np.float32((degrees - 1) * configuration.D * factor * self.tau * self.tau)
+        mass_p = np.float32((degrees - 1) * configuration.D * factor * self.tau_p * self.tau_p)
+        return degrees, mass_t, mass_p
+
+    def get_params(self, configuration, interactions_params=None, verbose=False):
+        degrees, mass_t, mass_p = self._masses(configuration)
+        self.barostat_state[2] = configuration.get_volume()
+        return (np.float32(self.dt), mass_t, mass_p, degrees, self.thermostat_state, self.barostat_state)
+
+    @staticmethod
+    def _func(f, what):
+        if not callable(f):
+            f = make_function_constant(value=float(f))
+        kind = getattr(f, "_gdb_tfunc", None)
+        if kind is None:
+            raise NotImplementedError(f"NPT_Atomic {what} must be a number, make_function_constant or "
+                                      "make_function_ramp (the step runs in CUDA)")
+        return kind, f._gdb_tparams
+
+    def configure_device(self, sim, configuration):
+        _, mass_t, mass_p = self._masses(configuration)
+        tk, tp = self._func(self.temperature, "temperature")
+        pk, pp = self._func(self.pressure, "pressure")
+        sim.set_npt(np.float32(self.dt), mass_t, mass_p, tk, tp, pk, pp)
+        self.barostat_state[2] = configuration.get_volume()
+        sim.set_npt_state(self.thermostat_state, self.barostat_state)
+        self._device = sim
+
+    def sync_from_device(self):
+        if self._device is not None:
+            ts, bs = self._device.npt_state()
+            self.thermostat_state[:] = ts
+            self.barostat_state[:] = bs

@@ -70,15 +70,18 @@ class ScalarSaver(RuntimeAction):
         output.attrs["scalar_names"] = list(self.sid.keys())
 
     def update_from_rows(self, block, rows, output, volume, compute_flags=None):
-        """rows: (saves, 5) float64 from the library (U, W, lapU, K, Fsq).
-        A column whose compute flag the run leaves off stays zero, as the
-        reference's saver sums per-particle values its kernels never filled
-        (scalar_saver.py:120-130)."""
+        """rows: (saves, 6) float64 from the library (U, W, lapU, K, Fsq,
+        Vol).  The Vol column is the box volume after each saved step when
+        the box changes (NPT_Atomic), zero otherwise, where ``volume`` is
+        used.  A column whose compute flag the run leaves off stays zero, as
+        the reference's saver sums per-particle values its kernels never
+        filled (scalar_saver.py:120-130)."""
         col = {"U": 0, "W": 1, "lapU": 2, "K": 3, "Fsq": 4}
         out = np.zeros((self.scalar_saves_per_block, self.num_scalars), np.float32)
+        vol_rows = rows[: self.scalar_saves_per_block, 5]
         for name, idx in self.sid.items():
             if name == "Vol":
-                out[:, idx] = volume
+                out[:, idx] = vol_rows if np.all(vol_rows > 0) else volume
             elif compute_flags is None or compute_flags.get(name, False):
                 out[:, idx] = rows[: self.scalar_saves_per_block, col[name]]
         output["scalars"][block, :] = out
@@ -97,11 +100,11 @@ class MomentumReset(RuntimeAction):
 class ConfigurationSaver(RuntimeAction):
     """Log-spaced positions and images per timeblock
     (runtime_actions/configuration_saver.py:9-141): dataset
-    ``block[block, save, {r, r_im}, N, D]`` float32, attr ``vectors_names``."""
+    ``block[block, save, {r, r_im}, N, D]`` float32, attr ``vectors_names``;
+    with ``include_simbox`` also ``sim_box[block, save, D]``, the box lengths
+    at each saved step."""
 
     def __init__(self, include_simbox=False, verbose=False):
-        if include_simbox:
-            raise NotImplementedError("include_simbox: the box is constant in the supported ensembles")
         self.include_simbox = include_simbox
         self.num_vectors = 2
         self.sid = {"r": 0, "r_im": 1}
@@ -116,6 +119,11 @@ class ConfigurationSaver(RuntimeAction):
         output.create_dataset("block", shape=(num_timeblocks, self.conf_per_block, self.num_vectors,
                                               configuration.N, configuration.D), dtype=np.float32)
         output.attrs["vectors_names"] = list(self.sid.keys())
+        if self.include_simbox:
+            output.create_dataset("sim_box", shape=(num_timeblocks, self.conf_per_block, configuration.D),
+                                  dtype=np.float32)
 
-    def update_from_frames(self, block, frames, output):
+    def update_from_frames(self, block, frames, output, boxes=None):
         output["block"][block] = frames
+        if self.include_simbox and boxes is not None:
+            output["sim_box"][block] = boxes

@@ -17,7 +17,7 @@ import numpy as np
 
 from . import _lib
 from .configuration import Configuration, get_default_compute_flags, unit_cells
-from .integrators import NVE, NVT, NVT_Langevin
+from .integrators import NPT_Atomic, NVE, NVT, NVT_Langevin
 from .interactions import Bonds, PairPotential
 from .runtime_actions import ConfigurationSaver, MomentumReset, ScalarSaver
 
@@ -84,6 +84,34 @@ def split_interactions(interactions):
     return pairs[0], (bonds[0] if bonds else None)
 
 
+def _autotune_cache_path():
+    import os
+    d = os.environ.get("GAMDPY_B200_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "gamdpy_b200")
+    return os.path.join(d, "autotune.json")
+
+
+def _autotune_cache_load():
+    import json
+    try:
+        with open(_autotune_cache_path()) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def _autotune_cache_store(key, value):
+    import json
+    import os
+    path = _autotune_cache_path()
+    data = _autotune_cache_load()
+    data[key] = value
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    tmp = path + f".{os.getpid()}"
+    with open(tmp, "w") as f:
+        json.dump(data, f, indent=1, sort_keys=True)
+    os.replace(tmp, path)
+
+
 def _lanes(tp):
     """Library lanes per particle for a gamdpy ``tp``: largest power of two
     <= tp, at most 32."""
@@ -106,8 +134,12 @@ class Simulation:
         self.interactions = interactions if isinstance(interactions, list) else [interactions]
         self._pair, self._bonds = split_interactions(self.interactions)
         self.integrator = integrator
-        if not isinstance(integrator, (NVE, NVT, NVT_Langevin)):
-            raise NotImplementedError("gamdpy_b200 supports the NVE, NVT and NVT_Langevin integrators")
+        if not isinstance(integrator, (NVE, NVT, NVT_Langevin, NPT_Atomic)):
+            raise NotImplementedError("gamdpy_b200 supports the NVE, NVT, NVT_Langevin and NPT_Atomic integrators")
+        if isinstance(integrator, NPT_Atomic):
+            flags = getattr(configuration, "compute_flags", None) or {}
+            if not flags.get("W", True):
+                raise ValueError("NPT_Atomic requires virial")  # NPT_Atomic.py:88-89
         self.dt = integrator.dt
         if num_timeblocks == 0:
             if num_steps == 0:
@@ -244,8 +276,11 @@ class Simulation:
         for name in ("U", "W", "lapU", "K", "Fsq"):
             if name in self.configuration.sid and not self.compute_flags.get(name, False):
                 self.configuration.scalars[:, self.configuration.sid[name]] = 0.0
-        if isinstance(self.integrator, NVT):
+        if isinstance(self.integrator, (NVT, NPT_Atomic)):
             self.integrator.sync_from_device()
+        if isinstance(self.integrator, NPT_Atomic):
+            # the box the run left (the reference's sim_box device array)
+            self.configuration.simbox.lengths[:] = self._sim.box()
         for interaction in self.interactions:
             interaction.check_datastructure_validity()
         if self._scalar_saver is not None:
@@ -253,8 +288,10 @@ class Simulation:
             self._scalar_saver.update_from_rows(block, rows, self.memory, self.configuration.get_volume(),
                                                 self.compute_flags)
         if self._conf_saver is not None:
-            frames = self._sim.saved_configurations(self._conf_saver.conf_per_block)
-            self._conf_saver.update_from_frames(block, frames, self.memory)
+            cpb = self._conf_saver.conf_per_block
+            frames = self._sim.saved_configurations(cpb)
+            boxes = self._sim.saved_boxes(cpb) if self._conf_saver.include_simbox else None
+            self._conf_saver.update_from_frames(block, frames, self.memory, boxes)
 
     def _finish_blocks(self, block_times):
         if self.timing:
@@ -301,42 +338,98 @@ class Simulation:
         """Steps per second over the timed blocks, as benchmarks/benchmark_LJ.py:90."""
         return self.last_num_blocks * self.steps_per_block / (np.sum(self.timing_numba_blocks) / 1000)
 
-    def autotune(self, tps_candidates=(1, 2, 4, 8, 16, 32), skins=None, steps=None, verbose=False):
-        """Pick lanes per particle (and optionally skin) by timing short runs,
-        as Simulation.autotune (Simulation.py:636-821) does for pb/tp/skin.
-        Keeps the fastest plan (``compute_plan['lanes']``, ``['skin']``); the
-        configuration is restored afterwards."""
+    def autotune(self, tps_candidates=(1, 2, 4, 8, 16, 32), skins=None, nblists=None, steps=None, cache=True,
+                 verbose=False):
+        """Pick the neighbour-list kind, lanes per particle and skin by timing
+        short runs, as Simulation.autotune (Simulation.py:636-821) searches
+        nblist, tp and skin.  nblists defaults to the plan's kind plus
+        'N squared' below 32 000 particles and 'linked lists' above 2000
+        (gamdpy's rules); skins to the plan's skin.  The fastest plan is
+        kept in ``compute_plan`` and, with ``cache``, stored per (GPU, N,
+        density, type count, integrator, candidate sets) in
+        ``$GAMDPY_B200_CACHE/autotune.json`` (default
+        ``~/.cache/gamdpy_b200``): a later call with the same key applies it
+        without timing.  The configuration, its box and the integrator state
+        are restored afterwards, so the run that follows equals a run started
+        with the chosen plan."""
+        if isinstance(self.integrator, NVT_Langevin):
+            raise NotImplementedError("autotune: the NVT_Langevin generators advance with every timed step")
         steps = steps or min(self.steps_per_block, 256)
         conf = self.configuration
-        saved = (conf["r"].copy(), conf["v"].copy(), conf.r_im.copy())
-        xi = self.integrator.thermostat_state.copy() if isinstance(self.integrator, NVT) else None
-        skins = list(skins) if skins is not None else [float(self.compute_plan["skin"])]
         pp = self._pair
+        skins = [float(x) for x in skins] if skins is not None else [float(self.compute_plan["skin"])]
+        if nblists is None:
+            nblists = [self.compute_plan["nblist"]]
+            if nblists[0] != "N squared" and conf.N < 32000:
+                nblists.append("N squared")
+            if nblists[0] != "linked lists" and conf.N > 2000:
+                nblists.append("linked lists")
+        key = self._autotune_key(list(tps_candidates), skins, list(nblists))
+        self.autotune_from_cache = False
+        if cache:
+            hit = _autotune_cache_load().get(key)
+            if hit is not None:
+                self._apply_plan(hit["nblist"], hit["lanes"], hit["skin"])
+                self.autotune_from_cache = True
+                return dict(self.compute_plan)
+        saved = self._save_state()
         best = None
-        for skin in skins:
-            for tp in tps_candidates:
-                self.compute_plan["skin"] = skin
-                self.compute_plan["lanes"] = tp
-                self._sim.set_nblist(pp.nblist.kind, float(np.float32(skin)), pp.max_num_nbs)
-                self._sim.set_plan(tp)
-                conf.copy_to_device()
-                self.integrate_self(0.0, steps)  # warm-up / graph capture
-                ms = self.integrate_self(0.0, steps)
-                if verbose:
-                    print(f"autotune: tp={tp} skin={skin}: {steps / ms * 1000:.1f} TPS")
-                if best is None or ms < best[0]:
-                    best = (ms, tp, skin)
-        _, tp, skin = best
-        self.compute_plan["lanes"], self.compute_plan["skin"] = tp, skin
-        self._sim.set_nblist(pp.nblist.kind, float(np.float32(skin)), pp.max_num_nbs)
-        self._sim.set_plan(tp)
-        conf["r"], conf["v"] = saved[0], saved[1]
-        conf.r_im[:] = saved[2]
-        if xi is not None:
-            self.integrator.thermostat_state[:] = xi
-            self._sim.set_thermostat_state(xi)
+        for nblist in nblists:
+            for skin in skins:
+                for tp in tps_candidates:
+                    self._apply_plan(nblist, tp, skin)
+                    self._restore_state(saved)
+                    self.integrate_self(0.0, steps)  # warm-up
+                    ms = self.integrate_self(0.0, steps)
+                    if verbose:
+                        print(f"autotune: {nblist} tp={tp} skin={skin}: {steps / ms * 1000:.1f} TPS")
+                    if best is None or ms < best[0]:
+                        best = (ms, nblist, tp, skin)
+        _, nblist, tp, skin = best
+        self._apply_plan(nblist, tp, skin)
+        self._restore_state(saved)
+        if cache:
+            _autotune_cache_store(key, {"nblist": nblist, "lanes": int(tp), "skin": float(skin),
+                                        "tps": steps / best[0] * 1000})
+        return dict(self.compute_plan)
+
+    def _autotune_key(self, tps, skins, nblists):
+        conf = self.configuration
+        rho = conf.N / float(np.prod(conf.simbox.lengths.astype(np.float64)))
+        return "|".join([_lib.device_name(self._sim.device), f"N={conf.N}", f"rho={rho:.4f}",
+                         f"nt={int(np.max(conf.ptype)) + 1 if conf.N else 1}", type(self.integrator).__name__,
+                         f"tp={tps}", f"skin={skins}", f"nblist={nblists}"])
+
+    def _apply_plan(self, nblist, tp, skin):
+        pp = self._pair
+        self.compute_plan["nblist"], self.compute_plan["lanes"], self.compute_plan["skin"] = nblist, tp, skin
+        kind = _lib.NBLIST_NSQ if nblist == "N squared" else _lib.NBLIST_CELLS
+        pp.make_nblist(self.configuration, self.compute_plan)
+        self._sim.set_nblist(kind, float(np.float32(skin)), pp.max_num_nbs)
+        self._sim.set_plan(int(tp))
+
+    def _save_state(self):
+        conf = self.configuration
+        st = {"r": conf["r"].copy(), "v": conf["v"].copy(), "r_im": conf.r_im.copy(),
+              "box": conf.simbox.lengths.copy()}
+        if isinstance(self.integrator, NVT):
+            st["xi"] = self._sim.thermostat_state()
+        if isinstance(self.integrator, NPT_Atomic):
+            st["npt"] = self._sim.npt_state()
+        return st
+
+    def _restore_state(self, st):
+        conf = self.configuration
+        conf["r"], conf["v"] = st["r"], st["v"]
+        conf.r_im[:] = st["r_im"]
+        conf.simbox.lengths[:] = st["box"]
+        if "xi" in st:
+            self._sim.set_thermostat_state(st["xi"])
+            self.integrator.thermostat_state[:] = st["xi"]
+        if "npt" in st:
+            self._sim.set_npt_state(*st["npt"])
+            self.integrator.thermostat_state[:], self.integrator.barostat_state[:] = st["npt"]
         conf.copy_to_device()
-        return self.compute_plan
 
 
 def get_default_sim():

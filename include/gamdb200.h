@@ -60,6 +60,7 @@ extern "C" {
 #define GDB_INTEGRATOR_NVE 0 /* integrators/NVE.py */
 #define GDB_INTEGRATOR_NVT 1 /* integrators/NVT.py */
 #define GDB_INTEGRATOR_LANGEVIN 2 /* integrators/NVT_Langevin.py */
+#define GDB_INTEGRATOR_NPT 3 /* integrators/NPT_Atomic.py */
 /* NVT target temperature T(t): misc/make_function.py */
 #define GDB_TFUNC_CONSTANT 0 /* make_function_constant :6-13, tparams = {T} */
 #define GDB_TFUNC_RAMP 1     /* make_function_ramp :16-34, tparams = {T0, t0, T1, t1} */
@@ -70,7 +71,8 @@ extern "C" {
 #define GDB_SCALAR_LAPU 2
 #define GDB_SCALAR_K 3
 #define GDB_SCALAR_FSQ 4
-#define GDB_NUM_SCALARS 5
+#define GDB_SCALAR_VOL 5 /* box volume after the step: NPT_Atomic runs only (zero otherwise) */
+#define GDB_NUM_SCALARS 6
 
 typedef struct gdb_sim gdb_sim;
 
@@ -79,6 +81,9 @@ int gdb_version(void);
 
 /* Number of visible CUDA devices. */
 int gdb_device_count(int *count);
+/* Name of CUDA device `device` (for the autotuner's per-GPU cache; no
+ * reference counterpart). */
+int gdb_device_name(int device, char *buf, int n);
 
 /* Create a simulation of n particles and ntypes particle types on `device`.
  * Replaces Configuration.copy_to_device's allocations and the per-object
@@ -179,6 +184,28 @@ int gdb_get_langevin_state(gdb_sim *h, uint64_t *states, float *old_beta);
 int gdb_get_thermostat_state(gdb_sim *h, float state[2]);
 int gdb_set_thermostat_state(gdb_sim *h, const float state[2]);
 
+/* NPT_Atomic (integrators/NPT_Atomic.py:38-50 get_params, :104-136 step,
+ * :138-166 thermostat/barostat update, :168-181 box scaling): leap-frog with
+ * the Martyna-Tobias-Klein thermostat and barostat.  mass_t and mass_p are
+ * the reference's masses without the temperature factor (float32, computed
+ * by the caller as get_params does); target temperature tfunc/tparams and
+ * target pressure pfunc/pparams take the forms of gdb_set_integrator_nvt.
+ * The box changes every step (gdb_get_box reads it back); the cell grid is
+ * recomputed from the current box at every list build, within the grid
+ * allocated for the box at gdb_set_nblist (the reference keeps the initial
+ * grid).  Runs on the persistent kernel only (not on thread-block clusters,
+ * not in batches); per-particle virials are evaluated every step. */
+int gdb_set_integrator_npt(gdb_sim *h, float dt, float mass_t, float mass_p, int tfunc, const float *tparams,
+                           int pfunc, const float *pparams);
+/* NPT_Atomic.thermostat_state = {p_xi/Q, 0} and barostat_state =
+ * {p_eps/W, 0, volume} (integrators/NPT_Atomic.py:35-36); set_npt_state
+ * with a NULL pointer leaves that part unchanged.  The volume of a new
+ * simulation is the box's. */
+int gdb_get_npt_state(gdb_sim *h, float ts[2], float bs[3]);
+int gdb_set_npt_state(gdb_sim *h, const float ts[2], const float bs[3]);
+/* The current box lengths (changed by NPT runs). */
+int gdb_get_box(gdb_sim *h, float lengths[3]);
+
 /* Runtime actions compiled into the step: ScalarSaver(steps_between_output)
  * (runtime_actions/scalar_saver.py:161-197) and MomentumReset(steps_between_reset)
  * (runtime_actions/momentum_reset.py:84-103); 0 disables. */
@@ -192,6 +219,10 @@ int gdb_set_runtime_actions(gdb_sim *h, int scalar_every, int momentum_every);
 int gdb_set_configuration_saver(gdb_sim *h, int conf_per_block);
 /* Frames saved during the last timeblock (same layout as above). */
 int gdb_get_saved_configurations(gdb_sim *h, float *out, int conf_per_block);
+/* The box of each saved frame (ConfigurationSaver(include_simbox=True),
+ * configuration_saver.py:47-51, 137-139): conf_per_block x 3 float32, the
+ * box lengths at the step the frame was taken (they change under NPT_Atomic). */
+int gdb_get_saved_boxes(gdb_sim *h, float *out, int conf_per_block);
 
 /* One evaluation of the interactions on the current state: neighbour-list
  * check/rebuild, then forces, U, W, lapU (Evaluator.evaluate,
@@ -313,6 +344,15 @@ typedef struct gdb_batch gdb_batch;
  * (spread over 16 CTAs, at least 32 particles each), so a system gives the
  * same bits in a batch as alone.  Tuned by SimulationBatch.autotune. */
 int gdb_batch_create(gdb_sim *const *sims, int count, int particles_per_cta, gdb_batch **out);
+/* As gdb_batch_create, with the shape of the systems above 4096 particles
+ * (which run the persistent phases on thread-block clusters with state in
+ * global memory, one 1024-thread CTA per SM): about clg_particles_per_cta
+ * particles per CTA (1 to 16 CTAs a system; 0 = the smallest count from 4096
+ * up whose CTAs fit the SMs left by the smaller systems' share of the
+ * particles) and clg_tp lanes per particle (1, 2, 4 or 8; 0 = 1).  Tuned by
+ * SimulationBatch.autotune. */
+int gdb_batch_create_ex(gdb_sim *const *sims, int count, int particles_per_cta, int clg_particles_per_cta,
+                        int clg_tp, gdb_batch **out);
 int gdb_batch_run(gdb_batch *b, double time_zero, int steps, float *ms);
 int gdb_batch_destroy(gdb_batch *b);
 int gdb_batch_get_last_error(gdb_batch *b, char *buf, int n);

@@ -427,6 +427,94 @@ void orc_langevin_step(int n, float *r, float *v, const float *f, const float *m
     }
 }
 
+/* integrators/NPT_Atomic.py (Martyna, Tobias and Klein thermostat-barostat,
+ * leap-frog), its three parts in order.  State as the reference's float32
+ * arrays: ts[0] = p_xi/Q, bs[0] = p_eps/W, bs[2] = volume; the K and W sums
+ * (ts[1], bs[1] there, float32 atomics) are float64 sums here, rounded to
+ * float32 where the reference reads the float32 accumulators.
+ *
+ * step (:104-136), per particle: factor = 0.5 dt ((1 + 3/degrees) bs0 + ts0)
+ * in float64, plus = 1/(1 + factor) and minus = 1 - factor in float32,
+ * rfactor = bs0 dt; v = plus (minus v + f/m dt), K += m v^2 / 2 (the new
+ * half-step velocity), r += v dt + rfactor r, then periodic boundaries in the
+ * box of the step.  Returns sum K; *wsum = sum W (the virial the force
+ * evaluation wrote per particle). */
+double orc_npt_step(int n, float *r, float *v, const float *f, const float *m, int32_t *img, const float *box,
+                    float dt, float ts0, float bs0, long long degrees, const float *W, float *K, double *wsum) {
+    const double factor = (double)(0.5f * dt) * ((1.0 + 3.0 / (double)degrees) * (double)bs0 + (double)ts0);
+    const float plus = 1.0f / (float)(1.0 + factor);
+    const float minus = (float)(1.0 - factor);
+    const float rfactor = bs0 * dt;
+    float *kbuf = (float *)malloc((size_t)n * sizeof(float));
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n; i++) {
+        const float my_m = m[i];
+        float k_i = 0.0f;
+        for (int k = 0; k < 3; k++) {
+            const size_t e = 3 * (size_t)i + k;
+            v[e] = plus * (minus * v[e] + f[e] / my_m * dt);
+            k_i += 0.5f * my_m * v[e] * v[e];
+            r[e] += v[e] * dt + rfactor * r[e];
+        }
+        orc_apply_pbc(r + 3 * (size_t)i, img + 3 * (size_t)i, box);
+        kbuf[i] = k_i;
+        if (K) K[i] = k_i;
+    }
+    double ks = 0.0, ws = 0.0;
+    for (int i = 0; i < n; i++) {
+        ks += kbuf[i];
+        ws += W[i];
+    }
+    free(kbuf);
+    *wsum = ws;
+    return ks;
+}
+
+/* scale_box (:168-181): every coordinate times (1 + dt D bs0)^(1/3), in
+ * float64, stored float32. */
+void orc_npt_scale(int n, float *r, float dt, float bs0) {
+    const double sf3 = 1.0 + (double)dt * 3.0 * (double)bs0;
+    const double sf = pow(sf3, 1.0 / 3.0);
+    for (size_t e = 0; e < 3 * (size_t)n; e++) r[e] = (float)(sf * (double)r[e]);
+}
+
+/* update_thermostat_barostat_state (:138-166) with the sums of the step: box
+ * and volume scaled by the factor of scale_box, then the state equations of
+ * the reference in its float32/float64 typing.  T_target, P_target: the
+ * target functions at the step's time. */
+void orc_npt_update(float *ts, float *bs, float *box, int n, long long degrees, float dt, float mass_t0,
+                    float mass_p0, double ksum, double wsum, double T_target, double P_target) {
+    const float ts1 = (float)ksum, bs1 = (float)wsum;
+    const double temperature = 2.0 * (double)ts1 / (double)degrees;
+    const double sf3 = 1.0 + (double)dt * 3.0 * (double)bs[0];
+    const double mass_t = (double)mass_t0 * temperature;
+    const double mass_p = (double)mass_p0 * temperature;
+    bs[2] = (float)((double)bs[2] * sf3);
+    const double sf = pow(sf3, 1.0 / 3.0);
+    for (int k = 0; k < 3; k++) box[k] = (float)((double)box[k] * sf);
+    const double p_inst = (temperature * (double)n + (double)bs1) / (double)bs[2];
+    const double ke_dev = ((double)(2.0f * ts1) + (double)(bs[0] * bs[0]) * mass_p) /
+                              ((double)(degrees + 1) * T_target) - 1.0;
+    const double p_dev = 3.0 * ((double)bs[2] * (p_inst - P_target) + (double)(0.5f * ts1) / (double)degrees);
+    ts[0] = (float)((double)ts[0] + (double)dt * ke_dev * (double)(degrees + 1) * T_target / mass_t);
+    bs[0] = (float)((double)bs[0] + (double)dt * (p_dev / mass_p + (double)(ts[0] * bs[0])));
+    ts[1] = 0.0f;
+    bs[1] = 0.0f;
+}
+
+/* NPT state for orc_run_timeblock's integrator 3 (set before the call):
+ * ts (2) and bs (3) float32 arrays, masses without the temperature factor
+ * (NPT_Atomic.py:45-48), constant target pressure. */
+static float *g_npt_ts = NULL, *g_npt_bs = NULL;
+static float g_npt_mass_t = 0.0f, g_npt_mass_p = 0.0f, g_npt_P = 0.0f;
+void orc_set_npt(float *ts, float *bs, float mass_t, float mass_p, float P) {
+    g_npt_ts = ts;
+    g_npt_bs = bs;
+    g_npt_mass_t = mass_t;
+    g_npt_mass_p = mass_p;
+    g_npt_P = P;
+}
+
 /* Langevin state for orc_run_timeblock's integrator 2 (set before the call) */
 static uint64_t *g_lv_states = NULL;
 static float *g_lv_beta = NULL;
@@ -437,7 +525,7 @@ void orc_set_langevin(uint64_t *states, float *old_beta, float alpha) {
     g_lv_alpha = alpha;
 }
 
-/* integrators/NVT.py:75-111 (step) and :226-237 (update_thermostat_state).
+/* integrators/NVT.py:75-111 (step) and :113-124 (update_thermostat_state).
  * state[0] = xi (float32), the kinetic-energy sum is returned in float64
  * (the reference accumulates it with float32 atomics into state[1]).
  * Returns sum_i K_i. */
@@ -500,7 +588,8 @@ void orc_momentum_reset(int n, float *v, const float *m) {
  *   ScalarSaver (scalar_saver.py:161-197) and MomentumReset
  *   (momentum_reset.py:84-103) in that order.
  *
- * integrator: 0 = NVE, 1 = NVT, 2 = NVT_Langevin (state from orc_set_langevin).
+ * integrator: 0 = NVE, 1 = NVT, 2 = NVT_Langevin (state from orc_set_langevin),
+ * 3 = NPT_Atomic (state from orc_set_npt; box is updated in place).
  * nvt_state[0] = xi (in/out).
  * nblist_kind: 0 = N squared, 1 = linked lists.  r_ref / have_list carry the
  * list state across calls (have_list = 0 forces a build).
@@ -509,7 +598,7 @@ void orc_momentum_reset(int n, float *v, const float *m) {
  * cell-grid error, -2 on neighbour-list overflow.
  */
 int orc_run_timeblock(int n, float *r, float *v, float *f, const float *m, int32_t *img, const int32_t *ptype,
-                      const float *box, const float *params, int np, int nt, int kind, int cutmode,
+                      float *box, const float *params, int np, int nt, int kind, int cutmode,
                       int nblist_kind, float skin, int max_nbs, int32_t *nbl, float *r_ref, int *have_list,
                       int integrator, float dt, float *nvt_state, float omega2, float T, int steps, int every,
                       int reset_every, float *U, float *W, float *K, double *scal_out, int fma) {
@@ -543,6 +632,13 @@ int orc_run_timeblock(int n, float *r, float *v, float *f, const float *m, int32
                 orc_nve_step(n, r, v, f, m, img, box, dt, K, NULL);
             } else if (integrator == 2) {
                 orc_langevin_step(n, r, v, f, m, img, box, dt, g_lv_alpha, T, g_lv_states, g_lv_beta, K);
+            } else if (integrator == 3) {
+                double ws = 0.0;
+                const double ks = orc_npt_step(n, r, v, f, m, img, box, dt, g_npt_ts[0], g_npt_bs[0], degrees, W, K,
+                                               &ws);
+                orc_npt_scale(n, r, dt, g_npt_bs[0]);
+                orc_npt_update(g_npt_ts, g_npt_bs, box, n, degrees, dt, g_npt_mass_t, g_npt_mass_p, ks, ws, (double)T,
+                               (double)g_npt_P);
             } else {
                 double ks = orc_nvt_step(n, r, v, f, m, img, box, dt, nvt_state[0], K, NULL);
                 nvt_state[0] = orc_nvt_thermostat_update(nvt_state[0], ks, dt, omega2, degrees, T);

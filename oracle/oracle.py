@@ -76,6 +76,7 @@ def lib():
         L.orc_xoro_normal_f32.restype = f
         L.orc_langevin_step.argtypes = [i, P, P, P, P, P, P, f, f, f, P, P, P]
         L.orc_set_langevin.argtypes = [P, P, f]
+        L.orc_set_npt.argtypes = [P, P, f, f, f]
         _lib = L
     return _lib
 
@@ -338,15 +339,29 @@ def xoro_normal_f32(states, index):
     return np.float32(lib().orc_xoro_normal_f32(row.ctypes.data_as(ctypes.c_void_p)))
 
 
+def npt_masses(n, D, tau, tau_p):
+    """Thermostat and barostat masses without the temperature factor, as
+    integrators/NPT_Atomic.py:44-48 computes them (numpy float32)."""
+    degrees = n * D - D
+    factor = np.float32(1. / (4 * np.pi * np.pi))
+    mass_t = np.float32((degrees - 1) * D * factor * tau * tau)
+    mass_p = np.float32((degrees - 1) * D * factor * tau_p * tau_p)
+    return mass_t, mass_p
+
+
 class Run:
     """State of one oracle simulation, advanced one timeblock at a time with
     the reference's composed loop (gamdpy/simulation/Simulation.py:330-346).
     integrator "NVT_Langevin" takes temperature, alpha and seed
-    (integrators/NVT_Langevin.py:44-53)."""
+    (integrators/NVT_Langevin.py:44-53); "NPT_Atomic" takes temperature,
+    tau, pressure and tau_p, with the state arrays ``ts`` (2) and ``bs`` (3)
+    and the masses of integrators/NPT_Atomic.py:38-50; its box changes in
+    place."""
 
     def __init__(self, r, v, m, ptype, box, table, kind=POT_LJ_SIGMA_EPSILON, cutmode=CUT_SF,
                  nblist="N squared", skin=0.5, max_nbs=300, integrator="NVE", dt=0.005,
-                 temperature=None, tau=None, every=0, reset_every=0, fma=0, alpha=None, seed=0):
+                 temperature=None, tau=None, every=0, reset_every=0, fma=0, alpha=None, seed=0, pressure=None,
+                 tau_p=None):
         n = len(r)
         self.n = n
         self.r = _f32(r).copy()
@@ -358,7 +373,13 @@ class Run:
         self.kind, self.cutmode = kind, cutmode
         self.nblist_kind = 0 if nblist == "N squared" else 1
         self.skin, self.max_nbs = float(skin), int(max_nbs)
-        self.integrator = {"NVE": 0, "NVT": 1, "NVT_Langevin": 2}[integrator]
+        self.integrator = {"NVE": 0, "NVT": 1, "NVT_Langevin": 2, "NPT_Atomic": 3}[integrator]
+        if self.integrator == 3:
+            self.ts = np.zeros(2, np.float32)
+            self.bs = np.zeros(3, np.float32)
+            self.bs[2] = np.float32(np.prod(self.box.astype(np.float32)))
+            self.mass_t, self.mass_p = npt_masses(n, 3, tau, tau_p)
+            self.P = np.float32(pressure)
         if self.integrator == 2:
             self.alpha = np.float32(alpha)
             self.rng = xoro_states(n, seed)
@@ -382,6 +403,8 @@ class Run:
         nt, _, npar = self.table.shape
         if self.integrator == 2:
             lib().orc_set_langevin(_p(self.rng), _p(self.old_beta), float(self.alpha))
+        if self.integrator == 3:
+            lib().orc_set_npt(_p(self.ts), _p(self.bs), float(self.mass_t), float(self.mass_p), float(self.P))
         rc = lib().orc_run_timeblock(
             self.n, _p(self.r), _p(self.v), _p(self.f), _p(self.m), _p(self.img), _p(self.ptype),
             _p(self.box), _p(self.table), npar, nt, self.kind, self.cutmode, self.nblist_kind,

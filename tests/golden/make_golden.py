@@ -475,6 +475,50 @@ def case_rdf_typed():
     print("rdf_typed: done")
 
 
+def case_lj256_npt():
+    """NPT_Atomic (integrators/NPT_Atomic.py) on an LJ liquid started from a
+    jittered FCC lattice well above the target pressure, so the barostat
+    moves the box from the first step: two timeblocks of 8 steps with
+    ScalarSaver(2) saving U, W, K and Vol and ConfigurationSaver frames with
+    their boxes (include_simbox).  The thermostat and barostat
+    states are read from gamdpy's device arrays after the kernel test step
+    and after the run."""
+    gp = _import_gamdpy_cached()
+    pos, box = lj_fcc_input([4, 4, 4], 0.973, seed=5, jitter=0.1)
+    vel = mb_velocities(len(pos), 2.0, seed=5)
+    conf = gp.Configuration(D=3, compute_flags={"Vol": True})
+    conf["r"] = pos.copy()
+    conf.simbox = gp.Orthorhombic(3, box)
+    conf["m"] = 1.0
+    conf["v"] = vel
+    params = [1.0, 1.0, 2.5]
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon), params=params, max_num_nbs=300)
+    T, tau, P, tau_p, dt = 2.0, 0.4, 4.7, 2.0, 0.004
+    integ = gp.integrators.NPT_Atomic(temperature=T, tau=tau, pressure=P, tau_p=tau_p, dt=dt)
+    r0, v0 = conf["r"].copy(), conf["v"].copy()
+    t0 = time.time()
+    sim = gp.Simulation(conf, pp, integ, [gp.ConfigurationSaver(include_simbox=True), gp.ScalarSaver(2)],
+                        num_timeblocks=2, steps_per_timeblock=8, compute_plan=plan("N squared", 0.5),
+                        storage="memory", timing=False)
+    ts_test = integ.d_thermostat_state.copy_to_host()
+    bs_test = integ.d_barostat_state.copy_to_host()
+    for _ in sim.run_timeblocks():
+        pass
+    ts = integ.d_thermostat_state.copy_to_host()
+    bs = integ.d_barostat_state.copy_to_host()
+    print(f"lj256_npt: {time.time() - t0:.1f}s  box={conf.simbox.lengths} ts={ts} bs={bs}")
+    np.savez_compressed(
+        os.path.join(HERE, "lj256_npt.npz"),
+        r0=r0, v0=v0, box0=box, sigma=np.float32(1.0), epsilon=np.float32(1.0), cut=np.float32(2.5),
+        temperature=np.float32(T), tau=np.float32(tau), pressure=np.float32(P), tau_p=np.float32(tau_p),
+        dt=np.float32(dt), nblist="N squared", skin=np.float32(0.5), blocks=2, steps=8, every=2,
+        r=conf["r"], v=conf["v"], r_im=conf.r_im, box=conf.simbox.lengths.copy(), scalars=sim.output["scalars"],
+        scalar_names=np.array(sim.output.attrs["scalar_names"]), ts_after_test=ts_test, bs_after_test=bs_test,
+        thermostat_state=ts, barostat_state=bs, frames=np.asarray(sim.output["block"]),
+        frame_boxes=np.asarray(sim.output["sim_box"]),
+    )
+
+
 CASES = {
     "known_answers": case_known_answers,
     "lj256_sf": case_lj256_sf,
@@ -488,6 +532,7 @@ CASES = {
     "chain200_bonds": case_chain200_bonds,
     "chain1200_cells": case_chain1200_cells,
     "chain200_nve": case_chain200_nve,
+    "lj256_npt": case_lj256_npt,
 }
 
 if __name__ == "__main__":

@@ -110,7 +110,8 @@ def test_runtime_action_validation():
         ss.setup(conf, 2, 4, out)
     ss.setup(conf, 2, 16, out)
     assert out["scalars"].shape == (2, 4, 3) and out.attrs["scalar_names"] == ["U", "W", "K"]
-    rows = np.arange(20, dtype=np.float64).reshape(4, 5)
+    rows = np.arange(24, dtype=np.float64).reshape(4, 6)
+    rows[:, 5] = 0.0  # no per-step volume: a fixed box
     ss.update_from_rows(1, rows, out, 1.0)
     U, K = gp.extract_scalars(out, ["U", "K"], first_block=1)
     assert np.array_equal(U, rows[:, 0]) and np.array_equal(K, rows[:, 3])

@@ -154,12 +154,14 @@ def test_force_error_against_float64(oracle):
     assert rel_rms(f_gpu, f_ref32) < FORCE_TOL
 
 
-def test_persistent_small_system_cell_request_vs_oracle(oracle, monkeypatch):
+@pytest.mark.parametrize("n", [2048, 3072])
+def test_persistent_small_system_cell_request_vs_oracle(oracle, monkeypatch, n):
     """Up to 3072 particles the persistent kernel answers a cell-list request
-    with the N^2 build: the same sets as the oracle's cell build, and the same
-    forces to float32 round-off."""
+    with the N^2 build over positions staged in shared memory (48 KiB at
+    3072, beyond the default limit with the kernel's static shared memory):
+    the same sets as the oracle's cell build, and the same forces to float32
+    round-off."""
     monkeypatch.setenv("GDB_CLUSTER", "0")
-    n = 2048
     conf = workloads.ka_configuration(n, seed=19, jitter=0.25)
     L = conf.simbox.lengths
     table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])

@@ -201,3 +201,49 @@ def test_oracle_molecules_vs_gamdpy(oracle):
         got = np.asarray(pair[k], np.float64) + bond[k]
         ref = d[k].astype(np.float64)
         assert np.sqrt(np.mean((got - ref) ** 2) / np.mean(ref ** 2)) < 1e-5, k
+
+
+def run_npt_golden(oracle, d):
+    """The oracle through gamdpy's sequence for lj256_npt: Simulation's one
+    test step on the device copy (Simulation.py:200-211; the configuration
+    and the box are uploaded again afterwards, the thermostat and barostat
+    states keep the step), then the timeblocks."""
+    tab = oracle.param_table([d["sigma"], d["epsilon"], d["cut"]])
+    run = oracle.Run(d["r0"], d["v0"], 1.0, None, d["box0"], tab, nblist=str(d["nblist"]), skin=float(d["skin"]),
+                     max_nbs=300, integrator="NPT_Atomic", dt=float(d["dt"]), temperature=float(d["temperature"]),
+                     tau=float(d["tau"]), pressure=float(d["pressure"]), tau_p=float(d["tau_p"]),
+                     every=int(d["every"]))
+    run.run_timeblock(1)
+    states_test = (run.ts.copy(), run.bs.copy())
+    run.r[:] = d["r0"]
+    run.v[:] = d["v0"]
+    run.img[:] = 0
+    run.box[:] = d["box0"]
+    run.have_list.value = 0
+    rows = np.array([run.run_timeblock(int(d["steps"])) for _ in range(int(d["blocks"]))])
+    return run, rows, states_test
+
+
+def test_npt_atomic_trajectory_vs_gamdpy(oracle):
+    """NPT_Atomic restated in the oracle against gamdpy's own run: states
+    after the test step and after two timeblocks, the box, positions,
+    velocities and the saved U, W, K to float32 round-off (the reference sums
+    K and W with float32 atomics in an undefined order)."""
+    d = golden("lj256_npt")
+    run, rows, (ts_t, bs_t) = run_npt_golden(oracle, d)
+    assert np.allclose(ts_t, d["ts_after_test"], rtol=1e-5, atol=1e-7)
+    assert np.allclose(bs_t, d["bs_after_test"], rtol=1e-5, atol=1e-7)
+    assert np.allclose(run.box, d["box"], rtol=2e-7, atol=0)
+    assert abs(run.ts[0] - d["thermostat_state"][0]) <= 1e-5 * abs(d["thermostat_state"][0])
+    assert abs(run.bs[0] - d["barostat_state"][0]) <= 1e-5 * abs(d["barostat_state"][0])
+    assert abs(run.bs[2] - d["barostat_state"][2]) <= 1e-6 * d["barostat_state"][2]
+    assert np.abs(run.r - d["r"]).max() < 1e-5
+    assert np.array_equal(run.img, d["r_im"])
+    assert rel_rms(run.v, d["v"]) < 1e-5
+    cols = {"U": 0, "W": 1, "K": 2}
+    for c, nm in enumerate(d["scalar_names"]):
+        if str(nm) in cols:
+            # 1e-5: the virial sum cancels (pairs of both signs), and the box
+            # feeds every float32 rounding of the run back into the forces
+            ref = d["scalars"][:, :, c]
+            assert np.abs(rows[:, :, cols[str(nm)]] - ref).max() <= 1e-5 * np.abs(ref).max(), nm
