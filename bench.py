@@ -205,7 +205,20 @@ def ncu_traffic_per_atom_step():
 def trace_summary(tags, ns):
     """Per-phase times from the persistent kernel's barrier trace (tags:
     1 step, 2 evaluation, 3 rebuild phase, 4 rebuild done, 5 start, 6 end of
-    block 0's step phase)."""
+    block 0's step phase; 7 and 8 the last block's arrival and release)."""
+    tags, ns = np.asarray(tags), np.asarray(ns)
+    order = np.argsort(ns, kind="stable")
+    tags, ns = tags[order], ns[order]
+    # the step barrier split: block 0's phase end -> last arrival -> release
+    # -> block 0 past the barrier (tags 7 and 8 come from the last block)
+    arrive_us, book_us, release_us = [], [], []
+    for k in range(len(tags) - 3):
+        if tags[k] == 6 and tags[k + 1] == 7 and tags[k + 2] == 8 and tags[k + 3] == 1:
+            arrive_us.append((ns[k + 1] - ns[k]) / 1e3)
+            book_us.append((ns[k + 2] - ns[k + 1]) / 1e3)
+            release_us.append((ns[k + 3] - ns[k + 2]) / 1e3)
+    keep = (tags != 7) & (tags != 8)
+    tags, ns = tags[keep], ns[keep]
     step_us, rebuild_us, phase_us, sphase_us, bar_us = [], [], [], [], []
     start = None
     for k in range(1, len(tags)):
@@ -230,7 +243,9 @@ def trace_summary(tags, ns):
             "step_phase_us_median": med(sphase_us), "step_barrier_us_median": med(bar_us),
             "step_us_mean": float(np.mean(step_us)) if step_us else None, "rebuilds": len(rebuild_us),
             "rebuild_us_median": med(rebuild_us),
-            "rebuild_phase_us": [round(x, 1) for x in phase_us[:5]]}
+            "rebuild_phase_us": [round(x, 1) for x in phase_us[:5]],
+            "barrier_split_us_median": {"to_last_arrival": med(arrive_us), "bookkeeping": med(book_us),
+                                        "release_to_block0": med(release_us)}}
 
 
 def cpu_reference(args, n, steps, seed=0):

@@ -82,17 +82,34 @@ struct DevCtrl {
 
 // Phase trace (block 0, thread 0 of the persistent kernel): one entry per
 // barrier with a tag naming the phase that just finished.
-enum TraceTag { TR_STEP = 1, TR_EVAL = 2, TR_REBUILD_PHASE = 3, TR_REBUILD_DONE = 4, TR_START = 5, TR_STEP_PHASE = 6 };
+enum TraceTag {
+    TR_STEP = 1,
+    TR_EVAL = 2,
+    TR_REBUILD_PHASE = 3,
+    TR_REBUILD_DONE = 4,
+    TR_START = 5,
+    TR_STEP_PHASE = 6,
+    TR_BAR_LAST_IN = 7,  // the last block to arrive at a grid barrier, before its bookkeeping
+    TR_BAR_RELEASE = 8   // the same block, releasing the others
+};
+
+// Entry by the last block of a grid barrier (any block index): the slot is
+// taken atomically, as block 0 writes its own entries meanwhile.
+__device__ __forceinline__ void trace_mark_last(DevCtrl *c, int tag) {
+    if (c->trace && threadIdx.x == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        const int k = atomicAdd(&c->trace_len, 1);
+        if (k < c->trace_cap) c->trace[k] = ((unsigned long long)tag << 56) | (t & 0x00ffffffffffffffULL);
+    }
+}
 
 __device__ __forceinline__ void trace_mark(DevCtrl *c, int tag) {
     if (c->trace && blockIdx.x == 0 && threadIdx.x == 0) {
         unsigned long long t;
         asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-        const int k = c->trace_len;
-        if (k < c->trace_cap) {
-            c->trace[k] = ((unsigned long long)tag << 56) | (t & 0x00ffffffffffffffULL);
-            c->trace_len = k + 1;
-        }
+        const int k = atomicAdd(&c->trace_len, 1);
+        if (k < c->trace_cap) c->trace[k] = ((unsigned long long)tag << 56) | (t & 0x00ffffffffffffffULL);
     }
 }
 

@@ -144,15 +144,27 @@ __device__ inline void run_steps(const SimArgs &a0, const PairEntry *s_tab, int 
     int cur = cur0;
     const int rounds = (a.n + (int)blockDim.x / TP - 1) / ((int)blockDim.x / TP);  // partial rows per step
     trace_mark(ctrl, TR_START);
+    __shared__ int s_flags[2];
     for (int s = 0; s < nsteps + do_eval; s++) {
         if (INTEG == GDB_INTEGRATOR_NPT) npt_refresh_box(a_npt);
-        if (*(volatile int *)&ctrl->rebuild) {
+        // the rebuild flag and the step index, read together by one thread
+        // (the step index does not change across a rebuild)
+        if (threadIdx.x == 0) {
+            const int rb = *(volatile int *)&ctrl->rebuild;
+            const int st = *(volatile int *)&ctrl->step;
+            s_flags[0] = rb;
+            s_flags[1] = st;
+        }
+        __syncthreads();
+        const int rebuild = s_flags[0];
+        const int step = s_flags[1];
+        __syncthreads();  // s_flags is written again next iteration
+        if (rebuild) {
             if (INTEG == GDB_INTEGRATOR_NPT) npt_cell_grid(a_npt);
             const bool ok = a.fma ? rebuild_phases<true>(a, cur, g, sync, scr, spos)
                                   : rebuild_phases<false>(a, cur, g, sync, scr, spos);
             if (!ok) return;
         }
-        const int step = *(volatile int *)&ctrl->step;
         bool ok;
         if (s < nsteps) {
             phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g);

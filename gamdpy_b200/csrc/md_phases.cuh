@@ -133,12 +133,14 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
     asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
-// Arrival is hierarchical: an acq_rel add on the counter of the block's group
-// of 16 (after a CTA barrier, so the block's writes are ordered before it);
-// the last of a group adds to the top counter, and the last there has seen
+// Arrival is an acq_rel add (after a CTA barrier, so the block's writes are
+// ordered before it): on one counter for grids of up to BAR_FLAT_MAX blocks,
+// hierarchical above (the counter of the block's group of 16, and the last
+// of a group adds to the top counter).  The last block to arrive has seen
 // every block's writes.  It runs `last`, resets the counters and publishes the
 // next generation with a release store; waiters poll it with acquire loads.
 constexpr int BAR_GROUP = 16;
+constexpr int BAR_FLAT_MAX = 160;
 
 template <typename F>
 __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
@@ -154,7 +156,9 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
         const unsigned gsize = min((unsigned)BAR_GROUP, gridDim.x - grp * BAR_GROUP);
         const unsigned ngroups = (gridDim.x + BAR_GROUP - 1) / BAR_GROUP;
         bool top = false;
-        if (atom_add_acq_rel_gpu(&c->bar_group[grp], 1u) == gsize - 1) {
+        if (gridDim.x <= BAR_FLAT_MAX) {
+            top = atom_add_acq_rel_gpu(&c->bar_count, 1u) == gridDim.x - 1;
+        } else if (atom_add_acq_rel_gpu(&c->bar_group[grp], 1u) == gsize - 1) {
             c->bar_group[grp] = 0;  // no block of this group arrives again before the release
             top = atom_add_acq_rel_gpu(&c->bar_count, 1u) == ngroups - 1;
         }
@@ -182,10 +186,12 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
     __syncthreads();
     if (!s_ok) return false;
     if (s_last) {
+        trace_mark_last(c, TR_BAR_LAST_IN);
         last();
         __syncthreads();
         if (threadIdx.x == 0) {
             c->bar_count = 0;
+            trace_mark_last(c, TR_BAR_RELEASE);
             st_release_gpu(&c->bar_gen, *(volatile unsigned *)&c->bar_gen + 1u);
         }
         __syncthreads();
@@ -884,9 +890,13 @@ __device__ __forceinline__ void neighbour_loop(const SimArgs &a, const float4 *p
     const size_t cstride = (size_t)a.stride;  // int4 units between chunks
     // the index chunks of the next two iterations are loaded before this
     // one's positions: the list streams from HBM, so its latency overlaps the
-    // work (measured on B200: two ahead beats one and three)
-    int4 jn = sub < nch ? load<NC>(base + sub * cstride) : make_int4(i, i, i, i);
-    int4 jn2 = sub + TP < nch ? load<NC>(base + (sub + TP) * cstride) : make_int4(i, i, i, i);
+    // work (measured on B200: two ahead beats one and three).  The first two
+    // are loaded without waiting for the count: every slot has max_nbs + 4
+    // entries, so their guard is a constant and the count's latency overlaps
+    // theirs (entries past the count are never used).
+    const int chunks_alloc = (a.max_nbs + NB_CHUNK) / NB_CHUNK;
+    int4 jn = sub < chunks_alloc ? load<NC>(base + sub * cstride) : make_int4(i, i, i, i);
+    int4 jn2 = sub + TP < chunks_alloc ? load<NC>(base + (sub + TP) * cstride) : make_int4(i, i, i, i);
     for (int ch = sub; ch < nch; ch += TP) {
         const int4 jj = jn;
         jn = jn2;
@@ -1113,13 +1123,10 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
     const bool rec = MODE == MODE_EVAL || INTEG == GDB_INTEGRATOR_NPT || (a.every > 0 && step % a.every == 0);
     const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
     const int ppar = (step & 1) ^ 1;
+    // independent loads, issued together (one latency after the barrier)
     const bool shift_pending = ctrl->pending[ppar] != 0;
-    float shx = 0.f, shy = 0.f, shz = 0.f;
-    if (shift_pending) {
-        shx = ctrl->shift[ppar][0];
-        shy = ctrl->shift[ppar][1];
-        shz = ctrl->shift[ppar][2];
-    }
+    const float shx0 = ctrl->shift[ppar][0], shy0 = ctrl->shift[ppar][1], shz0 = ctrl->shift[ppar][2];
+    const float shx = shift_pending ? shx0 : 0.f, shy = shift_pending ? shy0 : 0.f, shz = shift_pending ? shz0 : 0.f;
     const float xi = ctrl->xi;
     NptStep ns;
     if (INTEG == GDB_INTEGRATOR_NPT && MODE == MODE_STEP) ns = npt_step_consts(a, ctrl);
@@ -1240,15 +1247,39 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
     double tot[NQ];
 #pragma unroll
     for (int q = 0; q < NQ; q++) tot[q] = 0.0;
+    // Each thread sums rows threadIdx.x, + blockDim.x, ... in that order; the
+    // rows of a batch are loaded before they are added, so several loads are
+    // in flight (the same sums as one row at a time, bit for bit).
+    const int bs = blockDim.x;
     if (full) {
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) {
+        int b = threadIdx.x;
+        for (; b + 3 * bs < nblocks; b += 4 * bs) {
+            double v[4][NQ];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int q = 0; q < NQ; q++) v[u][q] = __ldcg(a.partials + (size_t)(b + u * bs) * NQ + q);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int q = 0; q < NQ; q++) tot[q] += v[u][q];
+        }
+        for (; b < nblocks; b += bs) {
 #pragma unroll
             for (int q = 0; q < NQ; q++) tot[q] += __ldcg(a.partials + (size_t)b * NQ + q);
         }
         block_sum<NQ>(tot, s_red);
     } else if (needk) {
         double t1[1] = {0.0};
-        for (int b = threadIdx.x; b < nblocks; b += blockDim.x) t1[0] += __ldcg(a.partials + (size_t)b * NQ);
+        int b = threadIdx.x;
+        for (; b + 7 * bs < nblocks; b += 8 * bs) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = __ldcg(a.partials + (size_t)(b + u * bs) * NQ);
+#pragma unroll
+            for (int u = 0; u < 8; u++) t1[0] += v[u];
+        }
+        for (; b < nblocks; b += bs) t1[0] += __ldcg(a.partials + (size_t)b * NQ);
         block_sum<1>(t1, s_red);
         tot[0] = t1[0];
     }

@@ -88,6 +88,35 @@ def test_lists_vs_oracle_larger(oracle, n, nblist):
     assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
 
 
+def test_forces_with_positions_outside_the_box(oracle):
+    """Positions uploaded outside [-L/2, L/2] (some shifted by a whole box
+    length, as gamdpy accepts them): every pair is taken on the minimum
+    image.  Forces equal the oracle's on the uploaded positions, and after
+    two steps (every position wrapped into the box) on the new ones."""
+    conf = workloads.ka_configuration(20000, seed=23, jitter=0.2)
+    L = conf.simbox.lengths
+    r = conf["r"].copy()
+    r -= (L * np.round(r / L)).astype(np.float32)  # the jittered lattice into the box, then some out
+    rng = np.random.default_rng(5)
+    pick = rng.choice(len(r), 500, replace=False)
+    r[pick] += (rng.integers(-1, 2, size=(500, 3)) * L).astype(np.float32)
+    assert np.any(np.abs(r) > L / 2)
+    table = oracle.param_table([workloads.KA_SIGMA, workloads.KA_EPSILON, workloads.KA_CUT])
+    sim = make_sim(r, L, conf.ptype, table, nblist=_lib.NBLIST_CELLS, skin=0.3)
+    sim.eval_forces()
+    cps = float(np.float32(2.5) + np.float32(0.3))
+    ref_list, _ = oracle.nblist_nsq(r, L, cps, 300, fma=1)
+    res = oracle.forces(r, conf.ptype, L, table, ref_list, fma=1)
+    assert rel_rms(sim.download()["f"], res["f"]) < FORCE_TOL
+    sim.run(0.0, 2)  # each step wraps by one box length: 1.5 L out needs two
+    st = sim.download()
+    out = np.argwhere(np.abs(st["r"]) > L / 2)
+    assert len(out) == 0, (out[:5], st["r"][out[:5, 0]], r[out[:5, 0]], L / 2)
+    ref_list, _ = oracle.nblist_nsq(st["r"], L, cps, 300, fma=1)
+    res = oracle.forces(st["r"], conf.ptype, L, table, ref_list, fma=1)
+    assert rel_rms(st["f"], res["f"]) < FORCE_TOL
+
+
 @pytest.mark.parametrize("n,face", [(1372, False), (1372, True), (600, False), (900, True), (20000, True)])
 def test_cell_build_paths_vs_oracle(oracle, n, face):
     """Both build paths: >= 7 cells per dimension uses per-range periodic
