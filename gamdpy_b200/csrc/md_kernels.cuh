@@ -79,6 +79,7 @@ __device__ inline bool rebuild_phases(const SimArgs &a, int cur, Span g, const S
     auto none = [] {};
     if (a.nb_kind == GDB_NBLIST_NSQ) {
         phase_nbl_nsq<FMA, false>(a, cur, g, spos);
+        trace_mark(c, TR_REBUILD_PHASE);
         const bool ok = sync(c, [&] {
             if (threadIdx.x == 0) rebuild_done(c);
         });

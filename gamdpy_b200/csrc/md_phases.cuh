@@ -203,50 +203,90 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
 // neighbour-list phases
 // ---------------------------------------------------------------------------
 
-// N^2 build (interactions/nblist.py:88-143): one warp per particle, lanes
+// N^2 build (interactions/nblist.py:88-143): a warp per particle, lanes
 // stride over j, ballot + popc append hits in ascending j (deterministic).
-// With `spos` (shared memory for all n positions) the block first copies the
-// positions there, so the candidate loads are shared-memory loads; four
-// candidates per lane are loaded before they are tested.
+// A warp takes its particles two at a time (i and i + the number of warps):
+// every candidate is loaded once for both, and the two append chains are
+// independent.  With `spos` (shared memory for all n positions) the block
+// first copies the positions there, so the candidate loads are shared-memory
+// loads; four candidates per lane are loaded before they are tested.
 template <bool FMA, bool NC>
 __device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_span(), float4 *spos = nullptr) {
     const float4 *pos = cur_pos(a, cur);
     const float4 *src = pos;
     if (spos) {
-        for (int k = threadIdx.x; k < a.n; k += blockDim.x) spos[k] = pos[k];
+        // eight loads in flight per thread before they are stored
+        const int bd = blockDim.x;
+        for (int k0 = threadIdx.x; k0 < a.n; k0 += 8 * bd) {
+            float4 t[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (k0 + u * bd < a.n) t[u] = pos[k0 + u * bd];
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                if (k0 + u * bd < a.n) spos[k0 + u * bd] = t[u];
+        }
         __syncthreads();
         src = spos;
+        trace_mark(a.ctrl, TR_REBUILD_PHASE);
     }
+    // the arguments the loop reads, in registers: the list stores below could
+    // otherwise force them to be reloaded after every store
+    const int n = a.n, max_nbs = a.max_nbs, stride = a.stride;
+    const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz, cps2 = a.cps2;
+    const int *excl = a.excl;
+    const int *orig = a.orig;
+    int *nbl = a.nbl;
     const int lane = threadIdx.x & 31;
     const int warps = (g.nb * (int)blockDim.x) >> 5;
-    for (int i = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; i < a.n; i += warps) {
-        const float4 pi = spos ? src[i] : load<NC>(pos + i);
-        int count = 0;
-        for (int j0 = 0; j0 < a.n; j0 += 128) {
+    const unsigned below = (1u << lane) - 1u;
+    for (int i0 = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; i0 < n; i0 += 2 * warps) {
+        const int i1 = i0 + warps;
+        const bool has1 = i1 < n;
+        const float4 p0 = spos ? src[i0] : load<NC>(pos + i0);
+        const float4 p1 = has1 ? (spos ? src[i1] : load<NC>(pos + i1)) : p0;
+        const int u0 = excl ? orig[i0] : 0, u1 = (excl && has1) ? orig[i1] : 0;
+        int c0 = 0, c1 = 0;
+        for (int j0 = 0; j0 < n; j0 += 128) {
             float4 q[4];
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int j = j0 + 32 * u + lane;
-                q[u] = j < a.n ? (spos ? src[j] : load<NC>(pos + j)) : pi;
+                q[u] = j < n ? (spos ? src[j] : load<NC>(pos + j)) : p0;
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int j = j0 + 32 * u + lane;
-                bool hit = false;
-                if (j < a.n && j != i) hit = dist_sq_exact<FMA>(q[u], pi, a.Lx, a.Ly, a.Lz) < a.cps2;
-                if (hit && a.excl) hit = !excluded(a, a.orig[i], a.orig[j]);
-                const unsigned m = __ballot_sync(0xffffffffu, hit);
-                if (hit) {
-                    const int k = count + __popc(m & ((1u << lane) - 1u));
-                    if (k < a.max_nbs) a.nbl[nbl_index(i, k, a.stride)] = j;
+                const bool in = j < n;
+                bool h0 = in && j != i0 && dist_sq_exact<FMA>(q[u], p0, Lx, Ly, Lz) < cps2;
+                bool h1 = has1 && in && j != i1 && dist_sq_exact<FMA>(q[u], p1, Lx, Ly, Lz) < cps2;
+                if (excl) {
+                    if (h0) h0 = !excluded(a, u0, orig[j]);
+                    if (h1) h1 = !excluded(a, u1, orig[j]);
                 }
-                count += __popc(m);
+                const unsigned m0 = __ballot_sync(0xffffffffu, h0);
+                const unsigned m1 = __ballot_sync(0xffffffffu, h1);
+                if (h0) {
+                    const int k = c0 + __popc(m0 & below);
+                    if (k < max_nbs) nbl[nbl_index(i0, k, stride)] = j;
+                }
+                if (h1) {
+                    const int k = c1 + __popc(m1 & below);
+                    if (k < max_nbs) nbl[nbl_index(i1, k, stride)] = j;
+                }
+                c0 += __popc(m0);
+                c1 += __popc(m1);
             }
         }
         if (lane == 0) {
-            a.nbc[i] = count;
-            a.rref[i] = pi;
-            atomicMax(&a.ctrl->maxcount, count);
+            a.nbc[i0] = c0;
+            a.rref[i0] = p0;
+            atomicMax(&a.ctrl->maxcount, c0);
+            if (has1) {
+                a.nbc[i1] = c1;
+                a.rref[i1] = p1;
+                atomicMax(&a.ctrl->maxcount, c1);
+            }
         }
     }
 }
