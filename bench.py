@@ -660,25 +660,24 @@ def run_lj_small(args):
         pg.destroy_process_group()
 
 
-def run_lj_large(args):
-    """Large-N LJ with on-the-fly structure: FCC 128^3 = 8 388 608 particles at
-    rho = 0.84, T = 1.0 (seeded), shifted-force rc = 2.5, NVE dt = 0.004, cell
-    lists skin 0.5; every 100 steps the RDF over [0, 5) with 1000 bins
-    (integer counts) and S(q) on the q-vectors of the first 200 |n|^2 shells
-    (the reference's non-negative generator), both from the device-resident
-    state.  MATS counts the analysis device time too (CUDA events on the
-    library's stream).  --lj-cells sets a smaller lattice for profiling."""
+def measure_lj_large(local, cells, steps, warmup, seed=0, tp=0):
+    """Large-N LJ with on-the-fly structure: FCC cells^3 (128^3 = 8 388 608
+    particles) at rho = 0.84, T = 1.0 (seeded), shifted-force rc = 2.5, NVE
+    dt = 0.004, cell lists skin 0.5; every 100 steps the RDF over [0, 5) with
+    1000 bins (integer counts) and S(q) on the q-vectors of the first 200
+    |n|^2 shells (the reference's non-negative generator), both from the
+    device-resident state.  Device times (CUDA events on the library's
+    stream) of MD, RDF and S(q), seconds; wall times of the update() calls."""
     import gamdpy_b200 as gp
     from gamdpy_b200 import workloads
-    rank, world, local, pg = dist_setup(args)
-    c = args.lj_cells
-    conf = workloads.lj_configuration([c, c, c], 0.84, 1.0, seed=rank)
+    c = cells
+    conf = workloads.lj_configuration([c, c, c], 0.84, 1.0, seed=seed)
     n = conf.N
     pp = workloads.lj_pair_potential(cut=2.5, shifted_force=True, max_num_nbs=200)
     every = 100
-    nblocks = max(1, args.steps // every)
+    nblocks = max(1, steps // every)
     steps = nblocks * every
-    plan = {"pb": 256, "tp": 1, "lanes": args.tp, "skin": 0.5, "UtilizeNIII": False, "gridsync": False,
+    plan = {"pb": 256, "tp": 1, "lanes": tp, "skin": 0.5, "UtilizeNIII": False, "gridsync": False,
             "nblist": "linked lists"}
     sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.004), [], num_timeblocks=nblocks, steps_per_timeblock=every,
                         compute_plan=plan, storage="memory", device=local)
@@ -688,14 +687,13 @@ def run_lj_large(args):
     L = float(conf.simbox.lengths[0])
     sq.generate_q_vectors(2 * np.pi * np.sqrt(237.5) / L)
     nq = len(sq.q_vectors)
-    dev.run(0.0, max(3, args.warmup))
+    dev.run(0.0, max(3, warmup))
     rdf.update()
     sq.update()
-    barrier(pg)
     clocks = ClockSampler(local)
     clocks.start()
-    t_md = t_rdf = t_sq = 0.0  # device times (CUDA events on the library's stream)
-    w_rdf = w_sq = 0.0  # wall times of the update() calls
+    t_md = t_rdf = t_sq = 0.0
+    w_rdf = w_sq = 0.0
     each_rdf, each_sq = [], []
     t0 = time.perf_counter()
     for b in range(nblocks):
@@ -713,24 +711,39 @@ def run_lj_large(args):
         w_sq += t3 - t2
     wall = time.perf_counter() - t0
     clock_info = clocks.stop()
-    t_all = allreduce_max(pg, t_md + t_rdf + t_sq, local)
     pairs = float(rdf.rdf_list[-1].sum())  # ordered pairs counted in one update
+    out = {"workload": f"LJ SF rc=2.5, FCC {c}^3 rho=0.84 T=1.0, NVE dt=0.004, cells skin 0.5; RDF r<5 "
+                       "1000 bins and S(q) on the first 200 |n|^2 shells every 100 steps",
+           "n": n, "nq": nq, "steps": steps, "t_md": t_md, "t_rdf": t_rdf, "t_sq": t_sq,
+           "mats": n * steps / (t_md + t_rdf + t_sq) / 1e6, "md_ms_per_step": t_md * 1e3 / steps,
+           "rdf_ms_per_update": t_rdf * 1e3 / nblocks, "rdf_pairs_per_update": pairs,
+           "rdf_pairs_per_s": pairs * nblocks / t_rdf if t_rdf > 0 else None,
+           "sq_ms_per_update": t_sq * 1e3 / nblocks, "sq_terms_per_s": n * nq * nblocks / t_sq if t_sq > 0 else None,
+           "rdf_ms_min_max": [min(each_rdf), max(each_rdf)], "sq_ms_min_max": [min(each_sq), max(each_sq)],
+           "rdf_wall_ms_per_update": w_rdf * 1e3 / nblocks, "sq_wall_ms_per_update": w_sq * 1e3 / nblocks,
+           "wall_s": wall, "timing": "device (CUDA events) for MD, RDF and S(q); wall times beside them",
+           "clocks": clock_info}
+    del sim, dev, rdf, sq
+    return out
+
+
+def run_lj_large(args):
+    """The large-N LJ workload with on-the-fly structure (measure_lj_large);
+    MATS counts the analysis device time too.  --lj-cells sets a smaller
+    lattice for profiling."""
+    rank, world, local, pg = dist_setup(args)
+    barrier(pg)
+    r = measure_lj_large(local, args.lj_cells, args.steps, args.warmup, seed=rank, tp=args.tp)
+    t_all = allreduce_max(pg, r["t_md"] + r["t_rdf"] + r["t_sq"], local)
+    n, steps = r["n"], r["steps"]
+    cfg = {k: v for k, v in r.items() if k not in ("t_md", "t_rdf", "t_sq", "mats", "steps", "clocks")}
+    cfg["l2"] = "working set of several GB > 126 MB L2, no flush"
     line = {
         "metric": f"MATS (million atom-timesteps/s), LJ N={n} NVE cells with RDF and S(q) every 100 steps, 1 B200",
         "value": n * steps * world / t_all / 1e6, "unit": "Matom-steps/s", "n_gpus": world, "steps": steps,
         "warmup": max(3, args.warmup), "ms_per_step": t_all * 1e3 / steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32 (f64 sums)", "data": "synthetic (seeded FCC lattice)",
-        "config": {"workload": f"LJ SF rc=2.5, FCC {c}^3 rho=0.84 T=1.0, NVE dt=0.004, cells skin 0.5; RDF r<5 "
-                               "1000 bins and S(q) on the first 200 |n|^2 shells every 100 steps",
-                   "n": n, "nq": nq, "md_ms_per_step": t_md * 1e3 / steps,
-                   "rdf_ms_per_update": t_rdf * 1e3 / nblocks, "rdf_pairs_per_update": pairs,
-                   "rdf_pairs_per_s": pairs * nblocks / t_rdf if t_rdf > 0 else None,
-                   "sq_ms_per_update": t_sq * 1e3 / nblocks, "sq_terms_per_s": n * nq * nblocks / t_sq if t_sq > 0 else None,
-                   "rdf_ms_min_max": [min(each_rdf), max(each_rdf)], "sq_ms_min_max": [min(each_sq), max(each_sq)],
-                   "rdf_wall_ms_per_update": w_rdf * 1e3 / nblocks, "sq_wall_ms_per_update": w_sq * 1e3 / nblocks,
-                   "wall_s": wall, "timing": "device (CUDA events) for MD, RDF and S(q); wall times beside them",
-                   "l2": "working set of several GB > 126 MB L2, no flush"},
-        "clocks": clock_info,
+        "config": cfg, "clocks": r["clocks"],
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -739,19 +752,17 @@ def run_lj_large(args):
         pg.destroy_process_group()
 
 
-def run_adjoint(args):
+def measure_adjoint(local, steps, warmup, seed=77, growth=True):
     """Adjoint workload: KA N=4096, rho 1.2, T 0.6, an NVE trajectory of
-    --steps steps (2000 by default) with checkpoints every 50; loss = squared
-    deviations of <U>/N and P plus the L2 distance of the soft A-A g(r) from
-    targets made at eps_AB = 1.45, sigma_AB = 0.82; one gradient with respect
-    to the 6 pair parameters per timed iteration."""
+    `steps` steps with checkpoints every 50; loss = squared deviations of
+    <U>/N and P plus the L2 distance of the soft A-A g(r) from targets made at
+    eps_AB = 1.45, sigma_AB = 0.82; gradients with respect to the 6 pair
+    parameters (wall times of whole gradients through AdjointNVE)."""
     import torch
 
     from gamdpy_b200 import adjoint, workloads
-    rank, world, local, pg = dist_setup(args)
     n = 4096
-    steps = args.steps
-    conf = workloads.ka_configuration(n, rho=1.2, temperature=0.6, seed=77 + rank)
+    conf = workloads.ka_configuration(n, rho=1.2, temperature=0.6, seed=seed)
     rdf = {"bins": 40, "r_lo": 0.7, "r_hi": 2.7, "width": 0.05, "every": 10}
     cut = workloads.KA_CUT.astype(np.float64)
     eng = adjoint.AdjointNVE(conf, cut, dt=0.005, steps=steps, checkpoint_every=50, rdf=rdf, device=local)
@@ -773,10 +784,9 @@ def run_adjoint(args):
         loss.backward()
         return float(loss), th.grad.detach().numpy().copy()
 
-    for _ in range(max(1, min(args.warmup, 3))):
+    for _ in range(max(1, min(warmup, 3))):
         gradient()
-    reps = max(1, min(args.steps // 1000, 3)) if args.steps >= 1000 else 3
-    t0 = time.perf_counter()
+    reps = max(1, min(steps // 1000, 3)) if steps >= 1000 else 3
     tf = 0.0
     for _ in range(reps):
         t1 = time.perf_counter()
@@ -787,40 +797,55 @@ def run_adjoint(args):
     for _ in range(reps):
         loss, g = gradient()
     t_grad = (time.perf_counter() - t0) / reps
-    # truncated adjoint (window of 100 steps) on the same trajectory, and the
-    # growth of the exact gradient with the horizon (chaos: ~exp(lambda t))
+    # truncated adjoint (window of 100 steps) on the same trajectory
     eng.set_window(100)
     loss_w, g_w = gradient()
     eng.set_window(0)
-    growth = {}
-    for t in (50, 100, 200, 400, 800):
-        e2 = adjoint.AdjointNVE(conf, cut, dt=0.005, steps=t, checkpoint_every=50, rdf=rdf, device=local)
-        tgt = torch.tensor(e2.forward(theta(1.45, 0.82)))
-        th = torch.tensor(theta(1.5, 0.8), requires_grad=True)
-        adjoint.matching_loss(e2.observables(th), tgt, n, vol, dr).backward()
-        growth[str(t)] = float(np.linalg.norm(th.grad.detach().numpy()))
-    # the plain path on the same system and trajectory length (forward only)
-    c2 = workloads.ka_configuration(n, rho=1.2, temperature=0.6, seed=77 + rank)
-    sim = __import__("gamdpy_b200").Simulation(
-        c2, workloads.ka_pair_potential(), __import__("gamdpy_b200").integrators.NVE(dt=0.005), [],
-        num_timeblocks=1, steps_per_timeblock=steps, storage="memory", steps_in_kernel_test=0, device=local,
-        compute_plan={"pb": 64, "tp": 1, "lanes": 0, "skin": 0.3, "UtilizeNIII": False, "gridsync": False,
-                      "nblist": "linked lists"})
-    sim._sim.run(0.0, steps)
-    ms_plain = sim._sim.run(0.0, steps)
+    out = {"workload": f"KA-LJ NVE N={n} rho=1.2 T=0.6, {steps} steps, checkpoints every 50, "
+                       "loss = (<U>/N, P, soft g_AA(r)) vs targets at eps_AB=1.45 sigma_AB=0.82",
+           "n": n, "steps": steps, "rdf": rdf, "gradients_per_s": 1.0 / t_grad, "forward_ms": t_fwd * 1e3,
+           "gradient_ms": t_grad * 1e3, "backward_over_forward": (t_grad - t_fwd) / t_fwd, "loss": loss,
+           "gradient": [float(x) for x in g], "gradient_window100": [float(x) for x in g_w],
+           "gradient_order": "eps_AA, eps_AB, eps_BB, sigma_AA, sigma_AB, sigma_BB"}
+    if growth:
+        # the growth of the exact gradient with the horizon (chaos: ~exp(lambda t))
+        gr = {}
+        for t in (50, 100, 200, 400, 800):
+            e2 = adjoint.AdjointNVE(conf, cut, dt=0.005, steps=t, checkpoint_every=50, rdf=rdf, device=local)
+            tgt = torch.tensor(e2.forward(theta(1.45, 0.82)))
+            th = torch.tensor(theta(1.5, 0.8), requires_grad=True)
+            adjoint.matching_loss(e2.observables(th), tgt, n, vol, dr).backward()
+            gr[str(t)] = float(np.linalg.norm(th.grad.detach().numpy()))
+        out["exact_gradient_norm_vs_steps"] = gr
+        # the plain path on the same system and trajectory length (forward only)
+        import gamdpy_b200 as gp
+        c2 = workloads.ka_configuration(n, rho=1.2, temperature=0.6, seed=seed)
+        sim = gp.Simulation(c2, workloads.ka_pair_potential(), gp.integrators.NVE(dt=0.005), [], num_timeblocks=1,
+                            steps_per_timeblock=steps, storage="memory", steps_in_kernel_test=0, device=local,
+                            compute_plan={"pb": 64, "tp": 1, "lanes": 0, "skin": 0.3, "UtilizeNIII": False,
+                                          "gridsync": False, "nblist": "linked lists"})
+        sim._sim.run(0.0, steps)
+        out["plain_forward_ms"] = sim._sim.run(0.0, steps)
+    del eng
+    return out
+
+
+def run_adjoint(args):
+    """The adjoint workload (measure_adjoint): one gradient per timed
+    iteration, with the horizon study and the plain path beside it."""
+    rank, world, local, pg = dist_setup(args)
+    steps = args.steps
+    r = measure_adjoint(local, steps, args.warmup, seed=77 + rank, growth=True)
+    n, rdf = r["n"], r["rdf"]
+    t_grad = r["gradient_ms"] / 1e3
     line = {
         "metric": "adjoint gradients/s, KA N=4096 NVE trajectory, 6 pair parameters, 1 B200",
         "value": 1.0 / t_grad, "unit": "gradients/s", "n_gpus": world, "steps": steps, "warmup": 1,
         "ms_per_step": t_grad * 1e3 / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32 forward, f64 adjoint", "data": "synthetic (seeded KA lattice)",
-        "config": {"workload": f"KA-LJ NVE N={n} rho=1.2 T=0.6, {steps} steps, checkpoints every 50, "
-                               "loss = (<U>/N, P, soft g_AA(r)) vs targets at eps_AB=1.45 sigma_AB=0.82",
-                   "rdf": rdf},
-        "forward_ms": t_fwd * 1e3, "gradient_ms": t_grad * 1e3, "backward_over_forward": (t_grad - t_fwd) / t_fwd,
-        "plain_forward_ms": ms_plain, "loss": loss, "gradient": [float(x) for x in g],
-        "gradient_window100": [float(x) for x in g_w],
-        "exact_gradient_norm_vs_steps": growth,
-        "gradient_order": "eps_AA, eps_AB, eps_BB, sigma_AA, sigma_AB, sigma_BB",
+        "config": {"workload": r["workload"], "rdf": rdf},
+        **{k: r[k] for k in ("forward_ms", "gradient_ms", "backward_over_forward", "plain_forward_ms", "loss",
+                             "gradient", "gradient_window100", "exact_gradient_norm_vs_steps", "gradient_order")},
         "e2e": {"value": 1.0 / t_grad, "unit": "gradients/s", "h2d_bytes_per_step": n * 24 / steps,
                 "d2h_bytes_per_step": 8 * (3 + rdf["bins"]) / steps,
                 "note": "host initial state in, observables and gradient out, through AdjointNVE"},
@@ -828,8 +853,6 @@ def run_adjoint(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     barrier(pg)
-    if pg is not None:
-        pg.destroy_process_group()
 
 
 def main():
@@ -973,6 +996,14 @@ def main():
         }
         # the batch shape is the project's autotuner's choice (untimed)
         line["batch"] = measure_batch(local, 128, 1000, 500, 10, autotune=True, seed=2024 + rank)
+        # the large-N structure workload (200 steps: two RDF and S(q) updates)
+        # and one adjoint gradient of the 2000-step KA trajectory
+        for key, fn in (("lj8m", lambda: measure_lj_large(local, 128, 200, 10, seed=rank)),
+                        ("adjoint", lambda: measure_adjoint(local, 2000, 1, seed=77 + rank, growth=False))):
+            try:
+                line[key] = fn()
+            except Exception as e:  # a sub-measurement never costs the main line
+                line[key] = {"error": f"{type(e).__name__}: {e}"[:300]}
     if rank == 0 and world == 1:
         cps = max(1, min(50, args.steps))  # about 10 s of host work at N = 1M
         cmats, threads, secs, rebuilds = cpu_reference(args, n, cps)

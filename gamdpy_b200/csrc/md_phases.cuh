@@ -243,8 +243,8 @@ __device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_sp
     for (int i0 = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; i0 < n; i0 += 2 * warps) {
         const int i1 = i0 + warps;
         const bool has1 = i1 < n;
-        const float4 p0 = spos ? src[i0] : load<NC>(pos + i0);
-        const float4 p1 = has1 ? (spos ? src[i1] : load<NC>(pos + i1)) : p0;
+        const float4 p0 = NC ? load<true>(pos + i0) : src[i0];
+        const float4 p1 = has1 ? (NC ? load<true>(pos + i1) : src[i1]) : p0;
         const int u0 = excl ? orig[i0] : 0, u1 = (excl && has1) ? orig[i1] : 0;
         int c0 = 0, c1 = 0;
         for (int j0 = 0; j0 < n; j0 += 128) {
@@ -252,7 +252,10 @@ __device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_sp
 #pragma unroll
             for (int u = 0; u < 4; u++) {
                 const int j = j0 + 32 * u + lane;
-                q[u] = j < n ? (spos ? src[j] : load<NC>(pos + j)) : p0;
+                // one load kind per instantiation: the read-only path for the
+                // standalone kernel (never staged), plain loads from the
+                // staged copy or the coherent buffer otherwise
+                q[u] = j < n ? (NC ? load<true>(pos + j) : src[j]) : p0;
             }
 #pragma unroll
             for (int u = 0; u < 4; u++) {
