@@ -402,11 +402,11 @@ static void free_graphs(gdb_sim *h) {
 
 static int choose_tp(const gdb_sim *h) {
     if (h->tp_req > 0) return h->tp_req;
-    // about 131k lanes in flight, at most 16 per particle (measured on B200:
-    // 1 lane per particle at N = 1M, 2 at 65k; at 2k, 16 lanes 92-95 k TPS
-    // against 85-96 k with 32, whose per-step barrier varied more)
+    // about 131k lanes in flight (measured on B200: 1 lane per particle at
+    // N = 1M, 2 at 65k; at 2k, 32 lanes on 256 blocks 100 k TPS against 93 k
+    // with 16 lanes, once grids up to 320 blocks take the one-level barrier)
     int tp = 1;
-    while (tp < 16 && (long long)h->n * tp < 131072) tp *= 2;
+    while (tp < 32 && (long long)h->n * tp < 131072) tp *= 2;
     return tp;
 }
 

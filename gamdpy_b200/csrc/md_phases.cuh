@@ -140,7 +140,7 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
 // every block's writes.  It runs `last`, resets the counters and publishes the
 // next generation with a release store; waiters poll it with acquire loads.
 constexpr int BAR_GROUP = 16;
-constexpr int BAR_FLAT_MAX = 160;
+constexpr int BAR_FLAT_MAX = 320;
 
 template <typename F>
 __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
