@@ -46,10 +46,12 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_step(SimA
 // Synchronisation of the blocks that share one system, between phases.
 // `last` runs on one whole block after every block has arrived and before
 // any leaves; the call returns false when the wait was abandoned.
+// With `flag`, a block reports that one of its particles moved more than
+// skin/2; the block that runs `last` finds in *any whether any block did.
 struct GridSync {  // bounded software barrier over a cooperative grid
     template <typename F>
-    __device__ __forceinline__ bool operator()(DevCtrl *c, F last) const {
-        return grid_barrier(c, last);
+    __device__ __forceinline__ bool operator()(DevCtrl *c, F last, bool flag = false, int *any = nullptr) const {
+        return grid_barrier(c, last, flag, any);
     }
 };
 
@@ -62,9 +64,16 @@ __device__ __forceinline__ void cluster_barrier() {
 struct ClusterSync {
     int rank;
     template <typename F>
-    __device__ __forceinline__ bool operator()(DevCtrl *, F last) const {
+    __device__ __forceinline__ bool operator()(DevCtrl *c, F last, bool flag = false, int *any = nullptr) const {
+        if (flag && threadIdx.x == 0) c->rebuild_next = 1;
         cluster_barrier();
-        if (rank == 0) last();
+        if (rank == 0) {
+            if (any && threadIdx.x == 0) {
+                *any = c->rebuild_next;
+                c->rebuild_next = 0;
+            }
+            last();
+        }
         cluster_barrier();
         return true;
     }
@@ -145,21 +154,17 @@ __device__ inline void run_steps(const SimArgs &a0, const PairEntry *s_tab, int 
     int cur = cur0;
     const int rounds = (a.n + (int)blockDim.x / TP - 1) / ((int)blockDim.x / TP);  // partial rows per step
     trace_mark(ctrl, TR_START);
-    __shared__ int s_flags[2];
+    __shared__ StepCtl s_ctl;
+    __shared__ int s_any;  // a particle moved beyond skin/2 (the block running `last`)
     for (int s = 0; s < nsteps + do_eval; s++) {
         if (INTEG == GDB_INTEGRATOR_NPT) npt_refresh_box(a_npt);
-        // the rebuild flag and the step index, read together by one thread
-        // (the step index does not change across a rebuild)
-        if (threadIdx.x == 0) {
-            const int rb = *(volatile int *)&ctrl->rebuild;
-            const int st = *(volatile int *)&ctrl->step;
-            s_flags[0] = rb;
-            s_flags[1] = st;
-        }
+        // the rebuild flag, the step index and the state the step reads
+        // (momentum shift, thermostat), loaded together by one thread: none
+        // of them changes across a rebuild
+        if (threadIdx.x == 0) load_step_ctl(ctrl, &s_ctl);
         __syncthreads();
-        const int rebuild = s_flags[0];
-        const int step = s_flags[1];
-        __syncthreads();  // s_flags is written again next iteration
+        const int rebuild = s_ctl.rebuild;
+        const int step = s_ctl.step;
         if (rebuild) {
             if (INTEG == GDB_INTEGRATOR_NPT) npt_cell_grid(a_npt);
             const bool ok = a.fma ? rebuild_phases<true>(a, cur, g, sync, scr, spos)
@@ -168,19 +173,20 @@ __device__ inline void run_steps(const SimArgs &a0, const PairEntry *s_tab, int 
         }
         bool ok;
         if (s < nsteps) {
-            phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g);
+            const bool moved = phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g,
+                                                                                   &s_ctl);
             trace_mark(ctrl, TR_STEP_PHASE);
-            ok = sync(ctrl, [&] {
-                finalize_step<MODE_STEP, INTEG>(a, step, rounds, s_red);
-                if (threadIdx.x == 0 && ctrl->rebuild_next) {
-                    ctrl->rebuild = 1;
-                    ctrl->rebuild_next = 0;
-                }
-            });
+            ok = sync(
+                ctrl,
+                [&] {
+                    finalize_step<MODE_STEP, INTEG>(a, step, rounds, s_red);
+                    if (threadIdx.x == 0 && s_any) ctrl->rebuild = 1;
+                },
+                moved, &s_any);
             cur ^= 1;
             trace_mark(ctrl, TR_STEP);
         } else {
-            phase_step<TP, NT, INTEG, MODE_EVAL, false, true>(a, s_tab, nt, cur, step, s_red, g);
+            phase_step<TP, NT, INTEG, MODE_EVAL, false, true>(a, s_tab, nt, cur, step, s_red, g, &s_ctl);
             ok = sync(ctrl, [&] {
                 finalize_step<MODE_EVAL>(a, step, rounds, s_red);
                 if (threadIdx.x == 0) ctrl->work[(step + 1) & 1] = 0;

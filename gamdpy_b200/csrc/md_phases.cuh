@@ -142,8 +142,14 @@ __device__ __forceinline__ void st_release_gpu(unsigned *p, unsigned v) {
 constexpr int BAR_GROUP = 16;
 constexpr int BAR_FLAT_MAX = 320;
 
+// A block may arrive with a flag (a particle of it moved more than skin/2):
+// the arrival adds FLAG_ONE as well, so the last block learns from the
+// counter whether any block raised it (*any) without another read.
+constexpr unsigned BAR_FLAG_ONE = 1u << 20;  // counts live in the low 20 bits
+constexpr unsigned BAR_COUNT_MASK = BAR_FLAG_ONE - 1u;
+
 template <typename F>
-__device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
+__device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last, bool flag = false, int *any = nullptr) {
     __shared__ int s_last, s_ok;
     __syncthreads();
     if (threadIdx.x == 0 && *(volatile int *)&c->abort) {
@@ -155,13 +161,23 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last) {
         const unsigned grp = blockIdx.x / BAR_GROUP;
         const unsigned gsize = min((unsigned)BAR_GROUP, gridDim.x - grp * BAR_GROUP);
         const unsigned ngroups = (gridDim.x + BAR_GROUP - 1) / BAR_GROUP;
-        bool top = false;
+        bool top = false, raised = false;
+        const unsigned inc = 1u | (flag ? BAR_FLAG_ONE : 0u);
         if (gridDim.x <= BAR_FLAT_MAX) {
-            top = atom_add_acq_rel_gpu(&c->bar_count, 1u) == gridDim.x - 1;
-        } else if (atom_add_acq_rel_gpu(&c->bar_group[grp], 1u) == gsize - 1) {
-            c->bar_group[grp] = 0;  // no block of this group arrives again before the release
-            top = atom_add_acq_rel_gpu(&c->bar_count, 1u) == ngroups - 1;
+            const unsigned old = atom_add_acq_rel_gpu(&c->bar_count, inc);
+            top = (old & BAR_COUNT_MASK) == gridDim.x - 1;
+            raised = ((old + inc) >> 20) != 0u;
+        } else {
+            const unsigned oldg = atom_add_acq_rel_gpu(&c->bar_group[grp], inc);
+            if ((oldg & BAR_COUNT_MASK) == gsize - 1) {
+                c->bar_group[grp] = 0;  // no block of this group arrives again before the release
+                const unsigned ginc = 1u | (((oldg + inc) >> 20) != 0u ? BAR_FLAG_ONE : 0u);
+                const unsigned oldt = atom_add_acq_rel_gpu(&c->bar_count, ginc);
+                top = (oldt & BAR_COUNT_MASK) == ngroups - 1;
+                raised = ((oldt + ginc) >> 20) != 0u;
+            }
         }
+        if (top && any) *any = raised;
         s_last = top;
         s_ok = 1;
         if (!s_last) {
@@ -1146,6 +1162,34 @@ __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 
     }  // MODE_STEP
 }
 
+// Control state a step reads after the barrier, loaded at once by one thread
+// of the persistent kernels (StepCtl; NULL: read from ctrl here).
+struct StepCtl {
+    int rebuild, step, pending[2];
+    float shift[2][3];
+    float xi;
+};
+__device__ __forceinline__ void load_step_ctl(const DevCtrl *c, StepCtl *sc) {
+    const int rb = *(volatile const int *)&c->rebuild;
+    const int st = *(volatile const int *)&c->step;
+    const int p0 = *(volatile const int *)&c->pending[0], p1 = *(volatile const int *)&c->pending[1];
+    float sh[2][3];
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) sh[q][k] = *(volatile const float *)&c->shift[q][k];
+    const float xi = *(volatile const float *)&c->xi;
+    sc->rebuild = rb;
+    sc->step = st;
+    sc->pending[0] = p0;
+    sc->pending[1] = p1;
+#pragma unroll
+    for (int q = 0; q < 2; q++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) sc->shift[q][k] = sh[q][k];
+    sc->xi = xi;
+}
+
 // Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
 // only (MODE_EVAL).  A round is blockDim/TP consecutive particles.
 // Standalone launches (PERSIST false) take rounds g.b, g.b + g.nb, ... and
@@ -1154,11 +1198,12 @@ __device__ __forceinline__ void finish_particle(const SimArgs &a, int i, float4 
 // faster SMs take more) and write one row per round to partials[round], so
 // the fixed-order sum does not depend on which block ran which round.  Only
 // the sums the step needs are reduced: all of them on saved and reset steps,
-// the kinetic energy (NVT) otherwise.  Sets the rebuild flag when a particle
-// has moved more than skin/2 since the build.
+// the kinetic energy (NVT) otherwise.  Returns (persistent kernels) or sets
+// (standalone) the rebuild flag when a particle has moved more than skin/2
+// since the build.
 template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
-__device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
-                                  Span g = grid_span()) {
+__device__ inline bool phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
+                                  Span g = grid_span(), const StepCtl *sc = nullptr) {
     DevCtrl *ctrl = a.ctrl;
     const float4 *pos = cur_pos(a, cur);
     float4 *pos_next = cur_pos(a, cur ^ 1);
@@ -1166,11 +1211,14 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
     const bool rec = MODE == MODE_EVAL || INTEG == GDB_INTEGRATOR_NPT || (a.every > 0 && step % a.every == 0);
     const bool reset = MODE == MODE_STEP && a.reset_every > 0 && step % a.reset_every == 0;
     const int ppar = (step & 1) ^ 1;
-    // independent loads, issued together (one latency after the barrier)
-    const bool shift_pending = ctrl->pending[ppar] != 0;
-    const float shx0 = ctrl->shift[ppar][0], shy0 = ctrl->shift[ppar][1], shz0 = ctrl->shift[ppar][2];
+    // independent loads, issued together (one latency after the barrier), or
+    // the copy the persistent kernels loaded with the step index
+    const bool shift_pending = (sc ? sc->pending[ppar] : ctrl->pending[ppar]) != 0;
+    const float shx0 = sc ? sc->shift[ppar][0] : ctrl->shift[ppar][0];
+    const float shy0 = sc ? sc->shift[ppar][1] : ctrl->shift[ppar][1];
+    const float shz0 = sc ? sc->shift[ppar][2] : ctrl->shift[ppar][2];
     const float shx = shift_pending ? shx0 : 0.f, shy = shift_pending ? shy0 : 0.f, shz = shift_pending ? shz0 : 0.f;
-    const float xi = ctrl->xi;
+    const float xi = sc ? sc->xi : ctrl->xi;
     NptStep ns;
     if (INTEG == GDB_INTEGRATOR_NPT && MODE == MODE_STEP) ns = npt_step_consts(a, ctrl);
     const int per_block = blockDim.x / TP;
@@ -1256,15 +1304,13 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
             round += g.nb;
         }
     }
+    bool block_moved = false;
     if (MODE == MODE_STEP) {
-        // inside the persistent kernel other blocks may still be reading
-        // ctrl->rebuild for this step: stage the flag, the barrier promotes it
-        if (__syncthreads_or(moved) && threadIdx.x == 0) {
-            if (PERSIST)
-                ctrl->rebuild_next = 1;
-            else
-                ctrl->rebuild = 1;
-        }
+        // inside the persistent kernels other blocks may still be reading
+        // ctrl->rebuild for this step: the flag goes to the barrier, which
+        // raises it for the next step (the caller)
+        block_moved = __syncthreads_or(moved) != 0;
+        if (!PERSIST && block_moved && threadIdx.x == 0) ctrl->rebuild = 1;
     }
     if (!PERSIST) {
         block_sum<NQ>(red, s_red);
@@ -1273,6 +1319,7 @@ __device__ inline void phase_step(const SimArgs &a, const PairEntry *tab, int nt
             for (int q = 0; q < NQ; q++) a.partials[(size_t)g.b * NQ + q] = red[q];
         }
     }
+    return block_moved;
 }
 
 // Fixed-order float64 sum of `nblocks` partial rows (blocks or rounds) and the
