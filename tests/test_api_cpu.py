@@ -146,3 +146,30 @@ def test_bond_exclusions_equal_gamdpy():
     u, s, umm = gp.harmonic_bond_function(np.float32(1.2), [1.0, 3000.0])
     assert np.isclose(u, 0.5 * 3000 * 0.2 ** 2, rtol=1e-6) and np.isclose(s, -3000 * 0.2 / 1.2, rtol=1e-6)
     assert umm == 3000.0
+
+
+def test_autotune_cache_round_trip(tmp_path, monkeypatch):
+    """The autotuner's per-GPU cache: a stored plan is read back by key, and
+    entries under other keys stay (host logic only)."""
+    from gamdpy_b200 import simulation as S
+    monkeypatch.setenv("GAMDPY_B200_CACHE", str(tmp_path))
+    assert S._autotune_cache_load() == {}
+    S._autotune_cache_store("gpu|N=10", {"nblist": "N squared", "lanes": 4, "skin": 0.3})
+    S._autotune_cache_store("gpu|N=20", {"nblist": "linked lists", "lanes": 1, "skin": 0.5})
+    d = S._autotune_cache_load()
+    assert d["gpu|N=10"]["lanes"] == 4 and d["gpu|N=20"]["nblist"] == "linked lists"
+    assert (tmp_path / "autotune.json").exists()
+
+
+def test_trace_summary_splits_the_step_barrier():
+    """bench.trace_summary: block 0's marks give the step, phase and barrier
+    times; the last block's arrival and release marks (tags 7, 8, written
+    from another block, so possibly out of order) split the barrier."""
+    import bench
+    tags = [5, 6, 8, 7, 1, 6, 7, 8, 1]
+    ns = [0, 100, 300, 200, 400, 500, 650, 700, 800]
+    t = bench.trace_summary(tags, ns)
+    assert t["steps"] == 1 and abs(t["step_barrier_us_median"] - 0.3) < 1e-9
+    split = t["barrier_split_us_median"]
+    assert abs(split["to_last_arrival"] - 0.125) < 1e-9
+    assert abs(split["bookkeeping"] - 0.075) < 1e-9 and abs(split["release_to_block0"] - 0.1) < 1e-9

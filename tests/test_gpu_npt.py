@@ -124,3 +124,53 @@ def test_npt_state_point():
     assert abs(n / V.mean() - rho) < 0.015 * rho
     assert abs(t_kin.mean() - T) < 0.01 * T
     assert abs(p_inst.mean() - P) < 0.03 * P
+
+
+def test_npt_autotune_restores_box_and_states(tmp_path, monkeypatch):
+    """Simulation.autotune under NPT_Atomic: the timed trials change the box
+    and the barostat; afterwards both are back, so the run that follows equals
+    a run started with the chosen plan bit for bit."""
+    monkeypatch.setenv("GAMDPY_B200_CACHE", str(tmp_path))
+
+    def make(plan_lanes=0, skin=0.5, nblist="linked lists"):
+        conf = workloads.lj_configuration([10, 10, 10], 0.9, 1.5, seed=9)
+        pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon), params=[1.0, 1.0, 2.5],
+                              max_num_nbs=300)
+        integ = gp.integrators.NPT_Atomic(temperature=1.5, tau=0.4, pressure=2.0, tau_p=2.0, dt=0.004)
+        plan = {"pb": 8, "tp": 1, "lanes": plan_lanes, "skin": skin, "nblist": nblist}
+        return gp.Simulation(conf, pp, integ, [gp.ScalarSaver(8)], num_timeblocks=2, steps_per_timeblock=32,
+                             compute_plan=plan, storage="memory"), conf, integ
+
+    a, ca, ia = make()
+    box0 = ca.simbox.lengths.copy()
+    chosen = a.autotune(tps_candidates=(1, 4), nblists=["linked lists"], steps=20)
+    assert np.array_equal(ca.simbox.lengths, box0)
+    for _ in a.run_timeblocks():
+        pass
+    b, cb, ib = make(chosen["lanes"], chosen["skin"], chosen["nblist"])
+    for _ in b.run_timeblocks():
+        pass
+    assert np.array_equal(ca["r"], cb["r"]) and np.array_equal(ca.simbox.lengths, cb.simbox.lengths)
+    assert np.array_equal(ia.barostat_state, ib.barostat_state)
+
+
+def test_batches_refuse_npt():
+    conf = workloads.lj_configuration([6, 6, 6], 0.9, 1.5, seed=1)
+    sim, _ = npt_sim(conf, 1.5, 0.4, 2.0, 2.0, 0.004, "N squared", 0.5, 1, 16, 4)
+    with pytest.raises(Exception, match="NPT"):
+        gp.SimulationBatch([sim])
+
+
+def test_saved_boxes_of_a_fixed_box():
+    """ConfigurationSaver(include_simbox=True) under NVE: every frame's box
+    row is the box."""
+    conf = workloads.lj_configuration([6, 6, 6], 0.9, 1.0, seed=2)
+    pp = gp.PairPotential(gp.apply_shifted_force_cutoff(gp.LJ_12_6_sigma_epsilon), params=[1.0, 1.0, 2.5],
+                          max_num_nbs=300)
+    sim = gp.Simulation(conf, pp, gp.integrators.NVE(dt=0.004), [gp.ConfigurationSaver(include_simbox=True)],
+                        num_timeblocks=2, steps_per_timeblock=16, storage="memory")
+    for _ in sim.run_timeblocks():
+        pass
+    boxes = sim.output["sim_box"]
+    assert boxes.shape == (2, 6, 3)
+    assert np.array_equal(boxes, np.broadcast_to(conf.simbox.lengths, boxes.shape))
