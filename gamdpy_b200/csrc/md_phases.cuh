@@ -508,6 +508,8 @@ constexpr int NBW = 4;         // particles of a cell handled per pass
 constexpr int NB_SEG_MAX = 64; // 25 rows x at most 2 ranges
 
 __device__ __forceinline__ int wrapi(int x, int n) { return ((x % n) + n) % n; }
+// x within two cells of [0, n), n >= 5: one compare each way, no division
+__device__ __forceinline__ int wrap_near(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 
 // s_lo, s_pre, s_sh: per-warp segment tables in shared memory (block warp w
 // uses entries [w * NB_SEG_MAX, ...), s_pre one more).
@@ -671,28 +673,40 @@ __device__ inline void phase_nbl_cells_tpp(const SimArgs &a, Span g) {
     const int maxn = a.max_nbs;
     const size_t cs = (size_t)a.stride * NB_CHUNK;
     const int ry = ncy < 5 ? ncy : 5, rz = ncz < 5 ? ncz : 5;
-    for (int s = g.b * (int)blockDim.x + (int)threadIdx.x; s < a.n; s += g.nb * (int)blockDim.x) {
+    // the arguments the walk reads, in registers: the list stores could
+    // otherwise force them to be reloaded after every store
+    const int n = a.n;
+    const int *excl = a.excl;
+    const int *orig_tmp = a.orig_tmp;
+    const int *cstart = a.cell_start;
+    const int *scell = a.scell;
+    int *nbl = a.nbl;
+    for (int s = g.b * (int)blockDim.x + (int)threadIdx.x; s < n; s += g.nb * (int)blockDim.x) {
         const float4 pi = pos[s];
-        const int c = a.scell[s];
-        const int cx = c % ncx, cy = (c / ncx) % ncy, cz = c / (ncx * ncy);
-        int *out = a.nbl + (size_t)s * NB_CHUNK;
+        const int c = scell[s];
+        const int cxy = ncx * ncy;
+        const int cz = c / cxy, rem = c - cz * cxy;
+        const int cy = rem / ncx, cx = rem - cy * ncx;
+        // entry k of slot s at chunk k/4 (cs apart), position k%4
+        int *chunk = nbl + (size_t)s * NB_CHUNK;
         int cnt = 0;
-        const int ui = a.excl ? a.orig_tmp[s] : 0;
+        const int ui = excl ? orig_tmp[s] : 0;
         auto test = [&](float4 pj, int j, float sx, float sy, float sz) {
             const float d2 =
                 SHIFTED ? dist_sq_shifted<FMA>(pj, pi, sx, sy, sz) : dist_sq_exact<FMA>(pj, pi, Lx, Ly, Lz);
-            if (d2 < cps2 && j != s && !(a.excl && excluded(a, ui, a.orig_tmp[j]))) {
-                if (cnt < maxn) out[(size_t)(cnt >> 2) * cs + (cnt & 3)] = j;
+            if (d2 < cps2 && j != s && !(excl && excluded(a, ui, orig_tmp[j]))) {
+                if (cnt < maxn) chunk[cnt & 3] = j;
                 cnt++;
+                if ((cnt & 3) == 0) chunk += cs;
             }
         };
         for (int za = 0; za < rz; za++) {
             const int zu = cz - 2 + za;
-            const int z = ncz < 5 ? za : wrapi(zu, ncz);
+            const int z = ncz < 5 ? za : wrap_near(zu, ncz);
             const float sz = SHIFTED ? (zu < 0 ? -Lz : (zu >= ncz ? Lz : 0.f)) : 0.f;
             for (int yb = 0; yb < ry; yb++) {
                 const int yu = cy - 2 + yb;
-                const int y = ncy < 5 ? yb : wrapi(yu, ncy);
+                const int y = ncy < 5 ? yb : wrap_near(yu, ncy);
                 const float sy = SHIFTED ? (yu < 0 ? -Ly : (yu >= ncy ? Ly : 0.f)) : 0.f;
                 const int rowbase = (z * ncy + y) * ncx;
                 int l0, h0, l1 = 0, h1 = 0;
@@ -724,7 +738,7 @@ __device__ inline void phase_nbl_cells_tpp(const SimArgs &a, Span g) {
                     const int lc = r ? l1 : l0, hc = r ? h1 : h0;
                     if (hc <= lc) continue;
                     const float sx = r ? sx1 : sx0;
-                    const int lo = a.cell_start[lc], hi = a.cell_start[hc];
+                    const int lo = cstart[lc], hi = cstart[hc];
                     int j = lo;
                     for (; j + 4 <= hi; j += 4) {  // four independent loads in flight
                         const float4 q0 = pos[j], q1 = pos[j + 1], q2 = pos[j + 2], q3 = pos[j + 3];
