@@ -72,6 +72,7 @@ struct DevCtrl {
     unsigned bar_count;   // grid barrier of the persistent kernel: top-level arrivals
     unsigned bar_gen;
     unsigned bar_group[64];  // arrivals per group of 16 blocks (grids up to 1024 blocks)
+    unsigned bar_all[3];  // step barrier where every block keeps the books: arrivals, by barrier index mod 3
     int abort;            // set when a barrier wait timed out
     unsigned work[2];     // persistent step: next round to hand out, by step parity
     long long bar_timeout;  // grid-barrier wait limit in SM clock cycles (0: the default, ~1 s)

@@ -135,6 +135,10 @@ struct gdb_sim {
     int brick_hcap = BRICK_HCAP;    // GDB_BRICK_HCAP lowers the stage the kernels may fill (tests of the fallback)
     int last_path = -1;      // 0 graph, 1 persistent grid, 2 cluster
     int grid_cap = 0;        // upper bound on the persistent grid (0: the whole GPU)
+    // persistent grid of at most BAR_FLAT_MAX blocks: every block does the
+    // step's bookkeeping after the step barrier (GDB_STEP_BARRIER=0: the last
+    // block to arrive does it and releases the others)
+    bool step_bar_all = true;
     ClusterJob *d_job = nullptr, *h_job = nullptr;
     bool uploaded = false;
     // graphs: [parity] for chunks of GRAPH_STEPS steps
@@ -240,6 +244,7 @@ __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
     ctrl->time_zero = time_zero;
     ctrl->bar_count = 0;
     for (int g = 0; g < 64; g++) ctrl->bar_group[g] = 0;
+    ctrl->bar_all[0] = ctrl->bar_all[1] = ctrl->bar_all[2] = 0;
     ctrl->abort = 0;
     ctrl->ticket = 0;
     ctrl->work[0] = ctrl->work[1] = 0;
@@ -254,6 +259,7 @@ __global__ void k_block_begin(DevCtrl *ctrl, double time_zero) {
 __global__ void k_block_resume(DevCtrl *ctrl) {
     ctrl->bar_count = 0;
     for (int g = 0; g < 64; g++) ctrl->bar_group[g] = 0;
+    ctrl->bar_all[0] = ctrl->bar_all[1] = ctrl->bar_all[2] = 0;
     ctrl->abort = 0;
     ctrl->ticket = 0;
     ctrl->work[0] = ctrl->work[1] = 0;
@@ -490,6 +496,7 @@ static int ensure_partials(gdb_sim *h, int nblocks) {
 static SimArgs make_args(gdb_sim *h) {
     SimArgs a;
     a.nsq_smem = 0;
+    a.bar_all = h->step_bar_all ? 1 : 0;
     a.pos0 = h->pos[0];
     a.pos1 = h->pos[1];
     a.vel = h->vel;
@@ -690,7 +697,9 @@ static int launch_run(gdb_sim *h, int steps, int do_eval) {
     int grid = 0;
     int rc = run_grid(h, fn, &grid, dsmem);
     if (rc) return rc;
-    if ((rc = ensure_partials(h, grid))) return rc;
+    // a row per round, two steps' rows where every block keeps the books
+    if ((rc = ensure_partials(h, std::max(grid, 2 * grid_for((long long)h->n * h->tp))))) return rc;
+    a.partials = h->partials;
     int cur0 = h->cur, ns = steps, ev = do_eval;
     void *args[] = {(void *)&a, (void *)&h->table, (void *)&cur0, (void *)&ns, (void *)&ev};
     CK(cudaLaunchCooperativeKernel(fn, dim3(grid), dim3(GDB_BLOCK), args, dsmem, h->st));
@@ -884,6 +893,8 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (bk && (bk[0] == '1' || bk[0] == '2')) h->bricks_req = true;
     const char *bm = getenv("GDB_BRICK_MIN_N");
     if (bm) h->brick_min_n = atoi(bm);
+    const char *sb = getenv("GDB_STEP_BARRIER");
+    if (sb && sb[0] == '0') h->step_bar_all = false;
     const char *bh = getenv("GDB_BRICK_HCAP");
     if (bh) h->brick_hcap = std::max(1, std::min(atoi(bh), BRICK_HCAP));
     cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, device);

@@ -49,6 +49,7 @@ __global__ void __launch_bounds__(GDB_BLOCK, GDB_STEP_MINBLOCKS(TP)) k_step(SimA
 // With `flag`, a block reports that one of its particles moved more than
 // skin/2; the block that runs `last` finds in *any whether any block did.
 struct GridSync {  // bounded software barrier over a cooperative grid
+    static constexpr bool kGrid = true;
     template <typename F>
     __device__ __forceinline__ bool operator()(DevCtrl *c, F last, bool flag = false, int *any = nullptr) const {
         return grid_barrier(c, last, flag, any);
@@ -62,6 +63,7 @@ __device__ __forceinline__ void cluster_barrier() {
     asm volatile("barrier.cluster.arrive.release;\n\tbarrier.cluster.wait.acquire;" ::: "memory");
 }
 struct ClusterSync {
+    static constexpr bool kGrid = false;
     int rank;
     template <typename F>
     __device__ __forceinline__ bool operator()(DevCtrl *c, F last, bool flag = false, int *any = nullptr) const {
@@ -155,13 +157,20 @@ __device__ inline void run_steps(const SimArgs &a0, const PairEntry *s_tab, int 
     const int rounds = (a.n + (int)blockDim.x / TP - 1) / ((int)blockDim.x / TP);  // partial rows per step
     trace_mark(ctrl, TR_START);
     __shared__ StepCtl s_ctl;
-    __shared__ int s_any;  // a particle moved beyond skin/2 (the block running `last`)
+    __shared__ int s_any;  // a particle moved beyond skin/2 (the block running `last`, or every block)
+    // a grid of at most BAR_FLAT_MAX blocks: every block keeps the books of a
+    // step (step_barrier_all, finalize_step_all), on rows double-buffered by
+    // step parity, as a block may write the next step's rows while another
+    // still sums this step's
+    const bool all = Sync::kGrid && INTEG != GDB_INTEGRATOR_NPT && a.bar_all && (int)gridDim.x <= BAR_FLAT_MAX;
+    unsigned seq = 0;  // step barriers of this launch
     for (int s = 0; s < nsteps + do_eval; s++) {
         if (INTEG == GDB_INTEGRATOR_NPT) npt_refresh_box(a_npt);
         // the rebuild flag, the step index and the state the step reads
         // (momentum shift, thermostat), loaded together by one thread: none
-        // of them changes across a rebuild
-        if (threadIdx.x == 0) load_step_ctl(ctrl, &s_ctl);
+        // of them changes across a rebuild.  Where every block keeps the
+        // books, its own copy is current after the first step.
+        if (threadIdx.x == 0 && (!all || s == 0)) load_step_ctl(ctrl, &s_ctl);
         __syncthreads();
         const int rebuild = s_ctl.rebuild;
         const int step = s_ctl.step;
@@ -173,16 +182,22 @@ __device__ inline void run_steps(const SimArgs &a0, const PairEntry *s_tab, int 
         }
         bool ok;
         if (s < nsteps) {
+            double *part = all ? a.partials + (size_t)(step & 1) * rounds * NQ : nullptr;
             const bool moved = phase_step<TP, NT, INTEG, MODE_STEP, false, true>(a, s_tab, nt, cur, step, s_red, g,
-                                                                                   &s_ctl);
+                                                                                   &s_ctl, part);
             trace_mark(ctrl, TR_STEP_PHASE);
-            ok = sync(
-                ctrl,
-                [&] {
-                    finalize_step<MODE_STEP, INTEG>(a, step, rounds, s_red);
-                    if (threadIdx.x == 0 && s_any) ctrl->rebuild = 1;
-                },
-                moved, &s_any);
+            if (all) {
+                ok = step_barrier_all(ctrl, seq++, moved, &s_any);
+                if (ok) finalize_step_all<INTEG>(a, step, rounds, part, s_red, &s_ctl, s_any);
+            } else {
+                ok = sync(
+                    ctrl,
+                    [&] {
+                        finalize_step<MODE_STEP, INTEG>(a, step, rounds, s_red);
+                        if (threadIdx.x == 0 && s_any) ctrl->rebuild = 1;
+                    },
+                    moved, &s_any);
+            }
             cur ^= 1;
             trace_mark(ctrl, TR_STEP);
         } else {

@@ -55,6 +55,7 @@ struct SimArgs {
     int brick_hcap;     // staged positions a brick's halo may hold (<= BRICK_HCAP)
     int nb_kind, fma;
     int nsq_smem;  // persistent N^2 build stages all positions in dynamic shared memory
+    int bar_all;   // persistent grid: every block keeps the step's books (grids of <= BAR_FLAT_MAX blocks)
     float Lx, Ly, Lz;
     float cps2;    // (max_cut + skin)^2, nblist.py:152
     float skin2q;  // skin*skin*0.25, orthorhombic.py:131
@@ -213,6 +214,55 @@ __device__ __forceinline__ bool grid_barrier(DevCtrl *c, F last, bool flag = fal
         __syncthreads();
     }
     return s_ok != 0;
+}
+
+// Step barrier of a persistent grid of at most BAR_FLAT_MAX blocks in which
+// every block does the step's bookkeeping itself (finalize_step_all): no
+// block runs a phase between arrival and departure, so there is no release
+// to wait for.  Barrier `seq` (counted from 0 in each launch) counts arrivals
+// on bar_all[seq % 3], with the moved flag in the high bits as above; every
+// block leaves when the count reaches the grid and reads the same final word.
+// Block 0 clears bar_all[(seq + 2) % 3] on its way out: every block has
+// arrived here, so none still polls barrier seq - 1, and block 0's arrival at
+// barrier seq + 1 orders the clear before any arrival at barrier seq + 2.
+// The launch starts with all three words zero.  Same abort and wait limit as
+// grid_barrier.
+__device__ __forceinline__ bool step_barrier_all(DevCtrl *c, unsigned seq, bool flag, int *any) {
+    __shared__ int s_ok2;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1, raised = 0;
+        if (*(volatile int *)&c->abort) {
+            ok = 0;
+        } else {
+            unsigned *cnt = &c->bar_all[seq % 3u];
+            const unsigned inc = 1u | (flag ? BAR_FLAG_ONE : 0u);
+            unsigned v = atom_add_acq_rel_gpu(cnt, inc) + inc;
+            const long long t0 = clock64();
+            const long long limit = c->bar_timeout > 0 ? c->bar_timeout : BARRIER_TIMEOUT_CYCLES;
+            int polls = 0;
+            while ((v & BAR_COUNT_MASK) != gridDim.x) {
+                if (*(volatile int *)&c->abort) {
+                    ok = 0;
+                    break;
+                }
+                if ((++polls & 63) == 0 && clock64() - t0 > limit) {
+                    atomicOr(&c->status, GDB_STATUS_BARRIER_TIMEOUT);
+                    c->abort = 1;
+                    ok = 0;
+                    break;
+                }
+                if (polls > 64) __nanosleep(32);
+                v = ld_acquire_gpu(cnt);
+            }
+            raised = (v >> 20) != 0u;
+            if (ok && blockIdx.x == 0) c->bar_all[(seq + 2u) % 3u] = 0u;
+        }
+        *any = raised;
+        s_ok2 = ok;
+    }
+    __syncthreads();
+    return s_ok2 != 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -1182,6 +1232,7 @@ struct StepCtl {
     int rebuild, step, pending[2];
     float shift[2][3];
     float xi;
+    double time_zero;
 };
 __device__ __forceinline__ void load_step_ctl(const DevCtrl *c, StepCtl *sc) {
     const int rb = *(volatile const int *)&c->rebuild;
@@ -1193,6 +1244,7 @@ __device__ __forceinline__ void load_step_ctl(const DevCtrl *c, StepCtl *sc) {
 #pragma unroll
         for (int k = 0; k < 3; k++) sh[q][k] = *(volatile const float *)&c->shift[q][k];
     const float xi = *(volatile const float *)&c->xi;
+    const double tz = *(volatile const double *)&c->time_zero;
     sc->rebuild = rb;
     sc->step = st;
     sc->pending[0] = p0;
@@ -1202,6 +1254,7 @@ __device__ __forceinline__ void load_step_ctl(const DevCtrl *c, StepCtl *sc) {
 #pragma unroll
         for (int k = 0; k < 3; k++) sc->shift[q][k] = sh[q][k];
     sc->xi = xi;
+    sc->time_zero = tz;
 }
 
 // Forces from pos[cur], integration into pos[cur^1] (MODE_STEP) or forces
@@ -1214,11 +1267,13 @@ __device__ __forceinline__ void load_step_ctl(const DevCtrl *c, StepCtl *sc) {
 // the sums the step needs are reduced: all of them on saved and reset steps,
 // the kinetic energy (NVT) otherwise.  Returns (persistent kernels) or sets
 // (standalone) the rebuild flag when a particle has moved more than skin/2
-// since the build.
+// since the build.  `part` (persistent kernels) replaces partials as the
+// rows' base.
 template <int TP, int NT, int INTEG, int MODE, bool NC, bool PERSIST>
 __device__ inline bool phase_step(const SimArgs &a, const PairEntry *tab, int nt, int cur, int step, double *s_red,
-                                  Span g = grid_span(), const StepCtl *sc = nullptr) {
+                                  Span g = grid_span(), const StepCtl *sc = nullptr, double *part = nullptr) {
     DevCtrl *ctrl = a.ctrl;
+    double *prow = part ? part : a.partials;  // the rows this step writes
     const float4 *pos = cur_pos(a, cur);
     float4 *pos_next = cur_pos(a, cur ^ 1);
     // NPT_Atomic reads every particle's virial every step (NPT_Atomic.py:115)
@@ -1296,12 +1351,12 @@ __device__ inline bool phase_step(const SimArgs &a, const PairEntry *tab, int nt
                 block_sum<NQ>(red, s_red);
                 if (threadIdx.x == 0) {
 #pragma unroll
-                    for (int q = 0; q < NQ; q++) a.partials[(size_t)round * NQ + q] = red[q];
+                    for (int q = 0; q < NQ; q++) prow[(size_t)round * NQ + q] = red[q];
                 }
             } else if (needk) {
                 double rk[1] = {red[0]};
                 block_sum<1>(rk, s_red);
-                if (threadIdx.x == 0) a.partials[(size_t)round * NQ] = rk[0];
+                if (threadIdx.x == 0) prow[(size_t)round * NQ] = rk[0];
             }
 #pragma unroll
             for (int q = 0; q < NQ; q++) red[q] = 0.0;
@@ -1336,6 +1391,69 @@ __device__ inline bool phase_step(const SimArgs &a, const PairEntry *tab, int nt
     return block_moved;
 }
 
+// Fixed-order float64 sums of `nrows` partial rows (blocks or rounds): every
+// column (full) or the kinetic energy alone (needk); the result is valid in
+// thread 0.  Each thread sums rows threadIdx.x, + blockDim.x, ... in that
+// order; the rows of a batch are loaded before they are added, so several
+// loads are in flight (the same sums as one row at a time, bit for bit).
+__device__ inline void sum_partial_rows(const double *part, int nrows, bool full, bool needk, double *s_red,
+                                        double (&tot)[NQ]) {
+#pragma unroll
+    for (int q = 0; q < NQ; q++) tot[q] = 0.0;
+    const int bs = blockDim.x;
+    if (full) {
+        int b = threadIdx.x;
+        for (; b + 3 * bs < nrows; b += 4 * bs) {
+            double v[4][NQ];
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int q = 0; q < NQ; q++) v[u][q] = __ldcg(part + (size_t)(b + u * bs) * NQ + q);
+#pragma unroll
+            for (int u = 0; u < 4; u++)
+#pragma unroll
+                for (int q = 0; q < NQ; q++) tot[q] += v[u][q];
+        }
+        for (; b < nrows; b += bs) {
+#pragma unroll
+            for (int q = 0; q < NQ; q++) tot[q] += __ldcg(part + (size_t)b * NQ + q);
+        }
+        block_sum<NQ>(tot, s_red);
+    } else if (needk) {
+        double t1[1] = {0.0};
+        int b = threadIdx.x;
+        for (; b + 7 * bs < nrows; b += 8 * bs) {
+            double v[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++) v[u] = __ldcg(part + (size_t)(b + u * bs) * NQ);
+#pragma unroll
+            for (int u = 0; u < 8; u++) t1[0] += v[u];
+        }
+        for (; b < nrows; b += bs) t1[0] += __ldcg(part + (size_t)b * NQ);
+        block_sum<1>(t1, s_red);
+        tot[0] = t1[0];
+    }
+}
+
+// Nose-Hoover friction after a step with kinetic-energy sum `sumk`
+// (NVT.py:113-124).
+__device__ __forceinline__ float nose_hoover_next(const SimArgs &a, float xi, double sumk, double time) {
+    const double T = target_temperature(a, time);
+    const double dev = 2.0 * sumk / ((double)a.dof * T) - 1.0;
+    return (float)((double)xi + (double)(a.dt * a.omega2) * dev);
+}
+
+// The ScalarSaver row of a recorded step (scalar_saver.py:165-179).
+__device__ __forceinline__ void write_scalar_row(const SimArgs &a, int step, const double tot[NQ]) {
+    if (step / a.every >= a.nrows) return;
+    double *row = a.rows + (size_t)(step / a.every) * GDB_NUM_SCALARS;
+    row[GDB_SCALAR_U] = tot[1];
+    row[GDB_SCALAR_W] = tot[2];
+    row[GDB_SCALAR_LAPU] = tot[3];
+    row[GDB_SCALAR_K] = tot[0];
+    row[GDB_SCALAR_FSQ] = tot[4];
+}
+
 // Fixed-order float64 sum of `nblocks` partial rows (blocks or rounds) and the
 // bookkeeping of a finished step (NVT.py:113-124, scalar_saver.py:165-179,
 // momentum_reset.py:64-78).  Run by one whole block.
@@ -1349,44 +1467,7 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
     const bool full = rec || reset || npt;
     const bool needk = full || a.omega2 > 0.f;
     double tot[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) tot[q] = 0.0;
-    // Each thread sums rows threadIdx.x, + blockDim.x, ... in that order; the
-    // rows of a batch are loaded before they are added, so several loads are
-    // in flight (the same sums as one row at a time, bit for bit).
-    const int bs = blockDim.x;
-    if (full) {
-        int b = threadIdx.x;
-        for (; b + 3 * bs < nblocks; b += 4 * bs) {
-            double v[4][NQ];
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-                for (int q = 0; q < NQ; q++) v[u][q] = __ldcg(a.partials + (size_t)(b + u * bs) * NQ + q);
-#pragma unroll
-            for (int u = 0; u < 4; u++)
-#pragma unroll
-                for (int q = 0; q < NQ; q++) tot[q] += v[u][q];
-        }
-        for (; b < nblocks; b += bs) {
-#pragma unroll
-            for (int q = 0; q < NQ; q++) tot[q] += __ldcg(a.partials + (size_t)b * NQ + q);
-        }
-        block_sum<NQ>(tot, s_red);
-    } else if (needk) {
-        double t1[1] = {0.0};
-        int b = threadIdx.x;
-        for (; b + 7 * bs < nblocks; b += 8 * bs) {
-            double v[8];
-#pragma unroll
-            for (int u = 0; u < 8; u++) v[u] = __ldcg(a.partials + (size_t)(b + u * bs) * NQ);
-#pragma unroll
-            for (int u = 0; u < 8; u++) t1[0] += v[u];
-        }
-        for (; b < nblocks; b += bs) t1[0] += __ldcg(a.partials + (size_t)b * NQ);
-        block_sum<1>(t1, s_red);
-        tot[0] = t1[0];
-    }
+    sum_partial_rows(a.partials, nblocks, full, needk, s_red, tot);
     if (threadIdx.x == 0) {
         if (MODE == MODE_STEP) {
             const double time = ctrl->time_zero + (double)step * (double)a.dt;
@@ -1419,23 +1500,16 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
                 ctrl->npt_ts0 = ts0;
                 ctrl->npt_bs0 = (float)((double)bs0 + (double)a.dt * (p_dev / mass_p + (double)(ts0 * bs0)));
             } else if (a.omega2 > 0.f) {
-                const double T = target_temperature(a, time);
-                const double dev = 2.0 * tot[0] / ((double)a.dof * T) - 1.0;
-                ctrl->xi = (float)((double)ctrl->xi + (double)(a.dt * a.omega2) * dev);
+                ctrl->xi = nose_hoover_next(a, ctrl->xi, tot[0], time);
             }
             ctrl->sumK = (float)tot[0];
-            if (rec && step / a.every < a.nrows) {
-                double *row = a.rows + (size_t)(step / a.every) * GDB_NUM_SCALARS;
-                row[GDB_SCALAR_U] = tot[1];
-                row[GDB_SCALAR_W] = tot[2];
-                row[GDB_SCALAR_LAPU] = tot[3];
-                row[GDB_SCALAR_K] = tot[0];
-                row[GDB_SCALAR_FSQ] = tot[4];
-                if (npt) {  // the saver reads the box the step left (scalar_saver.py:195)
+            if (rec) {
+                write_scalar_row(a, step, tot);
+                if (npt && step / a.every < a.nrows) {  // the saver reads the box the step left (scalar_saver.py:195)
                     float vol = ctrl->box[0];
                     vol *= ctrl->box[1];
                     vol *= ctrl->box[2];
-                    row[GDB_SCALAR_VOL] = vol;
+                    a.rows[(size_t)(step / a.every) * GDB_NUM_SCALARS + GDB_SCALAR_VOL] = vol;
                 }
             }
             if (reset) {
@@ -1451,6 +1525,55 @@ __device__ inline void finalize_step(const SimArgs &a, int step, int nblocks, do
             ctrl->evalW = tot[2];
         }
         ctrl->pending[ppar] = 0;
+    }
+}
+
+// The bookkeeping of finalize_step for a step (not NPT_Atomic) by every block
+// of the persistent grid after step_barrier_all: each block sums the same
+// rows (part, this step's half of the double-buffered rows) in the same
+// order, so each computes the same next control state, into its StepCtl.
+// Block 0 also writes that state to ctrl (for the host and the next launch)
+// with the scalar row, and clears the round counter of step + 2: every block
+// took its last round of this step before it arrived at the barrier.
+template <int INTEG>
+__device__ inline void finalize_step_all(const SimArgs &a, int step, int nrows, const double *part, double *s_red,
+                                         StepCtl *sc, int any) {
+    DevCtrl *ctrl = a.ctrl;
+    const bool rec = a.every > 0 && step % a.every == 0;
+    const bool reset = a.reset_every > 0 && step % a.reset_every == 0;
+    const int par = step & 1, ppar = par ^ 1;
+    const bool full = rec || reset;
+    const bool needk = full || a.omega2 > 0.f;
+    double tot[NQ];
+    sum_partial_rows(part, nrows, full, needk, s_red, tot);
+    if (threadIdx.x == 0) {
+        const bool writer = blockIdx.x == 0;
+        if (a.omega2 > 0.f) {
+            sc->xi = nose_hoover_next(a, sc->xi, tot[0], sc->time_zero + (double)step * (double)a.dt);
+            if (writer) ctrl->xi = sc->xi;
+        }
+        if (reset) {
+            sc->shift[par][0] = (float)(tot[5] / tot[8]);
+            sc->shift[par][1] = (float)(tot[6] / tot[8]);
+            sc->shift[par][2] = (float)(tot[7] / tot[8]);
+            sc->pending[par] = 1;
+        }
+        sc->pending[ppar] = 0;
+        sc->step = step + 1;
+        sc->rebuild = any;
+        if (writer) {
+            ctrl->sumK = (float)tot[0];
+            if (rec) write_scalar_row(a, step, tot);
+            if (reset) {
+#pragma unroll
+                for (int k = 0; k < 3; k++) ctrl->shift[par][k] = sc->shift[par][k];
+                ctrl->pending[par] = 1;
+            }
+            ctrl->pending[ppar] = 0;
+            ctrl->step = step + 1;
+            if (any) ctrl->rebuild = 1;
+            ctrl->work[step & 1] = 0;
+        }
     }
 }
 
