@@ -134,7 +134,7 @@ struct gdb_sim {
     int brick_min_n = BRICK_MIN_N;  // GDB_BRICK_MIN_N
     int brick_hcap = BRICK_HCAP;    // GDB_BRICK_HCAP lowers the stage the kernels may fill (tests of the fallback)
     int last_path = -1;      // 0 graph, 1 persistent grid, 2 cluster
-    int grid_cap = 0;        // upper bound on the persistent grid (0: the whole GPU)
+    int grid_cap = 0;        // upper bound on the persistent grid (0: the whole GPU; GDB_GRID_CAP)
     // persistent grid of at most BAR_FLAT_MAX blocks: every block does the
     // step's bookkeeping after the step barrier (GDB_STEP_BARRIER=0: the last
     // block to arrive does it and releases the others)
@@ -893,6 +893,8 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (bk && (bk[0] == '1' || bk[0] == '2')) h->bricks_req = true;
     const char *bm = getenv("GDB_BRICK_MIN_N");
     if (bm) h->brick_min_n = atoi(bm);
+    const char *gc = getenv("GDB_GRID_CAP");
+    if (gc) h->grid_cap = std::max(0, atoi(gc));
     const char *sb = getenv("GDB_STEP_BARRIER");
     if (sb && sb[0] == '0') h->step_bar_all = false;
     const char *bh = getenv("GDB_BRICK_HCAP");

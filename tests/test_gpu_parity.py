@@ -469,6 +469,35 @@ def test_runs_are_bitwise_reproducible():
     assert conf.N == 4000
 
 
+@pytest.mark.parametrize("n, lanes, cap", [(2048, 0, 0), (65536, 1, 100), (20000, 4, 0)])
+def test_step_barrier_forms_agree_bit_for_bit(monkeypatch, n, lanes, cap):
+    """The persistent grid's step barrier in its two forms -- every block
+    keeping the step's books from rows double-buffered by step parity (the
+    default for grids of up to 320 blocks) and the last block to arrive
+    keeping them (GDB_STEP_BARRIER=0) -- give the same trajectory, scalars
+    and thermostat state bit for bit: the same rows summed in the same order.
+    NVT with a ScalarSaver and MomentumReset, so the full rows, the momentum
+    shift and the friction all pass through the books; with a grid of 100
+    blocks for 256 rounds, the rounds are handed out by the counter."""
+    monkeypatch.setenv("GDB_CLUSTER", "0")
+    monkeypatch.setenv("GDB_GRID_CAP", str(cap))
+    outs = []
+    for mode in ("1", "0"):
+        monkeypatch.setenv("GDB_STEP_BARRIER", mode)
+        c = workloads.ka_configuration(n, seed=7)
+        integ = gp.integrators.NVT(0.45, 0.2, 0.005)
+        sim = gp.Simulation(c, workloads.ka_pair_potential(max_num_nbs=300), integ,
+                            [gp.ScalarSaver(10), gp.MomentumReset(30)], num_timeblocks=2, steps_per_timeblock=150,
+                            compute_plan={"pb": 64, "tp": 1, "lanes": lanes, "skin": 0.3, "nblist": "linked lists"},
+                            storage="memory")
+        for _ in sim.run_timeblocks():
+            pass
+        assert sim._sim.last_path() == 1
+        outs.append((c["r"].copy(), c["v"].copy(), np.array(sim.output["scalars"]), integ.thermostat_state.copy()))
+    for a, b in zip(*outs):
+        assert np.array_equal(a, b)
+
+
 def test_nve_energy_conservation():
     """tests/test_LJ_nxyz.py:10-111 of the reference: LJ rho 0.8442, T0 1.44,
     shifted force, dt 0.005, 2 x 4096 steps: var(E)/N < 1e-4 and
