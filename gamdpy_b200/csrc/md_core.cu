@@ -122,6 +122,7 @@ struct gdb_sim {
     bool cluster_ok = true;  // small systems run resident in one thread-block cluster
     bool cluster_force = false;  // GDB_CLUSTER=1: the cluster path whenever it fits
     int nsq_auto_max = NSQ_AUTO_MAX;  // persistent kernel: N^2 build up to this N (GDB_NSQ_AUTO)
+    bool nsq_stage = true;            // persistent N^2 build from staged positions (GDB_NSQ_STAGE=0: from L2)
     // the staged-halo path of large cell-list systems on the persistent
     // kernel (md_bricks.cuh): cells numbered in bricks of 4 x 4 x 4 cells,
     // each brick's halo staged in shared memory.  Off by default (measured
@@ -690,7 +691,8 @@ static int launch_run(gdb_sim *h, int steps, int do_eval) {
         a.nbx = a.nby = a.nbz = 0;
     }
     // small N^2 systems: every block stages the positions for the list build
-    const size_t dsmem = (a.nb_kind == GDB_NBLIST_NSQ && h->n <= NSQ_SMEM_MAX) ? (size_t)h->n * sizeof(float4) : 0;
+    const size_t dsmem =
+        (a.nb_kind == GDB_NBLIST_NSQ && h->n <= NSQ_SMEM_MAX && h->nsq_stage) ? (size_t)h->n * sizeof(float4) : 0;
     a.nsq_smem = dsmem > 0;
     // static plus dynamic shared memory above 48 KiB needs the opt-in
     if (dsmem > 0) CK(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
@@ -893,6 +895,8 @@ int gdb_sim_create(int n, int ntypes, int device, gdb_sim **out) {
     if (bk && (bk[0] == '1' || bk[0] == '2')) h->bricks_req = true;
     const char *bm = getenv("GDB_BRICK_MIN_N");
     if (bm) h->brick_min_n = atoi(bm);
+    const char *st = getenv("GDB_NSQ_STAGE");
+    if (st && st[0] == '0') h->nsq_stage = false;
     const char *gc = getenv("GDB_GRID_CAP");
     if (gc) h->grid_cap = std::max(0, atoi(gc));
     const char *sb = getenv("GDB_STEP_BARRIER");

@@ -269,13 +269,70 @@ __device__ __forceinline__ bool step_barrier_all(DevCtrl *c, unsigned seq, bool 
 // neighbour-list phases
 // ---------------------------------------------------------------------------
 
+// One pass of the N^2 candidate walk of a warp: lanes test candidates
+// j0 + 32u + lane (u < 4, loaded before they are tested) against particle i0
+// and, with TWO, i1; hits are appended in ascending j by ballot + popc.  CHECK
+// (the last, partial pass only) masks candidates j >= n.  The tests are
+// combined without short-circuit branches: the distance is cheap and pure.
+struct NsqWalk {
+    const float4 *pos, *src;
+    int n, max_nbs;
+    size_t cstride;  // stride * NB_CHUNK: entries k and k + 4 of a particle
+    float Lx, Ly, Lz, cps2;
+    const int *excl, *orig;
+    int *nbl;
+    int lane;
+    unsigned below;
+};
+template <bool FMA, bool NC, bool TWO, bool CHECK>
+__device__ __forceinline__ void nsq_pass(const SimArgs &a, const NsqWalk &w, int j0, int i0, int i1, float4 p0,
+                                         float4 p1, int u0, int u1, int &c0, int &c1) {
+    float4 q[4];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int j = j0 + 32 * u + w.lane;
+        // one load kind per instantiation: the read-only path for the
+        // standalone kernel (never staged), plain loads from the staged copy
+        // or the coherent buffer otherwise
+        q[u] = (!CHECK || j < w.n) ? (NC ? load<true>(w.pos + j) : w.src[j]) : p0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+        const int j = j0 + 32 * u + w.lane;
+        const bool in = !CHECK || j < w.n;
+        bool h0 = in & (j != i0) & (dist_sq_exact<FMA>(q[u], p0, w.Lx, w.Ly, w.Lz) < w.cps2);
+        bool h1 = false;
+        if (TWO) h1 = in & (j != i1) & (dist_sq_exact<FMA>(q[u], p1, w.Lx, w.Ly, w.Lz) < w.cps2);
+        if (w.excl) {
+            if (h0) h0 = !excluded(a, u0, w.orig[j]);
+            if (TWO && h1) h1 = !excluded(a, u1, w.orig[j]);
+        }
+        const unsigned m0 = __ballot_sync(0xffffffffu, h0);
+        if (h0) {
+            const int k = c0 + __popc(m0 & w.below);
+            if (k < w.max_nbs) w.nbl[(size_t)(k >> 2) * w.cstride + (size_t)i0 * NB_CHUNK + (k & 3)] = j;
+        }
+        c0 += __popc(m0);
+        if (TWO) {
+            const unsigned m1 = __ballot_sync(0xffffffffu, h1);
+            if (h1) {
+                const int k = c1 + __popc(m1 & w.below);
+                if (k < w.max_nbs) w.nbl[(size_t)(k >> 2) * w.cstride + (size_t)i1 * NB_CHUNK + (k & 3)] = j;
+            }
+            c1 += __popc(m1);
+        }
+    }
+}
+
 // N^2 build (interactions/nblist.py:88-143): a warp per particle, lanes
 // stride over j, ballot + popc append hits in ascending j (deterministic).
 // A warp takes its particles two at a time (i and i + the number of warps):
 // every candidate is loaded once for both, and the two append chains are
-// independent.  With `spos` (shared memory for all n positions) the block
-// first copies the positions there, so the candidate loads are shared-memory
-// loads; four candidates per lane are loaded before they are tested.
+// independent.  Whether a warp has a second particle is uniform over the
+// warp, so the walk is instantiated for one and for two particles, and the
+// full passes skip the j < n test of the last one.  With `spos` (shared
+// memory for all n positions) the block first copies the positions there,
+// so the candidate loads are shared-memory loads.
 template <bool FMA, bool NC>
 __device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_span(), float4 *spos = nullptr) {
     const float4 *pos = cur_pos(a, cur);
@@ -296,58 +353,43 @@ __device__ inline void phase_nbl_nsq(const SimArgs &a, int cur, Span g = grid_sp
         src = spos;
         trace_mark(a.ctrl, TR_REBUILD_PHASE);
     }
-    // the arguments the loop reads, in registers: the list stores below could
+    // the arguments the loop reads, in registers: the list stores could
     // otherwise force them to be reloaded after every store
-    const int n = a.n, max_nbs = a.max_nbs, stride = a.stride;
-    const float Lx = a.Lx, Ly = a.Ly, Lz = a.Lz, cps2 = a.cps2;
-    const int *excl = a.excl;
-    const int *orig = a.orig;
-    int *nbl = a.nbl;
-    const int lane = threadIdx.x & 31;
+    NsqWalk w;
+    w.pos = pos;
+    w.src = src;
+    w.n = a.n;
+    w.max_nbs = a.max_nbs;
+    w.cstride = (size_t)a.stride * NB_CHUNK;
+    w.Lx = a.Lx;
+    w.Ly = a.Ly;
+    w.Lz = a.Lz;
+    w.cps2 = a.cps2;
+    w.excl = a.excl;
+    w.orig = a.orig;
+    w.nbl = a.nbl;
+    w.lane = threadIdx.x & 31;
+    w.below = (1u << w.lane) - 1u;
+    const int n = w.n;
+    const int nfull = n & ~127;  // candidates covered by full passes
     const int warps = (g.nb * (int)blockDim.x) >> 5;
-    const unsigned below = (1u << lane) - 1u;
     for (int i0 = (g.b * (int)blockDim.x + (int)threadIdx.x) >> 5; i0 < n; i0 += 2 * warps) {
         const int i1 = i0 + warps;
-        const bool has1 = i1 < n;
+        const bool has1 = i1 < n;  // the same for every lane of the warp
         const float4 p0 = NC ? load<true>(pos + i0) : src[i0];
         const float4 p1 = has1 ? (NC ? load<true>(pos + i1) : src[i1]) : p0;
-        const int u0 = excl ? orig[i0] : 0, u1 = (excl && has1) ? orig[i1] : 0;
+        const int u0 = w.excl ? w.orig[i0] : 0, u1 = (w.excl && has1) ? w.orig[i1] : 0;
         int c0 = 0, c1 = 0;
-        for (int j0 = 0; j0 < n; j0 += 128) {
-            float4 q[4];
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int j = j0 + 32 * u + lane;
-                // one load kind per instantiation: the read-only path for the
-                // standalone kernel (never staged), plain loads from the
-                // staged copy or the coherent buffer otherwise
-                q[u] = j < n ? (NC ? load<true>(pos + j) : src[j]) : p0;
-            }
-#pragma unroll
-            for (int u = 0; u < 4; u++) {
-                const int j = j0 + 32 * u + lane;
-                const bool in = j < n;
-                bool h0 = in && j != i0 && dist_sq_exact<FMA>(q[u], p0, Lx, Ly, Lz) < cps2;
-                bool h1 = has1 && in && j != i1 && dist_sq_exact<FMA>(q[u], p1, Lx, Ly, Lz) < cps2;
-                if (excl) {
-                    if (h0) h0 = !excluded(a, u0, orig[j]);
-                    if (h1) h1 = !excluded(a, u1, orig[j]);
-                }
-                const unsigned m0 = __ballot_sync(0xffffffffu, h0);
-                const unsigned m1 = __ballot_sync(0xffffffffu, h1);
-                if (h0) {
-                    const int k = c0 + __popc(m0 & below);
-                    if (k < max_nbs) nbl[nbl_index(i0, k, stride)] = j;
-                }
-                if (h1) {
-                    const int k = c1 + __popc(m1 & below);
-                    if (k < max_nbs) nbl[nbl_index(i1, k, stride)] = j;
-                }
-                c0 += __popc(m0);
-                c1 += __popc(m1);
-            }
+        if (has1) {
+            int j0 = 0;
+            for (; j0 < nfull; j0 += 128) nsq_pass<FMA, NC, true, false>(a, w, j0, i0, i1, p0, p1, u0, u1, c0, c1);
+            if (j0 < n) nsq_pass<FMA, NC, true, true>(a, w, j0, i0, i1, p0, p1, u0, u1, c0, c1);
+        } else {
+            int j0 = 0;
+            for (; j0 < nfull; j0 += 128) nsq_pass<FMA, NC, false, false>(a, w, j0, i0, i1, p0, p1, u0, u1, c0, c1);
+            if (j0 < n) nsq_pass<FMA, NC, false, true>(a, w, j0, i0, i1, p0, p1, u0, u1, c0, c1);
         }
-        if (lane == 0) {
+        if (w.lane == 0) {
             a.nbc[i0] = c0;
             a.rref[i0] = p0;
             atomicMax(&a.ctrl->maxcount, c0);
