@@ -274,6 +274,11 @@ __device__ __forceinline__ bool step_barrier_all(DevCtrl *c, unsigned seq, bool 
 // and, with TWO, i1; hits are appended in ascending j by ballot + popc.  CHECK
 // (the last, partial pass only) masks candidates j >= n.  The tests are
 // combined without short-circuit branches: the distance is cheap and pure.
+template <bool B>
+struct BoolTag {
+    static constexpr bool value = B;
+};
+
 struct NsqWalk {
     const float4 *pos, *src;
     int n, max_nbs;
@@ -773,79 +778,89 @@ __device__ inline void phase_nbl_cells_tpp(const SimArgs &a, Span g) {
     const int *cstart = a.cell_start;
     const int *scell = a.scell;
     int *nbl = a.nbl;
-    for (int s = g.b * (int)blockDim.x + (int)threadIdx.x; s < n; s += g.nb * (int)blockDim.x) {
-        const float4 pi = pos[s];
-        const int c = scell[s];
-        const int cxy = ncx * ncy;
-        const int cz = c / cxy, rem = c - cz * cxy;
-        const int cy = rem / ncx, cx = rem - cy * ncx;
-        // entry k of slot s at chunk k/4 (cs apart), position k%4
-        int *chunk = nbl + (size_t)s * NB_CHUNK;
-        int cnt = 0;
-        const int ui = excl ? orig_tmp[s] : 0;
-        auto test = [&](float4 pj, int j, float sx, float sy, float sz) {
-            const float d2 =
-                SHIFTED ? dist_sq_shifted<FMA>(pj, pi, sx, sy, sz) : dist_sq_exact<FMA>(pj, pi, Lx, Ly, Lz);
-            if (d2 < cps2 && j != s && !(excl && excluded(a, ui, orig_tmp[j]))) {
-                if (cnt < maxn) chunk[cnt & 3] = j;
-                cnt++;
-                if ((cnt & 3) == 0) chunk += cs;
-            }
-        };
-        for (int za = 0; za < rz; za++) {
-            const int zu = cz - 2 + za;
-            const int z = ncz < 5 ? za : wrap_near(zu, ncz);
-            const float sz = SHIFTED ? (zu < 0 ? -Lz : (zu >= ncz ? Lz : 0.f)) : 0.f;
-            for (int yb = 0; yb < ry; yb++) {
-                const int yu = cy - 2 + yb;
-                const int y = ncy < 5 ? yb : wrap_near(yu, ncy);
-                const float sy = SHIFTED ? (yu < 0 ? -Ly : (yu >= ncy ? Ly : 0.f)) : 0.f;
-                const int rowbase = (z * ncy + y) * ncx;
-                int l0, h0, l1 = 0, h1 = 0;
-                float sx0 = 0.f, sx1 = 0.f;
-                if (ncx <= 5) {
-                    l0 = rowbase;
-                    h0 = rowbase + ncx;
-                } else {
-                    const int x0 = cx - 2, x1 = cx + 2;
-                    if (x0 >= 0 && x1 < ncx) {
-                        l0 = rowbase + x0;
-                        h0 = rowbase + x1 + 1;
-                    } else if (x0 < 0) {
-                        l0 = rowbase + x0 + ncx;
+    // the walk instantiated with and without pair exclusions (uniform)
+    auto walk = [&](auto ex_tag) {
+        constexpr bool EX = decltype(ex_tag)::value;
+        for (int s = g.b * (int)blockDim.x + (int)threadIdx.x; s < n; s += g.nb * (int)blockDim.x) {
+            const float4 pi = pos[s];
+            const int c = scell[s];
+            const int cxy = ncx * ncy;
+            const int cz = c / cxy, rem = c - cz * cxy;
+            const int cy = rem / ncx, cx = rem - cy * ncx;
+            // entry k of slot s at chunk k/4 (cs apart), position k%4
+            int *chunk = nbl + (size_t)s * NB_CHUNK;
+            int cnt = 0;
+            const int ui = EX ? orig_tmp[s] : 0;
+            // the append without a branch: the store (predicated), the count and
+            // the step to the next chunk when one fills
+            auto test = [&](float4 pj, int j, float sx, float sy, float sz) {
+                const float d2 =
+                    SHIFTED ? dist_sq_shifted<FMA>(pj, pi, sx, sy, sz) : dist_sq_exact<FMA>(pj, pi, Lx, Ly, Lz);
+                bool hit = (d2 < cps2) & (j != s);
+                if (EX && hit) hit = !excluded(a, ui, orig_tmp[j]);
+                if (hit & (cnt < maxn)) chunk[cnt & 3] = j;
+                cnt += hit ? 1 : 0;
+                chunk += (hit & ((cnt & 3) == 0)) ? cs : (size_t)0;
+            };
+            for (int za = 0; za < rz; za++) {
+                const int zu = cz - 2 + za;
+                const int z = ncz < 5 ? za : wrap_near(zu, ncz);
+                const float sz = SHIFTED ? (zu < 0 ? -Lz : (zu >= ncz ? Lz : 0.f)) : 0.f;
+                for (int yb = 0; yb < ry; yb++) {
+                    const int yu = cy - 2 + yb;
+                    const int y = ncy < 5 ? yb : wrap_near(yu, ncy);
+                    const float sy = SHIFTED ? (yu < 0 ? -Ly : (yu >= ncy ? Ly : 0.f)) : 0.f;
+                    const int rowbase = (z * ncy + y) * ncx;
+                    int l0, h0, l1 = 0, h1 = 0;
+                    float sx0 = 0.f, sx1 = 0.f;
+                    if (ncx <= 5) {
+                        l0 = rowbase;
                         h0 = rowbase + ncx;
-                        l1 = rowbase;
-                        h1 = rowbase + x1 + 1;
-                        sx0 = -Lx;
                     } else {
-                        l0 = rowbase + x0;
-                        h0 = rowbase + ncx;
-                        l1 = rowbase;
-                        h1 = rowbase + x1 - ncx + 1;
-                        sx1 = Lx;
+                        const int x0 = cx - 2, x1 = cx + 2;
+                        if (x0 >= 0 && x1 < ncx) {
+                            l0 = rowbase + x0;
+                            h0 = rowbase + x1 + 1;
+                        } else if (x0 < 0) {
+                            l0 = rowbase + x0 + ncx;
+                            h0 = rowbase + ncx;
+                            l1 = rowbase;
+                            h1 = rowbase + x1 + 1;
+                            sx0 = -Lx;
+                        } else {
+                            l0 = rowbase + x0;
+                            h0 = rowbase + ncx;
+                            l1 = rowbase;
+                            h1 = rowbase + x1 - ncx + 1;
+                            sx1 = Lx;
+                        }
                     }
-                }
-#pragma unroll
-                for (int r = 0; r < 2; r++) {
-                    const int lc = r ? l1 : l0, hc = r ? h1 : h0;
-                    if (hc <= lc) continue;
-                    const float sx = r ? sx1 : sx0;
-                    const int lo = cstart[lc], hi = cstart[hc];
-                    int j = lo;
-                    for (; j + 4 <= hi; j += 4) {  // four independent loads in flight
-                        const float4 q0 = pos[j], q1 = pos[j + 1], q2 = pos[j + 2], q3 = pos[j + 3];
-                        test(q0, j, sx, sy, sz);
-                        test(q1, j + 1, sx, sy, sz);
-                        test(q2, j + 2, sx, sy, sz);
-                        test(q3, j + 3, sx, sy, sz);
+    #pragma unroll
+                    for (int r = 0; r < 2; r++) {
+                        const int lc = r ? l1 : l0, hc = r ? h1 : h0;
+                        if (hc <= lc) continue;
+                        const float sx = r ? sx1 : sx0;
+                        const int lo = cstart[lc], hi = cstart[hc];
+                        int j = lo;
+                        for (; j + 4 <= hi; j += 4) {  // four independent loads in flight
+                            const float4 q0 = pos[j], q1 = pos[j + 1], q2 = pos[j + 2], q3 = pos[j + 3];
+                            test(q0, j, sx, sy, sz);
+                            test(q1, j + 1, sx, sy, sz);
+                            test(q2, j + 2, sx, sy, sz);
+                            test(q3, j + 3, sx, sy, sz);
+                        }
+                        for (; j < hi; j++) test(pos[j], j, sx, sy, sz);
                     }
-                    for (; j < hi; j++) test(pos[j], j, sx, sy, sz);
                 }
             }
+            a.nbc[s] = cnt;
+            atomicMax(&a.ctrl->maxcount, cnt);
         }
-        a.nbc[s] = cnt;
-        atomicMax(&a.ctrl->maxcount, cnt);
-    }
+    };
+    if (excl)
+        walk(BoolTag<true>{});
+    else
+        walk(BoolTag<false>{});
 }
 
 // Per-warp segment tables of the cell build, in shared memory, for blocks of
