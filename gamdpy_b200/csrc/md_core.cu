@@ -750,11 +750,12 @@ static int status_to_rc(gdb_sim *h) {
 
 // Cluster path or persistent grid for a system that fits a cluster: the
 // cluster (at most 16 SMs, no grid barrier) wins while the list holds fewer
-// than about 160 000 entries, N x (4 pi / 3) (max_cut + skin)^3 N / V;
+// than about 70 000 entries, N x (4 pi / 3) (max_cut + skin)^3 N / V;
 // above that the whole GPU's grid kernel is faster despite its barriers
-// (measured on B200, TPS cluster vs grid: KA rho 1.2 N 1024 87k vs 58k,
-// N 2048 56k vs 56k, N 3000 38k vs 48k; LJ rho 0.973 N 2048 78k vs 89k).
-constexpr double CL_LIST_ENTRIES_MAX = 160000.0;
+// (measured on B200 with every block keeping the step's books, TPS cluster
+// vs grid: KA rho 1.2 N 512 142k vs 132k, N 768 120k vs 126k, N 1024 85k vs
+// 126k; LJ rho 0.973 N 500 191k vs 154k, N 864 134k vs 150k).
+constexpr double CL_LIST_ENTRIES_MAX = 70000.0;
 static bool cluster_preferred(const gdb_sim *h) {
     if (h->cluster_force) return true;
     const double vol = (double)h->box[0] * h->box[1] * h->box[2];
